@@ -1,0 +1,194 @@
+"""Host-side mirror of cc4s's ``CoupledCluster`` algorithm step.
+
+``CoupledCluster().run(arguments)`` takes the same keys as the reference's YAML
+step (src/main/algorithms/CoupledCluster.cxx:56-191) and returns the same
+output map; all work goes through the C ABI of the CUDA library
+(include/cc4s_cc.h).  ``Solver`` is the thin handle wrapper underneath.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+
+class CoupledClusterError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("status %d: %s" % (status, message))
+        self.status = status
+
+
+def _options(lib, arguments):
+    o = _abi.Options()
+    lib.cc4s_cc_default_options(ctypes.byref(o))
+    method = arguments.get("method", "Ccsd")
+    if method not in _abi.METHODS:
+        raise CoupledClusterError(_abi.ERR_INVALID_ARGUMENT, "Unknown method: '%s'" % method)
+    o.method = _abi.METHODS[method]
+    mixer = arguments.get("mixer") or {}
+    mtype = mixer.get("type", "DiisMixer")
+    if mtype not in _abi.MIXERS:
+        raise CoupledClusterError(_abi.ERR_INVALID_ARGUMENT, "Unknown mixer type: '%s'" % mtype)
+    o.mixer = _abi.MIXERS[mtype]
+    o.max_residua = int(mixer.get("maxResidua", 4))
+    o.ratio = float(mixer.get("ratio", 1.0))
+    o.max_iterations = int(arguments.get("maxIterations", 16))
+    o.energy_convergence = float(arguments.get("energyConvergence", 1e-7))
+    o.amplitudes_convergence = float(arguments.get("amplitudesConvergence", 1e-6))
+    o.level_shift = float(arguments.get("levelShift", 0.0))
+    o.integrals_slice_size = int(arguments.get("integralsSliceSize", 0) or 0)
+    o.ppl = 1 if arguments.get("ppl", True) else 0
+    o.precision = _abi.PRECISIONS[arguments.get("precision", "fp64")]
+    o.device = int(arguments.get("device", 0))
+    return o
+
+
+class Solver:
+    """One library handle: inputs resident on the device, residual and run entries."""
+
+    def __init__(self, arguments=None, lib=None):
+        self.lib = _abi.load(lib)
+        self.h = ctypes.c_void_p()
+        self.opts = _options(self.lib, arguments or {})
+        st = self.lib.cc4s_cc_create(ctypes.byref(self.opts), ctypes.byref(self.h))
+        if st:
+            raise CoupledClusterError(st, self.lib.cc4s_cc_last_error(None).decode())
+        self.No = self.Nv = self.NG = None
+        self.cplx = False
+
+    def _check(self, st, ok=(0,)):
+        if st not in ok:
+            raise CoupledClusterError(st, self.lib.cc4s_cc_last_error(self.h).decode())
+        return st
+
+    def close(self):
+        if self.h:
+            self.lib.cc4s_cc_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_inputs(self, eps_h, eps_p, gamma, half_grid=True):
+        eps_h = np.ascontiguousarray(eps_h, dtype=np.float64)
+        eps_p = np.ascontiguousarray(eps_p, dtype=np.float64)
+        gamma = np.asarray(gamma)
+        NG, Np, Np2 = gamma.shape
+        No, Nv = eps_h.size, eps_p.size
+        if Np != No + Nv or Np2 != Np:
+            raise CoupledClusterError(_abi.ERR_BAD_SHAPE, "vertex shape %s vs No=%d Nv=%d" % (gamma.shape, No, Nv))
+        cplx = np.iscomplexobj(gamma)
+        g = _abi.as_f64(gamma)
+        self._check(self.lib.cc4s_cc_set_inputs(self.h, _abi.ptr(eps_h), No, _abi.ptr(eps_p), Nv,
+                                                _abi.ptr(g), NG, int(cplx), int(bool(half_grid))))
+        self.No, self.Nv, self.NG = No, Nv, NG
+        self.cplx = cplx and not half_grid
+
+    def _dtype(self):
+        return np.complex128 if self.cplx else np.float64
+
+    def set_initial_amplitudes(self, T1, T2):
+        t1 = _abi.as_f64(np.asarray(T1, dtype=self._dtype()))
+        t2 = _abi.as_f64(np.asarray(T2, dtype=self._dtype()))
+        self._check(self.lib.cc4s_cc_set_initial_amplitudes(self.h, _abi.ptr(t1), _abi.ptr(t2)))
+
+    def _alloc_amps(self):
+        k = 2 if self.cplx else 1
+        return (np.zeros(self.Nv * self.No * k), np.zeros((self.Nv * self.No) ** 2 * k))
+
+    def _unpack(self, b1, b2):
+        No, Nv = self.No, self.Nv
+        if self.cplx:
+            b1, b2 = b1.view(np.complex128), b2.view(np.complex128)
+        return b1.reshape((Nv, No), order="F"), b2.reshape((Nv, Nv, No, No), order="F")
+
+    def residual(self, T=None):
+        """One residual evaluation, Ccsd::getResiduum; T is None or (T1, T2)."""
+        r1, r2 = self._alloc_amps()
+        if T is None:
+            self._check(self.lib.cc4s_cc_residual(self.h, None, None, _abi.ptr(r1), _abi.ptr(r2)))
+        else:
+            t1 = _abi.as_f64(np.asarray(T[0], dtype=self._dtype()))
+            t2 = _abi.as_f64(np.asarray(T[1], dtype=self._dtype()))
+            self._check(self.lib.cc4s_cc_residual(self.h, _abi.ptr(t1), _abi.ptr(t2),
+                                                  _abi.ptr(r1), _abi.ptr(r2)))
+        return self._unpack(r1, r2)
+
+    def run(self):
+        res = _abi.Result()
+        st = self._check(self.lib.cc4s_cc_run(self.h, ctypes.byref(res)),
+                         ok=(0, _abi.WARN_NOT_CONVERGED))
+        n = res.history_len
+        hist = [dict(energy=res.energy[k], dE=res.delta_energy[k], dR=res.residuum_norm[k],
+                     seconds=res.seconds[k]) for k in range(n)]
+        return dict(status=st, correlation=res.correlation, direct=res.direct,
+                    exchange=res.exchange, secondOrder=res.second_order,
+                    correlation_imag=res.correlation_imag, iterations=res.iterations,
+                    converged=bool(res.converged), history=hist,
+                    flops_per_iteration=res.flops_per_iteration)
+
+    def amplitudes(self):
+        t1, t2 = self._alloc_amps()
+        self._check(self.lib.cc4s_cc_get_amplitudes(self.h, _abi.ptr(t1), _abi.ptr(t2)))
+        return self._unpack(t1, t2)
+
+    def stats(self):
+        s = _abi.Stats()
+        self._check(self.lib.cc4s_cc_get_stats(self.h, ctypes.byref(s)))
+        return dict(gemm_launches=s.gemm_launches, other_launches=s.other_launches,
+                    device_bytes=s.device_bytes, flops_per_residual=s.flops_per_residual)
+
+
+def _full_vertex(arguments):
+    if "coulombVertex" in arguments:
+        return np.asarray(arguments["coulombVertex"])
+    sl = arguments["slicedCoulombVertex"]
+    hh, hp, ph, pp = (np.asarray(sl[k]) for k in ("hh", "hp", "ph", "pp"))
+    NG, No, Nv = hh.shape[0], hh.shape[1], pp.shape[1]
+    dt = np.result_type(hh, hp, ph, pp)
+    g = np.zeros((NG, No + Nv, No + Nv), dtype=dt)
+    g[:, :No, :No], g[:, :No, No:], g[:, No:, :No], g[:, No:, No:] = hh, hp, ph, pp
+    return g
+
+
+class CoupledCluster:
+    """The cc4s ``CoupledCluster`` step (methods Ccsd and Ccd).
+
+    ``arguments`` holds the reference's input keys: slicedEigenEnergies
+    ({'h': eps_h, 'p': eps_p}), slicedCoulombVertex ({'hh','hp','ph','pp'}
+    slices of Gamma[G,p,q]) or coulombVertex (the full Gamma), halfGrid (the
+    vertex metadata that selects the real integral path), coulombIntegrals
+    (accepted and not needed), method, mixer, maxIterations,
+    energyConvergence, amplitudesConvergence, levelShift, initialAmplitudes
+    ({'ph': T1, 'pphh': T2}), integralsSliceSize and ppl.
+    """
+
+    def __init__(self, lib=None):
+        self.lib = lib
+
+    def run(self, arguments):
+        eps = arguments["slicedEigenEnergies"]
+        gamma = _full_vertex(arguments)
+        half_grid = bool(arguments.get("halfGrid", not np.iscomplexobj(gamma)))
+        s = Solver(arguments, lib=self.lib)
+        try:
+            s.set_inputs(eps["h"], eps["p"], gamma, half_grid=half_grid)
+            init = arguments.get("initialAmplitudes")
+            if init is not None:
+                s.set_initial_amplitudes(init["ph"], init["pphh"])
+            r = s.run()
+            T1, T2 = s.amplitudes()
+        finally:
+            s.close()
+        energy = dict(correlation=r["correlation"], direct=r["direct"], exchange=r["exchange"],
+                      unit=1.0)
+        if not np.isnan(r["secondOrder"]):
+            energy["secondOrder"] = r["secondOrder"]
+        return {"energy": energy, "convergenceReached": r["converged"],
+                "amplitudes": {"ph": T1, "pphh": T2}, "iterations": r["iterations"],
+                "history": r["history"]}

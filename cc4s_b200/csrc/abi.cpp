@@ -1,0 +1,293 @@
+// Iteration loop (CoupledCluster::run) and the extern "C" entry points.
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <string>
+
+#include "driver.h"
+
+namespace cc4s_b200 {
+
+// Reference layout T1[a,i], T2[a,b,i,j] (first index fastest) -> amplitude vector.
+void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2) {
+  const int64_t o = shape.o, v = shape.v, n1 = v * o;
+  double* st = Rs[0];
+  ops::h2d(st, T1, n1, stream);
+  ops::h2d(st + n1, T2, n1 * n1, stream);
+  const int64_t d1[4] = {1, 1, o, v};
+  const int p1[4] = {0, 1, 3, 2};
+  ops::permute4(dst, st, d1, p1, 1.0, 0.0, stream);
+  const int64_t d2[4] = {o, o, v, v};  // [j][i][b][a]
+  const int p2[4] = {3, 1, 2, 0};      // -> [a][i][b][j]
+  ops::permute4(dst + n1, st + n1, d2, p2, 1.0, 0.0, stream);
+}
+
+void Handle::download_amplitudes(const double* src, double* T1, double* T2) {
+  const int64_t o = shape.o, v = shape.v, n1 = v * o;
+  double* st = Rs[0];
+  const int64_t d1[4] = {1, 1, v, o};
+  const int p1[4] = {0, 1, 3, 2};
+  ops::permute4(st, src, d1, p1, 1.0, 0.0, stream);
+  const int64_t d2[4] = {v, o, v, o};  // [a][i][b][j]
+  const int p2[4] = {3, 1, 2, 0};      // -> [j][i][b][a]
+  ops::permute4(st + n1, src + n1, d2, p2, 1.0, 0.0, stream);
+  if (T1) ops::d2h(T1, st, n1, stream);
+  if (T2) ops::d2h(T2, st + n1, n1 * n1, stream);
+  ops::sync(stream);
+}
+
+void Handle::set_initial(const double* T1, const double* T2) {
+  require_inputs();
+  if (!T1 || !T2) throw Error(ERR_INVALID_ARGUMENT, "null amplitudes");
+  const int64_t n1 = shape.n1();
+  for (int64_t k = 0; k < n1; ++k)
+    if (!std::isfinite(T1[k])) throw Error(ERR_NON_FINITE, "non-finite T1");
+  for (int64_t k = 0; k < n1 * n1; ++k)
+    if (!std::isfinite(T2[k])) throw Error(ERR_NON_FINITE, "non-finite T2");
+  upload_amplitudes(Tcur, T1, T2);
+  ops::sync(stream);
+  have_T = true;
+}
+
+void Handle::mix(double* A_new, double* dT_new, double* norm2_dev) {
+  const int64_t n = shape.total();
+  if (opt.mixer == CC4S_MIXER_LINEAR) {
+    const double r = opt.ratio;
+    if (!linear_has_last) {
+      ops::d2d(Tcur, A_new, n, stream);
+      ops::d2d(dTlast, dT_new, n, stream);
+      linear_has_last = true;
+    } else {
+      ops::axpby(Tcur, r, A_new, 1.0 - r, Tcur, 0.0, n, stream);
+      ops::axpby(dTlast, r, dT_new, 1.0 - r, dTlast, 0.0, n, stream);
+    }
+    const double* ys[1] = {dTlast};
+    ops::dots(dTlast, ys, 1, n, norm2_dev, ws, stream);
+    return;
+  }
+  const int N = static_cast<int>(A.size());
+  const int next = next_index;
+  valid[next] = 1;
+  const double* ys[8];
+  int ny = 0;
+  for (int i = 0; i < N; ++i)
+    if (valid[i]) ys[ny++] = Rs[i];
+  ops::dots(Rs[next], ys, ny, n, scal + 8, ws, stream);
+  if (count < N) ++count;
+  ops::diis_solve(B, scal + 8, valid.data(), N, next, count, coef, status_dev, stream);
+  const double* xs[16];
+  const double* rs[16];
+  for (int j = 0; j < count; ++j) {
+    const int slot = (next + N - j) % N;
+    xs[j] = A[slot];
+    rs[j] = Rs[slot];
+  }
+  ops::lincomb(Tcur, xs, rs, coef, count, n, norm2_dev, ws, stream);
+  next_index = (next + 1) % N;
+}
+
+int Handle::run(cc4s_cc_result* out) {
+  require_inputs();
+  std::memset(out, 0, sizeof(*out));
+  out->second_order = std::nan("");
+  reset_mixer();
+  const int maxIt = opt.max_iterations;
+  const double shift = opt.level_shift;
+  const int N = static_cast<int>(A.size());
+  std::complex<double> e(0.0, 0.0), prev(0.0, 0.0);
+  double host[8];
+  double Dr = 0, Xr = 0;
+  int i = 0;
+  for (; i < maxIt; ++i) {
+    ops::event_record(ev0, stream);
+    solver->residual(have_T ? Tcur : nullptr, Rbuf);
+    const int slot = opt.mixer == CC4S_MIXER_DIIS ? next_index : 0;
+    ops::jacobi(A[slot], Rs[slot], Rbuf, have_T ? Tcur : nullptr, sys.eh, sys.ep, shape, shift,
+                stream);
+    const bool second = !have_T;
+    mix(A[slot], Rs[slot], scal + 4);
+    have_T = true;
+    ops::energy(Tcur, solver->Vd(), nullptr, solver->Ve(), nullptr, shape, scal, ws, stream);
+    ops::event_record(ev1, stream);
+    ops::d2h(host, scal, 5, stream);
+    double st = 0.0;
+    if (opt.mixer == CC4S_MIXER_DIIS) ops::d2h(&st, reinterpret_cast<double*>(status_dev), 1, stream);
+    ops::sync(stream);
+    const float ms = ops::event_ms(ev0, ev1);
+    int status_int;
+    std::memcpy(&status_int, &st, sizeof(int));
+    if (opt.mixer == CC4S_MIXER_DIIS && status_int != 0)
+      throw Error(ERR_DIIS_SINGULAR, "Diagonalization failed (singular DIIS system)");
+    Dr = host[0]; Xr = host[1];
+    e = std::complex<double>(host[0] + host[1], host[2] + host[3]);
+    const double norm = std::sqrt(host[4]);
+    if (!std::isfinite(e.real()) || !std::isfinite(norm))
+      throw Error(ERR_NON_FINITE, "non-finite energy or residuum norm at iteration " + std::to_string(i + 1));
+    if (i < CC4S_MAX_HISTORY) {
+      out->energy[i] = e.real();
+      out->delta_energy[i] = (e - prev).real();
+      out->residuum_norm[i] = norm;
+      out->seconds[i] = ms * 1e-3;
+      out->history_len = i + 1;
+    }
+    if (second) out->second_order = e.real();
+    if (std::abs(e - prev) < opt.energy_convergence && norm < opt.amplitudes_convergence) break;
+    prev = e;
+  }
+  (void)N;
+  if (maxIt == 0) {
+    if (!have_T) throw Error(ERR_STATE, "maxIterations = 0 needs initial amplitudes");
+    ops::energy(Tcur, solver->Vd(), nullptr, solver->Ve(), nullptr, shape, scal, ws, stream);
+    ops::d2h(host, scal, 4, stream);
+    ops::sync(stream);
+    Dr = host[0]; Xr = host[1];
+    e = std::complex<double>(host[0] + host[1], host[2] + host[3]);
+  }
+  out->correlation = e.real();
+  out->correlation_imag = e.imag();
+  out->direct = Dr;
+  out->exchange = Xr;
+  out->iterations = (i < maxIt) ? i + 1 : maxIt;
+  out->converged = i < maxIt ? 1 : 0;
+  out->flops_per_iteration = solver->flops_per_residual();
+  return (maxIt > 0 && i == maxIt) ? ERR_NOT_CONVERGED : OK;
+}
+
+void Handle::get_amplitudes(double* T1, double* T2) {
+  require_inputs();
+  if (!have_T) throw Error(ERR_STATE, "no amplitudes: run first");
+  download_amplitudes(Tcur, T1, T2);
+}
+
+void Handle::residual(const double* T1, const double* T2, double* R1, double* R2) {
+  require_inputs();
+  const int64_t n1 = shape.n1();
+  const bool first = (T1 == nullptr && T2 == nullptr);
+  if (!first) {
+    if (!T1 || !T2) throw Error(ERR_INVALID_ARGUMENT, "give both T1 and T2, or neither");
+    upload_amplitudes(A[0], T1, T2);
+  }
+  solver->residual(first ? nullptr : A[0], Rbuf);
+  download_amplitudes(Rbuf, R1, R2);
+  (void)n1;
+}
+
+}  // namespace cc4s_b200
+
+// ---------------------------------------------------------------------------
+using cc4s_b200::Error;
+using cc4s_b200::Handle;
+
+struct cc4s_cc_handle {
+  Handle* impl;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(cc4s_cc_handle* h, F&& f) {
+  try {
+    return f();
+  } catch (const Error& e) {
+    if (h && h->impl) h->impl->error = e.what(); else g_create_error = e.what();
+    return e.status;
+  } catch (const std::exception& e) {
+    if (h && h->impl) h->impl->error = e.what(); else g_create_error = e.what();
+    return cc4s_b200::ERR_CUDA;
+  } catch (...) {
+    if (h && h->impl) h->impl->error = "unknown error"; else g_create_error = "unknown error";
+    return cc4s_b200::ERR_CUDA;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+void cc4s_cc_default_options(cc4s_cc_options* o) {
+  if (!o) return;
+  o->method = CC4S_METHOD_CCSD;
+  o->precision = CC4S_PRECISION_FP64;
+  o->mixer = CC4S_MIXER_DIIS;
+  o->max_residua = 4;
+  o->ratio = 1.0;
+  o->max_iterations = 16;
+  o->energy_convergence = 1e-7;
+  o->amplitudes_convergence = 1e-6;
+  o->level_shift = 0.0;
+  o->integrals_slice_size = 0;
+  o->ppl = 1;
+  o->device = 0;
+}
+
+int cc4s_cc_create(const cc4s_cc_options* opt, cc4s_cc_handle** h) {
+  if (!opt || !h) { g_create_error = "null argument"; return CC4S_ERR_INVALID_ARGUMENT; }
+  *h = nullptr;
+  return guarded(nullptr, [&] {
+    auto* hh = new cc4s_cc_handle{nullptr};
+    try {
+      hh->impl = new Handle(*opt);
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *h = hh;
+    return 0;
+  });
+}
+
+int cc4s_cc_set_inputs(cc4s_cc_handle* h, const double* eps_h, int64_t No, const double* eps_p,
+                       int64_t Nv, const double* gamma, int64_t NG, int is_complex,
+                       int half_grid) {
+  if (!h || !h->impl) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] {
+    h->impl->set_inputs(eps_h, No, eps_p, Nv, gamma, NG, is_complex != 0, half_grid != 0);
+    return 0;
+  });
+}
+
+int cc4s_cc_set_initial_amplitudes(cc4s_cc_handle* h, const double* T1, const double* T2) {
+  if (!h || !h->impl) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] { h->impl->set_initial(T1, T2); return 0; });
+}
+
+int cc4s_cc_run(cc4s_cc_handle* h, cc4s_cc_result* out) {
+  if (!h || !h->impl || !out) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] { return h->impl->run(out); });
+}
+
+int cc4s_cc_get_amplitudes(cc4s_cc_handle* h, double* T1, double* T2) {
+  if (!h || !h->impl) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] { h->impl->get_amplitudes(T1, T2); return 0; });
+}
+
+int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, double* R1,
+                     double* R2) {
+  if (!h || !h->impl || !R1 || !R2) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] { h->impl->residual(T1, T2, R1, R2); return 0; });
+}
+
+int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
+  if (!h || !h->impl || !out) return CC4S_ERR_INVALID_ARGUMENT;
+  out->gemm_launches = cc4s_b200::gemm_launch_count();
+  out->other_launches = cc4s_b200::ops::launch_count();
+  size_t bytes = 0;
+  if (h->impl->solver) bytes += h->impl->solver->device_bytes();
+  out->device_bytes = bytes;
+  out->flops_per_residual = h->impl->solver ? h->impl->solver->flops_per_residual() : 0.0;
+  return 0;
+}
+
+int cc4s_cc_destroy(cc4s_cc_handle* h) {
+  if (!h) return CC4S_ERR_INVALID_ARGUMENT;
+  int st = guarded(h, [&] { delete h->impl; h->impl = nullptr; return 0; });
+  delete h;
+  return st;
+}
+
+const char* cc4s_cc_last_error(const cc4s_cc_handle* h) {
+  if (h && h->impl) return h->impl->error.c_str();
+  return g_create_error.c_str();
+}
+
+}  // extern "C"

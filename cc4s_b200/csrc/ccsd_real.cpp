@@ -1,0 +1,502 @@
+// Real-path CCSD / CCD residual, restated from cc4s Ccsd<Real>::getResiduum
+// (src/main/algorithms/coupledcluster/Ccsd.cxx:77-378) as a schedule of FP64
+// tensor-core contractions on HBM-resident tensors.
+//
+// Layouts (row-major, all FP64):
+//   T1, R1        [a][i]                         (v x o)
+//   T2, R2 "pair" [a][i][b][j]  = X_abij          ((vo) x (vo), symmetric matrix)
+//   "exchange"    Ae[a][i][b][j] = A_abji          (pair layout with i <-> j)
+//   "pp"          Ap[a][b][i][j] = A_abij
+//   vertex        Gpp[G][a][b], Gph[G][a][i], Ghh[G][k][i], Ghp[G][i][a]
+//
+// Exact algebraic rearrangements relative to the reference (each term is the
+// same sum, only the contraction order changes):
+//   * ring (Ccsd.cxx:215-229): the two V_dclk terms are folded into the
+//     vertex, Z_Gai = sum_dl Gamma_Gdl (T_adil - X'_dail/2), and the vertex part of
+//     Xakic is contracted as (dGamma + Z)^T (Gamma (2T - T^x)) without forming
+//     the v^2 o^2 intermediate; only the exchange part -V_cdlk T_adil / 2 is a
+//     (vo)^3 contraction;
+//   * crossed ring (Ccsd.cxx:233-253): the second term, sum Xbkci T_ackj, is
+//     written straight into the exchange pairing of R2;
+//   * the particle-particle ladder (Ccsd.cxx:283-333) is evaluated on square
+//     slabs of the virtual index pair (a >= b blocks, mirrored into (b,a,j,i)),
+//     V_abcd built per slab from the dressed vertex and never stored whole;
+//   * singles (Ccsd.cxx:339-375): the Gamma.Gamma.X pair shares one
+//     Gamma (2X - X^x) intermediate.
+#include "ccsd_real.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace cc4s_b200 {
+
+namespace {
+View vw(double* p, int64_t s_ro, int64_t s_ri, int64_t s_co, int64_t s_ci, int64_t s_bo = 0,
+        int64_t s_bi = 0) {
+  View v;
+  v.p = p; v.s_ro = s_ro; v.s_ri = s_ri; v.s_co = s_co; v.s_ci = s_ci; v.s_bo = s_bo;
+  v.s_bi = s_bi;
+  return v;
+}
+inline double* cp(const double* p) { return const_cast<double*>(p); }
+}  // namespace
+
+double* CcsdReal::take(size_t elems) {
+  double* p = ops::alloc(elems);
+  owned_.push_back(p);
+  bytes_ += elems * sizeof(double);
+  return p;
+}
+
+CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
+    : sys_(sys), opt_(opt), s_(s) {
+  const int64_t o = sys.o, v = sys.v, G = sys.G, n1 = v * o, D2 = n1 * n1;
+  if (o <= 0 || v <= 0 || G <= 0) throw Error(ERR_BAD_SHAPE, "CcsdReal: empty dimension");
+  try {
+    // split-K scratch
+    scratch_.elems = static_cast<size_t>(std::max<int64_t>(int64_t(1) << 22,
+                                                           std::min<int64_t>(64 * v * v, int64_t(1) << 25)));
+    scratch_.p = take(scratch_.elems);
+    Vd_ = take(D2); Ve_ = take(D2); Vp_ = take(D2); Vtp_ = take(D2);
+    Vhhhh_ = take(o * o * o * o); Vhhhp_ = take(o * o * o * v); Vh2_ = take(o * o * o * v);
+    Xd_ = take(D2); Xp_ = take(D2); Te_ = take(D2); Y_ = take(D2); W8_ = take(D2);
+    Tp_ = take(D2); EX_ = take(D2);
+    Kki_ = take(o * o); Kac_ = take(v * v); Lac_ = take(v * v); Lki_ = take(o * o);
+    jG_ = take(G);
+    U_ = take(G * n1); dGph_ = take(G * n1); W_ = take(G * n1); Z_ = take(G * n1);
+    W1_ = take(G * n1); F_ = take(G * n1);
+    dGpp_ = take(G * v * v); dGhh_ = take(G * o * o);
+    Q_ = take(n1 * o * o); Xkl1_ = take(o * o * o * o); Xkl2_ = take(o * o * o * o);
+    kck_ = take(n1); P1_ = take(o * o); P_ = take(G * o * v);
+    // PPL slab: s x s virtual pairs times v^2, bounded to 2^28 doubles.
+    int64_t sl = opt.slab;
+    if (sl <= 0) {
+      const double budget = double(int64_t(1) << 28);
+      sl = static_cast<int64_t>(std::floor(std::sqrt(budget / double(v * v))));
+      if (sl >= 16) sl = (sl / 8) * 8;
+      sl = std::max<int64_t>(1, std::min(sl, v));
+    }
+    slab_rows_ = std::min(sl, v);
+    if (opt.ppl) slab_ = take(slab_rows_ * slab_rows_ * v * v);
+  } catch (...) {
+    for (double* p : owned_) ops::release(p);
+    owned_.clear();
+    throw;
+  }
+  count_flops_ = false;
+  build_integrals();
+  count_flops_ = true;
+}
+
+CcsdReal::~CcsdReal() {
+  for (double* p : owned_) ops::release(p);
+}
+
+void CcsdReal::gemm_(const Contraction& c) {
+  if (count_flops_) flops_ += 2.0 * double(c.M) * double(c.N) * double(c.K) * double(c.batch);
+  gemm(c, s_, scratch_);
+}
+
+// Iteration-independent integrals (VertexCoulombIntegrals.cxx:87-121).
+void CcsdReal::build_integrals() {
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o;
+  // Vd[(a,i),(b,j)] = V_abij = sum_G Gph[G][a][i] Gph[G][b][j]
+  {
+    Contraction c; c.M = n1; c.N = n1; c.K = G;
+    c.A = tr(sys_.Gph, n1); c.B = rm(sys_.Gph, n1); c.C = rm(Vd_, n1);
+    gemm_(c);
+  }
+  const int64_t d4[4] = {v, o, v, o};
+  // Ve[(a,i),(b,j)] = V_baij = V_abji ; Vp[a][b][i][j] = V_abij
+  { const int pm[4] = {0, 3, 2, 1}; ops::permute4(Ve_, Vd_, d4, pm, 1.0, 0.0, s_); }
+  { const int pm[4] = {0, 2, 1, 3}; ops::permute4(Vp_, Vd_, d4, pm, 1.0, 0.0, s_); }
+  // Vtp[c][d][k][l] = 2 V_cdkl - V_dckl = 2 Vp[c][d][k][l] - Vp[c][d][l][k]
+  {
+    const int64_t dp[4] = {v, v, o, o};
+    const int pm[4] = {0, 1, 3, 2};
+    ops::permute4(Vtp_, Vp_, dp, pm, -1.0, 0.0, s_);
+    ops::axpby(Vtp_, 2.0, Vp_, 1.0, Vtp_, 0.0, n1 * n1, s_);
+  }
+  // Vhhhh[k][l][i][j] = sum_G Ghh[G][k][i] Ghh[G][l][j]
+  {
+    Contraction c; c.M = o * o; c.N = o * o; c.K = G; c.Mi = o; c.Ni = o;
+    c.A = vw(sys_.Ghh, o, 1, 0, o * o);            // (m=(k,i), G)
+    c.B = vw(sys_.Ghh, 0, o * o, o, 1);            // (G, n=(l,j))
+    c.C = vw(Vhhhh_, o * o * o, o, o * o, 1);      // [k][l][i][j]
+    gemm_(c);
+  }
+  // Vhhhp[k][l][i][c] = sum_G Ghh[G][k][i] Ghp[G][l][c]
+  {
+    Contraction c; c.M = o * o; c.N = o * v; c.K = G; c.Mi = o; c.Ni = v;
+    c.A = vw(sys_.Ghh, o, 1, 0, o * o);
+    c.B = vw(sys_.Ghp, 0, o * v, v, 1);
+    c.C = vw(Vhhhp_, o * o * v, v, o * v, 1);
+    gemm_(c);
+  }
+  // Vh2[i][c][k][l] = 2 V_klic - V_lkic
+  {
+    const int64_t dh[4] = {o, o, o, v};
+    const int pa[4] = {2, 3, 0, 1};
+    const int pb[4] = {2, 3, 1, 0};
+    ops::permute4(Vh2_, Vhhhp_, dh, pa, 2.0, 0.0, s_);
+    ops::permute4(Vh2_, Vhhhp_, dh, pb, -1.0, 1.0, s_);
+  }
+}
+
+void CcsdReal::residual(const double* T, double* R) {
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o, D2 = n1 * n1;
+  double* R1 = R;
+  double* R2 = R + n1;
+  if (!T) {  // Ccsd.cxx:97-102
+    ops::zero(R1, n1, s_);
+    ops::d2d(R2, Vd_, D2, s_);
+    return;
+  }
+  const bool ccd = opt_.ccd;
+  flops_ = 0.0;
+  double* t = cp(T);
+  double* Td = cp(T + n1);
+  double* Gpp = sys_.Gpp;
+  double* Gph = sys_.Gph;
+  double* Ghh = sys_.Ghh;
+  const int64_t d4[4] = {v, o, v, o};
+  const int p_pp[4] = {0, 2, 1, 3};   // pair -> pp
+  const int p_ex[4] = {0, 3, 2, 1};   // pair -> exchange
+
+  // ---- X = T2 + T1 T1 (Ccsd.cxx:169-170) -----------------------------------
+  if (ccd) ops::d2d(Xd_, Td, D2, s_);
+  else ops::rank1(Xd_, 1.0, Td, 1.0, t, n1, s_);
+  ops::permute4(Xp_, Xd_, d4, p_pp, 1.0, 0.0, s_);
+
+  // ---- Kki, Kac (Ccsd.cxx:172-178) -------------------------------------------
+  {  // Kki[k][i] = sum_{cd,l} Vtp[cd][k][l] Xp[cd][i][l]
+    Contraction c; c.M = o; c.N = o; c.K = v * v * o; c.Ki = o;
+    c.A = vw(Vtp_, 0, o, o * o, 1);
+    c.B = vw(Xp_, o * o, 1, 0, o);
+    c.C = rm(Kki_, o);
+    gemm_(c);
+  }
+  {  // Kac[a][c] = -sum_{dkl} Xp[a][dkl] Vtp[c][dkl]
+    Contraction c; c.M = v; c.N = v; c.K = v * o * o;
+    c.A = rm(Xp_, v * o * o); c.B = tr(Vtp_, v * o * o); c.C = rm(Kac_, v);
+    c.alpha = -1.0;
+    gemm_(c);
+  }
+  // ---- Lac (Ccsd.cxx:180-189) --------------------------------------------------
+  ops::d2d(Lac_, Kac_, v * v, s_);
+  if (!ccd) {
+    {  // jG[G] = sum_{dk} Gph[G][dk] t[dk]
+      Contraction c; c.M = G; c.N = 1; c.K = n1;
+      c.A = rm(Gph, n1); c.B = vw(t, 0, 1, 0, 0); c.C = vw(jG_, 0, 1, 0, 0);
+      gemm_(c);
+    }
+    {  // Lac[a][c] += 2 sum_G Gpp[G][c][a] jG[G]      (m = (c,a))
+      Contraction c; c.M = v * v; c.N = 1; c.K = G; c.Mi = v;
+      c.A = vw(Gpp, v, 1, 0, v * v);
+      c.B = vw(jG_, 0, 1, 0, 0);
+      c.C = vw(Lac_, 1, v, 0, 0);
+      c.alpha = 2.0; c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // U[G][a][k] = sum_d Gpp[G][d][a] t[d][k]
+      Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(tr(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(U_, o), n1);
+      gemm_(c);
+    }
+    {  // Lac[a][c] -= sum_{G,k} U[G][a][k] Gph[G][c][k]
+      Contraction c; c.M = v; c.N = v; c.K = G * o; c.Ki = o;
+      c.A = vw(U_, 0, o, n1, 1);
+      c.B = vw(Gph, n1, 1, 0, o);
+      c.C = rm(Lac_, v);
+      c.alpha = -1.0; c.beta = 1.0;
+      gemm_(c);
+    }
+  }
+  // ---- Lki (Ccsd.cxx:175,192-193) --------------------------------------------
+  ops::d2d(Lki_, Kki_, o * o, s_);
+  if (!ccd) {  // Lki[k][i] += sum_{c,l} (2 V_klic - V_lkic) t[c][l]
+    Contraction c; c.M = o * o; c.N = 1; c.K = v * o; c.Mi = o; c.Ki = o;
+    c.A = vw(Vh2_, v * o * o, o, o * o, 1);
+    c.B = vw(t, o, 1, 0, 0);
+    c.C = vw(Lki_, 1, o, 0, 0);
+    c.beta = 1.0;
+    gemm_(c);
+  }
+  // ---- R2 = Lac T2 - Lki T2 (Ccsd.cxx:195-197) ---------------------------------
+  {
+    Contraction c; c.M = v; c.N = o * n1; c.K = v;
+    c.A = rm(Lac_, v); c.B = rm(Td, o * n1); c.C = rm(R2, o * n1);
+    gemm_(c);
+  }
+  {
+    Contraction c; c.M = o; c.N = n1; c.K = o; c.batch = v;
+    c.A = tr(Lki_, o); c.B = with_batch(rm(Td, n1), o * n1); c.C = with_batch(rm(R2, n1), o * n1);
+    c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  // ---- T1-dressed vertex terms (Ccsd.cxx:201-210) ----------------------------
+  ops::d2d(dGph_, Gph, G * n1, s_);
+  if (!ccd) {
+    {  // dGph[G][a][i] -= sum_k t[a][k] Ghh[G][k][i]
+      Contraction c; c.M = v; c.N = o; c.K = o; c.batch = G;
+      c.A = rm(t, o); c.B = with_batch(rm(Ghh, o), o * o); c.C = with_batch(rm(dGph_, o), n1);
+      c.alpha = -1.0; c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // W[G][b][j] = sum_c Gpp[G][b][c] t[c][j]
+      Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(rm(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(W_, o), n1);
+      gemm_(c);
+    }
+    {  // R2 += dGph^T W
+      Contraction c; c.M = n1; c.N = n1; c.K = G;
+      c.A = tr(dGph_, n1); c.B = rm(W_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // R2[a][i][b][j] -= sum_k Vhhhp[j][i][k][a] t[b][k]      (batch j, m = (a,i))
+      Contraction c; c.M = n1; c.N = v; c.K = o; c.batch = o; c.Mi = o;
+      c.A = vw(Vhhhp_, 1, o * v, 0, v, 0, o * o * v);
+      c.B = tr(t, o);
+      c.C = vw(R2, o * n1, n1, 0, o, 0, 1);
+      c.alpha = -1.0; c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // Q[(a,i)][k][j] = sum_c Vd[(a,i)][c][k] t[c][j]
+      Contraction c; c.M = o; c.N = o; c.K = v; c.batch = n1;
+      c.A = with_batch(tr(Vd_, o), n1); c.B = rm(t, o); c.C = with_batch(rm(Q_, o), o * o);
+      gemm_(c);
+    }
+    {  // R2[(a,i)][b][j] -= sum_k t[b][k] Q[(a,i)][k][j]
+      Contraction c; c.M = v; c.N = o; c.K = o; c.batch = n1;
+      c.A = rm(t, o); c.B = with_batch(rm(Q_, o), o * o); c.C = with_batch(rm(R2, o), n1);
+      c.alpha = -1.0; c.beta = 1.0;
+      gemm_(c);
+    }
+  }
+  // ---- ring Xakic (Ccsd.cxx:215-229) -------------------------------------------
+  ops::permute4(Te_, Td, d4, p_ex, 1.0, 0.0, s_);                 // Te = T^x
+  if (ccd) ops::d2d(W8_, Td, D2, s_);
+  else ops::rank1(W8_, 1.0, Td, 2.0, t, n1, s_);                 // X' = T2 + 2 T1 T1
+  ops::permute4(Y_, W8_, d4, p_ex, 1.0, 0.0, s_);                 // X'^x
+  ops::axpby(W8_, 1.0, Td, -0.5, Y_, 0.0, D2, s_);               // M1 = T - X'^x / 2
+  ops::axpby(Y_, 2.0, Td, -1.0, Te_, 0.0, D2, s_);               // Y = 2T - T^x
+  {  // Z = Gph M1
+    Contraction c; c.M = G; c.N = n1; c.K = n1;
+    c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(Z_, n1);
+    gemm_(c);
+  }
+  if (!ccd) {  // dGph[G][a][i] += sum_d Gpp[G][a][d] t[d][i]
+    Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+    c.A = with_batch(rm(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(dGph_, o), n1);
+    c.beta = 1.0;
+    gemm_(c);
+  }
+  ops::axpby(dGph_, 1.0, dGph_, 1.0, Z_, 0.0, G * n1, s_);       // A2 = dGph + Z
+  {  // W1 = Gph Y
+    Contraction c; c.M = G; c.N = n1; c.K = n1;
+    c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(W1_, n1);
+    gemm_(c);
+  }
+  {  // R2 += A2^T W1
+    Contraction c; c.M = n1; c.N = n1; c.K = G;
+    c.A = tr(dGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // EX = -1/2 T Ve
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(Td, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
+    gemm_(c);
+  }
+  {  // R2 += EX Y
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(EX_, n1); c.B = rm(Y_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+    gemm_(c);
+  }
+  // ---- crossed ring Xakci (Ccsd.cxx:233-253) ------------------------------------
+  ops::d2d(dGpp_, Gpp, G * v * v, s_);
+  ops::d2d(dGhh_, Ghh, G * o * o, s_);
+  if (!ccd) {
+    {  // dGpp[G][a][c] -= sum_l t[a][l] Gph[G][c][l]
+      Contraction c; c.M = v; c.N = v; c.K = o; c.batch = G;
+      c.A = rm(t, o); c.B = with_batch(tr(Gph, o), n1); c.C = with_batch(rm(dGpp_, v), v * v);
+      c.alpha = -1.0; c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // dGhh[G][k][i] += sum_d Gph[G][d][k] t[d][i]
+      Contraction c; c.M = o; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(tr(Gph, o), n1); c.B = rm(t, o); c.C = with_batch(rm(dGhh_, o), o * o);
+      c.beta = 1.0;
+      gemm_(c);
+    }
+  }
+  {  // EX = -1/2 T^x Ve
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(Te_, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
+    gemm_(c);
+  }
+  {  // EX[a][i][c][k] += sum_G dGpp[G][a][c] dGhh[G][k][i]      (m = (a,c), n = (k,i))
+    Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
+    c.A = vw(dGpp_, v, 1, 0, v * v);
+    c.B = vw(dGhh_, 0, o * o, o, 1);
+    c.C = vw(EX_, o * n1, o, 1, n1);
+    c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // R2 -= EX T
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(EX_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1);
+    c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // R2_abij -= sum_ck T_ackj X_bkci : exchange pairing m = (a,j), n = (b,i)
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
+    c.A = vw(Te_, o * n1, n1, 0, 1);
+    c.B = vw(EX_, 0, 1, o * n1, n1);
+    c.C = vw(R2, o * n1, 1, o, n1);
+    c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  // ---- P(ab,ij) symmetrisation and +V (Ccsd.cxx:256,263) ----------------------
+  ops::symmetrize(R2, n1, s_);
+  ops::axpby(R2, 1.0, R2, 1.0, Vd_, 0.0, D2, s_);
+  // ---- hole-hole ladder (Ccsd.cxx:267-281) --------------------------------------
+  ops::d2d(Xkl1_, Vhhhh_, o * o * o * o, s_);
+  if (!ccd) {
+    {  // Xkl1[k][l][i][j] += sum_c Vhhhp[k][l][i][c] t[c][j]
+      Contraction c; c.M = o * o * o; c.N = o; c.K = v;
+      c.A = rm(Vhhhp_, v); c.B = rm(t, o); c.C = rm(Xkl1_, o); c.beta = 1.0;
+      gemm_(c);
+    }
+    {  // Xkl1[k][l][i][j] += sum_c Vhhhp[l][k][j][c] t[c][i]     (batch l, m = (k,j))
+      Contraction c; c.M = o * o; c.N = o; c.K = v; c.batch = o; c.Mi = o;
+      c.A = vw(Vhhhp_, o * v, v, 0, 1, 0, o * o * v);
+      c.B = rm(t, o);
+      c.C = vw(Xkl1_, o * o * o, 1, 0, o, 0, o * o);
+      c.beta = 1.0;
+      gemm_(c);
+    }
+  }
+  ops::permute4(Tp_, Td, d4, p_pp, 1.0, 0.0, s_);
+  {  // Xkl2[kl][ij] = sum_cd V_cdkl X_cdij
+    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
+    c.A = tr(Vp_, o * o); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
+    gemm_(c);
+  }
+  {  // R2 += Xkl1 X_abkl  (m = (a,b), n = (i,j))
+    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
+    c.A = vw(Xp_, v * o * o, o * o, 0, 1);
+    c.B = vw(Xkl1_, 0, o * o, o, 1);
+    c.C = vw(R2, o * n1, o, n1, 1);
+    c.beta = 1.0;
+    gemm_(c);
+    c.A.p = opt_.ppl ? Tp_ : Xp_;
+    c.B.p = Xkl2_;
+    gemm_(c);
+  }
+  // ---- particle-particle ladder (Ccsd.cxx:283-333) ------------------------------
+  if (opt_.ppl) ppl(Xp_, R2, dGpp_);
+  if (ccd) {
+    ops::zero(R1, n1, s_);
+    return;
+  }
+  // ---- singles (Ccsd.cxx:339-375) ------------------------------------------------
+  {
+    Contraction c; c.M = v; c.N = o; c.K = v;
+    c.A = rm(Kac_, v); c.B = rm(t, o); c.C = rm(R1, o);
+    gemm_(c);
+  }
+  {
+    Contraction c; c.M = v; c.N = o; c.K = o;
+    c.A = rm(t, o); c.B = rm(Kki_, o); c.C = rm(R1, o); c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // kck = 2 Vd t - Ve t
+    Contraction c; c.M = n1; c.N = 1; c.K = n1;
+    c.A = rm(Vd_, n1); c.B = vw(t, 0, 1, 0, 0); c.C = vw(kck_, 0, 1, 0, 0); c.alpha = 2.0;
+    gemm_(c);
+    c.A = rm(Ve_, n1); c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // R1 += (2T - T^x) kck
+    Contraction c; c.M = n1; c.N = 1; c.K = n1;
+    c.A = rm(Y_, n1); c.B = vw(kck_, 0, 1, 0, 0); c.C = vw(R1, 0, 1, 0, 0); c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // P1[k][i] = sum_c kck[c][k] t[c][i];  R1 += t P1
+    Contraction c; c.M = o; c.N = o; c.K = v;
+    c.A = tr(kck_, o); c.B = rm(t, o); c.C = rm(P1_, o);
+    gemm_(c);
+    Contraction d; d.M = v; d.N = o; d.K = o;
+    d.A = rm(t, o); d.B = rm(P1_, o); d.C = rm(R1, o); d.beta = 1.0;
+    gemm_(d);
+  }
+  {  // R1 += 2 Vd t
+    Contraction c; c.M = n1; c.N = 1; c.K = n1;
+    c.A = rm(Vd_, n1); c.B = vw(t, 0, 1, 0, 0); c.C = vw(R1, 0, 1, 0, 0);
+    c.alpha = 2.0; c.beta = 1.0;
+    gemm_(c);
+  }
+  {  // P[G][i][c] = sum_k Ghh[G][i][k] t[c][k];  R1[a][i] -= sum_{G,c} Gpp[G][c][a] P[G][i][c]
+    Contraction c; c.M = o; c.N = v; c.K = o; c.batch = G;
+    c.A = with_batch(rm(Ghh, o), o * o); c.B = tr(t, o); c.C = with_batch(rm(P_, v), o * v);
+    gemm_(c);
+    Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
+    d.A = vw(Gpp, 0, 1, v * v, v);
+    d.B = vw(P_, o * v, 1, 0, v);
+    d.C = rm(R1, o);
+    d.alpha = -1.0; d.beta = 1.0;
+    gemm_(d);
+  }
+  {  // F = Gph (2X - X^x);  R1[a][i] += sum_{G,x} Gpp[G][x][a] F[G][x][i]
+    ops::permute4(W8_, Xd_, d4, p_ex, 1.0, 0.0, s_);
+    ops::axpby(W8_, 2.0, Xd_, -1.0, W8_, 0.0, D2, s_);
+    Contraction c; c.M = G; c.N = n1; c.K = n1;
+    c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(F_, n1);
+    gemm_(c);
+    Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
+    d.A = vw(Gpp, 0, 1, v * v, v);
+    d.B = vw(F_, n1, o, 0, 1);
+    d.C = rm(R1, o);
+    d.beta = 1.0;
+    gemm_(d);
+  }
+  {  // R1[a][i] -= sum_{ckl} Xp[a][c][k][l] Vh2[i][c][k][l]
+    Contraction c; c.M = v; c.N = o; c.K = v * o * o;
+    c.A = rm(Xp_, v * o * o); c.B = tr(Vh2_, v * o * o); c.C = rm(R1, o);
+    c.alpha = -1.0; c.beta = 1.0;
+    gemm_(c);
+  }
+}
+
+// Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of size s,
+//   V[x][y][c][d] = sum_G dGpp[G][x0+x][c] dGpp[G][y0+y][d]          (GEMM, K = G)
+//   R_{x y i j} += sum_cd V[x][y][c][d] X_cdij, mirrored into R_{y x j i} (GEMM, K = v^2)
+void CcsdReal::ppl(const double* Xp, double* R2, const double* dGpp) {
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o;
+  const int64_t s = slab_rows_;
+  const int64_t nb = (v + s - 1) / s;
+  for (int64_t X = 0; X < nb; ++X) {
+    for (int64_t Yb = 0; Yb <= X; ++Yb) {
+      const int64_t x0 = X * s, sx = std::min(s, v - x0);
+      const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
+      {
+        Contraction c; c.M = sx * v; c.N = sy * v; c.K = G; c.Mi = v; c.Ni = v;
+        c.A = vw(cp(dGpp) + x0 * v, v, 1, 0, v * v);
+        c.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
+        c.C = vw(slab_, sy * v * v, v, v * v, 1);
+        gemm_(c);
+      }
+      {
+        Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
+        c.A = vw(slab_, sy * v * v, v * v, 0, 1);
+        c.B = vw(cp(Xp), 0, o * o, o, 1);
+        c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
+        if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
+        c.beta = 1.0;
+        gemm_(c);
+      }
+    }
+  }
+}
+
+}  // namespace cc4s_b200

@@ -1,0 +1,147 @@
+// CoupledCluster iteration driver and C ABI (include/cc4s_cc.h).
+//
+// Host-side restatement of CoupledCluster::run (CoupledCluster.cxx:56-191) and
+// of the mixers (DiisMixer.cxx:59-107, LinearMixer.cxx:44-61).  Amplitudes,
+// residual, DIIS history, overlap matrix and coefficients stay on the device;
+// per iteration only the energy and the residual norm (5 doubles) and the
+// DIIS status come back to the host for the convergence test.
+#include "driver.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace cc4s_b200 {
+
+Handle::Handle(const cc4s_cc_options& o) : opt(o) {
+  if (opt.method != CC4S_METHOD_CCSD && opt.method != CC4S_METHOD_CCD)
+    throw Error(ERR_INVALID_ARGUMENT, "Unknown method");
+  if (opt.mixer != CC4S_MIXER_DIIS && opt.mixer != CC4S_MIXER_LINEAR)
+    throw Error(ERR_INVALID_ARGUMENT, "Unknown mixer type");
+  if (opt.mixer == CC4S_MIXER_DIIS && (opt.max_residua < 1 || opt.max_residua > 8))
+    throw Error(ERR_UNSUPPORTED, "maxResidua must be in [1, 8]");
+  if (opt.precision != CC4S_PRECISION_FP64)
+    throw Error(ERR_UNSUPPORTED, "only the FP64 form is available in this build");
+  if (opt.max_iterations < 0) throw Error(ERR_INVALID_ARGUMENT, "maxIterations < 0");
+  stream = ops::stream_create(opt.device);
+  ev0 = ops::event_create();
+  ev1 = ops::event_create();
+}
+
+Handle::~Handle() {
+  free_state();
+  for (double* p : vertex) ops::release(p);
+  ops::event_destroy(ev0);
+  ops::event_destroy(ev1);
+  ops::stream_destroy(stream);
+}
+
+double* Handle::take(size_t elems) {
+  double* p = ops::alloc(elems);
+  state.push_back(p);
+  return p;
+}
+
+void Handle::free_state() {
+  solver.reset();
+  for (double* p : state) ops::release(p);
+  state.clear();
+  A.clear(); Rs.clear();
+  Tcur = Rbuf = dTlast = scal = ws = B = coef = nullptr;
+  status_dev = nullptr;
+  have_T = false;
+}
+
+void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, int64_t Nv,
+                        const double* gamma, int64_t NG, bool is_complex, bool half_grid) {
+  if (!eps_h || !eps_p || !gamma) throw Error(ERR_INVALID_ARGUMENT, "null input");
+  if (No <= 0 || Nv <= 0 || NG <= 0) throw Error(ERR_BAD_SHAPE, "No, Nv, NG must be positive");
+  const int64_t Np = No + Nv;
+  const int64_t nin = NG * Np * Np * (is_complex ? 2 : 1);
+  for (int64_t k = 0; k < No; ++k)
+    if (!std::isfinite(eps_h[k])) throw Error(ERR_NON_FINITE, "non-finite eps_h");
+  for (int64_t k = 0; k < Nv; ++k)
+    if (!std::isfinite(eps_p[k])) throw Error(ERR_NON_FINITE, "non-finite eps_p");
+  bool has_imag = false;
+  for (int64_t k = 0; k < nin; ++k) {
+    if (!std::isfinite(gamma[k])) throw Error(ERR_NON_FINITE, "non-finite Coulomb vertex");
+    if (is_complex && (k & 1) && gamma[k] != 0.0) has_imag = true;
+  }
+  if (!half_grid)
+    throw Error(ERR_UNSUPPORTED, "the complex integral path is not available in this build");
+  free_state();
+  for (double* p : vertex) ops::release(p);
+  vertex.clear();
+  // Real path: stack Re and (if present) Im rows into one real auxiliary index.
+  const int64_t parts = has_imag ? 2 : 1;
+  const int64_t G = NG * parts;
+  auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
+  RealSystem rs;
+  rs.o = No; rs.v = Nv; rs.G = G;
+  rs.eh = vtake(No); rs.ep = vtake(Nv);
+  rs.Gpp = vtake(G * Nv * Nv); rs.Gph = vtake(G * Nv * No);
+  rs.Ghh = vtake(G * No * No); rs.Ghp = vtake(G * No * Nv);
+  ops::h2d(rs.eh, eps_h, No, stream);
+  ops::h2d(rs.ep, eps_p, Nv, stream);
+  {
+    double* staging = ops::alloc(nin);
+    try {
+      ops::h2d(staging, gamma, nin, stream);
+      for (int64_t part = 0; part < parts; ++part) {
+        const int64_t off = part * NG;
+        ops::gather_vertex(rs.Gpp + off * Nv * Nv, staging, is_complex, (int)part, NG, Np, No, Nv, No, Nv, stream);
+        ops::gather_vertex(rs.Gph + off * Nv * No, staging, is_complex, (int)part, NG, Np, No, Nv, 0, No, stream);
+        ops::gather_vertex(rs.Ghh + off * No * No, staging, is_complex, (int)part, NG, Np, 0, No, 0, No, stream);
+        ops::gather_vertex(rs.Ghp + off * No * Nv, staging, is_complex, (int)part, NG, Np, 0, No, No, Nv, stream);
+      }
+      ops::sync(stream);
+    } catch (...) {
+      ops::release(staging);
+      throw;
+    }
+    ops::release(staging);
+  }
+  sys = rs;
+  shape = ops::AmpShape{No, Nv, 1};
+  complex_path = false;
+  allocate_state();
+}
+
+void Handle::allocate_state() {
+  RealOptions ro;
+  ro.ccd = opt.method == CC4S_METHOD_CCD;
+  ro.ppl = opt.ppl != 0;
+  solver.reset(new CcsdReal(sys, ro, stream));
+  const int64_t n = shape.total();
+  Tcur = take(n);
+  Rbuf = take(n);
+  const int N = opt.mixer == CC4S_MIXER_DIIS ? opt.max_residua : 1;
+  for (int k = 0; k < N; ++k) { A.push_back(take(n)); Rs.push_back(take(n)); }
+  if (opt.mixer == CC4S_MIXER_LINEAR) dTlast = take(n);
+  scal = take(64);
+  ws = take(4096 * 8);
+  B = take((N + 1) * (N + 1));
+  coef = take(32);
+  status_dev = reinterpret_cast<int*>(take(4));
+  reset_mixer();
+  ops::sync(stream);
+}
+
+void Handle::reset_mixer() {
+  const int N = static_cast<int>(A.size());
+  std::vector<double> b((N + 1) * (N + 1), 0.0);
+  for (int i = 1; i <= N; ++i) { b[i] = -1.0; b[i * (N + 1)] = -1.0; }
+  ops::h2d(B, b.data(), b.size(), stream);
+  valid.assign(N, 0);
+  next_index = 0;
+  count = 0;
+  linear_has_last = false;
+}
+
+void Handle::require_inputs() const {
+  if (!solver) throw Error(ERR_STATE, "inputs not set");
+}
+
+}  // namespace cc4s_b200

@@ -1,0 +1,64 @@
+// State behind one cc4s_cc_handle.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/cc4s_cc.h"
+#include "ccsd_real.h"
+#include "ops.h"
+
+namespace cc4s_b200 {
+
+struct Handle {
+  explicit Handle(const cc4s_cc_options& o);
+  ~Handle();
+
+  void set_inputs(const double* eps_h, int64_t No, const double* eps_p, int64_t Nv,
+                  const double* gamma, int64_t NG, bool is_complex, bool half_grid);
+  void set_initial(const double* T1, const double* T2);
+  int run(cc4s_cc_result* out);
+  void get_amplitudes(double* T1, double* T2);
+  void residual(const double* T1, const double* T2, double* R1, double* R2);
+
+  // helpers
+  double* take(size_t elems);
+  void free_state();
+  void allocate_state();
+  void reset_mixer();
+  void require_inputs() const;
+  void upload_amplitudes(double* dst, const double* T1, const double* T2);
+  void download_amplitudes(const double* src, double* T1, double* T2);
+  void mix(double* A_new, double* dT_new, double* norm2_dev);
+
+  cc4s_cc_options opt;
+  Stream stream = nullptr;
+  void* ev0 = nullptr;
+  void* ev1 = nullptr;
+  std::string error;
+
+  RealSystem sys;
+  ops::AmpShape shape{0, 0, 1};
+  bool complex_path = false;
+  std::vector<double*> vertex;  // device inputs (vertex slices, energies)
+  std::vector<double*> state;   // amplitudes, DIIS history, scalars
+  std::unique_ptr<CcsdReal> solver;
+
+  double* Tcur = nullptr;   // current amplitudes (mixer output)
+  double* Rbuf = nullptr;   // residual
+  double* dTlast = nullptr; // linear mixer: last change
+  std::vector<double*> A;   // DIIS amplitude slots
+  std::vector<double*> Rs;  // DIIS change slots
+  double* scal = nullptr;   // [0..3] energy, [4] norm^2, [8..] dots
+  double* ws = nullptr;     // reduction partials
+  double* B = nullptr;      // DIIS bordered overlap matrix
+  double* coef = nullptr;   // DIIS coefficients
+  int* status_dev = nullptr;
+  std::vector<int> valid;
+  int next_index = 0, count = 0;
+  bool linear_has_last = false;
+  bool have_T = false;
+};
+
+}  // namespace cc4s_b200

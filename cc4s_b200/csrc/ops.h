@@ -1,0 +1,99 @@
+// Device operations used by the CoupledCluster schedule.
+//
+// The CCSD schedule (ccsd_real.cpp) and the iteration driver (driver.cpp) are
+// written against this interface only.  The product library implements it with
+// CUDA kernels for sm_100a (ops_cuda.cu, gemm_f64.cu).
+#pragma once
+
+#include "gemm_f64.cuh"
+
+namespace cc4s_b200 {
+
+using Stream = cudaStream_t;
+
+namespace ops {
+
+// ---- memory ---------------------------------------------------------------
+double* alloc(size_t elems);  // throws Error(ERR_OUT_OF_MEMORY) on failure
+void release(void* p);
+void zero(double* p, size_t elems, Stream s);
+void h2d(double* dst, const double* src, size_t elems, Stream s);
+void d2h(double* dst, const double* src, size_t elems, Stream s);
+void d2d(double* dst, const double* src, size_t elems, Stream s);
+void sync(Stream s);
+Stream stream_create(int device);
+void stream_destroy(Stream s);
+void* event_create();
+void event_record(void* e, Stream s);
+float event_ms(void* start, void* stop);  // synchronises on stop
+void event_destroy(void* e);
+
+// ---- bandwidth kernels ----------------------------------------------------
+// dst = alpha * permute(src) + beta * dst.  src is row-major with dims d[0..3];
+// destination axis k is source axis perm[k].
+void permute4(double* dst, const double* src, const int64_t d[4], const int perm[4],
+              double alpha, double beta, Stream s);
+// out = a*x + b*y + c*out   (y may be null; c == 0 does not read out)
+void axpby(double* out, double a, const double* x, double b, const double* y, double c,
+           int64_t n, Stream s);
+// out[r][c] = a*A[r][c] + b*t[r]*t[c] for an n x n matrix (A may alias out).
+void rank1(double* out, double a, const double* A, double b, const double* t, int64_t n,
+           Stream s);
+// R <- R + R^T for an n x n matrix, in place.
+void symmetrize(double* R, int64_t n, Stream s);
+
+// Gathers one block of the input Coulomb vertex into a row-major [NG][nx][ny] array:
+//   out[g][x][y] = part(Gamma(g, row0 + x, col0 + y)),
+// where the input is column-major Gamma[NG][Np][Np] (G fastest), real (part 0 only)
+// or complex interleaved (part 0 = real, 1 = imaginary).
+void gather_vertex(double* out, const double* in, bool in_complex, int part, int64_t NG,
+                   int64_t Np, int64_t row0, int64_t nx, int64_t col0, int64_t ny, Stream s);
+
+// Amplitude vectors: [T1 (v x o, row-major [a][i]) | T2 ((v o) x (v o), row-major [a][i][b][j])],
+// repeated once per plane (real plane, then imaginary plane for complex systems).
+struct AmpShape {
+  int64_t o, v, planes;
+  int64_t n1() const { return v * o; }
+  int64_t plane() const { return v * o + (v * o) * (v * o); }
+  int64_t total() const { return plane() * planes; }
+};
+
+// Jacobi update of CoupledCluster::residuumToAmplitudes:
+//   Tnew = -(R - shift*Told) / (D + shift),  dT = Tnew - Told   (Told may be null)
+// with D_ai = ep[a]-eh[i], D_abij = ep[a]+ep[b]-eh[i]-eh[j].
+void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const double* eh,
+            const double* ep, const AmpShape& sh, double shift, Stream s);
+
+// Correlation energy of amplitudes T (AmpShape layout) with the pair-layout integrals
+// Vd[(a,i),(b,j)] = V_abij and Ve[(a,i),(b,j)] = V_abji (real and optional imaginary planes).
+// Writes 4 doubles to out_dev: Re(direct), Re(exchange), Im(direct), Im(exchange).
+void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
+            const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s);
+
+// out_dev[k] = sum_e x[e] * ys[k][e] for k < ny (ny <= 8), deterministic order.
+void dots(const double* x, const double* const* ys, int ny, int64_t n, double* out_dev,
+          double* ws, Stream s);
+
+// DIIS (DiisMixer.cxx:59-107) on the device:
+//   B (device, (N+1)^2, row-major) receives the new overlaps 2*dots[i] at
+//   (i+1, next+1) and (next+1, i+1) for the valid slots listed in valid[];
+//   the (count+1)^2 corner is solved for rhs (-1, 0, ...) and coef_dev[j]
+//   receives the coefficient of slot (next + N - j) % N, j < count.
+//   status_dev[0] = 0 on success, 1 if the system is singular.
+void diis_solve(double* B, const double* dots_dev, const int* valid_host, int N, int next,
+                int count, double* coef_dev, int* status_dev, Stream s);
+
+// out = sum_j coef[j] * xs[j]; if ys != null also norm2_out = |sum_j coef[j] ys[j]|^2
+// (written to norm2_dev).  Coefficients are read from device memory.
+void lincomb(double* out, const double* const* xs, const double* const* ys,
+             const double* coef_dev, int nx, int64_t n, double* norm2_dev, double* ws,
+             Stream s);
+
+// Small host-visible scalars.
+void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, Stream s);
+
+// Number of bandwidth-kernel launches issued so far.
+uint64_t launch_count();
+
+}  // namespace ops
+}  // namespace cc4s_b200

@@ -1,0 +1,583 @@
+// Bandwidth kernels of the CoupledCluster step (sm_100a).
+//
+// All kernels are grid-stride loops sized in multiples of the 148 SMs, with
+// coalesced 64-bit accesses; transposing permutations stage 32 x 32 tiles in
+// shared memory.  Reductions are two-pass and deterministic: each block writes
+// a partial sum (warp shuffles + shared memory), a single block then adds the
+// partials in a fixed order.
+#include "ops.h"
+
+#include <atomic>
+#include <cmath>
+
+namespace cc4s_b200 {
+namespace ops {
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+inline void count() { g_launches.fetch_add(1); }
+constexpr int RED_BLOCKS = 148 * 4;  // partial sums per reduction
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of NV values; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+  __shared__ double sh[NV][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[k][w] = v[k];
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double x = lane < nw ? sh[k][lane] : 0.0;
+      v[k] = warp_sum(x);
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+struct Perm4 {
+  int64_t e[4];   // destination dims
+  int64_t ss[4];  // source stride of destination axis k
+  int64_t ds[4];  // destination strides
+};
+
+// Destination inner axis is the source inner axis: straight copy of rows.
+__global__ void permute_rows_kernel(double* dst, const double* src, Perm4 p, double alpha,
+                                    double beta) {
+  const int64_t rows = p.e[0] * p.e[1] * p.e[2];
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int64_t i2 = r % p.e[2];
+    const int64_t i1 = (r / p.e[2]) % p.e[1];
+    const int64_t i0 = r / (p.e[2] * p.e[1]);
+    const double* s = src + i0 * p.ss[0] + i1 * p.ss[1] + i2 * p.ss[2];
+    double* d = dst + r * p.e[3];
+    for (int64_t x = threadIdx.x; x < p.e[3]; x += blockDim.x) {
+      const double v = alpha * s[x];
+      d[x] = (beta != 0.0) ? v + beta * d[x] : v;
+    }
+  }
+}
+
+// General permutation: tile over (destination inner axis 3, destination axis q that
+// holds the source inner axis); the other two destination axes form the batch.
+__global__ void permute_tiled_kernel(double* dst, const double* src, Perm4 p, int q, int b0,
+                                     int b1, double alpha, double beta) {
+  __shared__ double tile[32][33];
+  const int64_t nx = p.e[3], ny = p.e[q];
+  const int64_t tx = (nx + 31) / 32, ty = (ny + 31) / 32;
+  const int64_t nb = p.e[b0] * p.e[b1];
+  const int64_t total = tx * ty * nb;
+  for (int64_t blk = blockIdx.x; blk < total; blk += gridDim.x) {
+    const int64_t bx = blk % tx;
+    const int64_t by = (blk / tx) % ty;
+    const int64_t bb = blk / (tx * ty);
+    const int64_t ib1 = bb % p.e[b1], ib0 = bb / p.e[b1];
+    const int64_t sbase = ib0 * p.ss[b0] + ib1 * p.ss[b1];
+    const int64_t dbase = ib0 * p.ds[b0] + ib1 * p.ds[b1];
+    // Read: source inner axis (= destination axis q) is contiguous; lanes along y.
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t x = bx * 32 + r, y = by * 32 + threadIdx.x;
+      if (x < nx && y < ny) tile[r][threadIdx.x] = src[sbase + x * p.ss[3] + y * p.ss[q]];
+    }
+    __syncthreads();
+    // Write: destination axis 3 contiguous; lanes along x.
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t y = by * 32 + r, x = bx * 32 + threadIdx.x;
+      if (x < nx && y < ny) {
+        double* d = dst + dbase + y * p.ds[q] + x;
+        const double v = alpha * tile[threadIdx.x][r];
+        *d = (beta != 0.0) ? v + beta * *d : v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void axpby_kernel(double* out, double a, const double* x, double b,
+                             const double* y, double c, int64_t n) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double v = a * x[e];
+    if (y) v += b * y[e];
+    if (c != 0.0) v += c * out[e];
+    out[e] = v;
+  }
+}
+
+__global__ void rank1_kernel(double* out, double a, const double* A, double b, const double* t,
+                             int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n, c = e - (e / n) * n;
+    out[e] = a * A[e] + b * t[r] * t[c];
+  }
+}
+
+// R <- R + R^T on 32 x 32 tile pairs (I <= J).
+__global__ void symmetrize_kernel(double* R, int64_t n) {
+  __shared__ double t1[32][33];
+  __shared__ double t2[32][33];
+  const int64_t T = (n + 31) / 32;
+  const int64_t pairs = T * (T + 1) / 2;
+  for (int64_t blk = blockIdx.x; blk < pairs; blk += gridDim.x) {
+    // Map blk -> (I, J), I <= J, row-major over the upper triangle.
+    int64_t I = static_cast<int64_t>((2.0 * T + 1.0 - sqrt((2.0 * T + 1.0) * (2.0 * T + 1.0) - 8.0 * blk)) / 2.0);
+    if (I < 0) I = 0;
+    while (I > 0 && I * T - I * (I - 1) / 2 > blk) --I;
+    while ((I + 1) * T - (I + 1) * I / 2 <= blk) ++I;
+    const int64_t J = I + (blk - (I * T - I * (I - 1) / 2));
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t rr = I * 32 + r, cc = J * 32 + threadIdx.x;
+      t1[r][threadIdx.x] = (rr < n && cc < n) ? R[rr * n + cc] : 0.0;
+      const int64_t rr2 = J * 32 + r, cc2 = I * 32 + threadIdx.x;
+      t2[r][threadIdx.x] = (rr2 < n && cc2 < n) ? R[rr2 * n + cc2] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t rr = I * 32 + r, cc = J * 32 + threadIdx.x;
+      // element (rr, cc) of block (I,J) pairs with element (cc, rr) of block (J,I)
+      const double s = t1[r][threadIdx.x] + t2[threadIdx.x][r];
+      if (rr < n && cc < n) R[rr * n + cc] = s;
+      const int64_t rr2 = J * 32 + r, cc2 = I * 32 + threadIdx.x;
+      const double s2 = t2[r][threadIdx.x] + t1[threadIdx.x][r];
+      if (I != J && rr2 < n && cc2 < n) R[rr2 * n + cc2] = s2;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void gather_vertex_kernel(double* out, const double* in, int cplx, int part,
+                                     int64_t NG, int64_t Np, int64_t row0, int64_t nx,
+                                     int64_t col0, int64_t ny) {
+  __shared__ double tile[32][33];
+  const int64_t tg = (NG + 31) / 32, tyn = (ny + 31) / 32;
+  const int64_t total = tg * tyn * nx;
+  const int64_t es = cplx ? 2 : 1;
+  for (int64_t blk = blockIdx.x; blk < total; blk += gridDim.x) {
+    const int64_t bg = blk % tg;
+    const int64_t by = (blk / tg) % tyn;
+    const int64_t x = blk / (tg * tyn);
+    const int64_t p = row0 + x;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t y = by * 32 + r, g = bg * 32 + threadIdx.x;
+      if (y < ny && g < NG) {
+        const int64_t q = col0 + y;
+        tile[r][threadIdx.x] = in[(g + NG * (p + Np * q)) * es + part];
+      }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t g = bg * 32 + r, y = by * 32 + threadIdx.x;
+      if (y < ny && g < NG) out[(g * nx + x) * ny + y] = tile[threadIdx.x][r];
+    }
+    __syncthreads();
+  }
+}
+
+struct JacobiArgs {
+  double* Tnew; double* dT; const double* R; const double* Told;
+  const double* eh; const double* ep;
+  int64_t o, v, plane, total;
+  double shift;
+};
+
+__global__ void jacobi_kernel(JacobiArgs a) {
+  const int64_t n1 = a.v * a.o;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q = e % a.plane;
+    double D;
+    if (q < n1) {
+      const int64_t ai = q;
+      D = a.ep[ai / a.o] - a.eh[ai % a.o];
+    } else {
+      const int64_t r = q - n1;
+      const int64_t ai = r / n1, bj = r - (r / n1) * n1;
+      D = a.ep[ai / a.o] - a.eh[ai % a.o] + a.ep[bj / a.o] - a.eh[bj % a.o];
+    }
+    double rv = a.R[e];
+    const double told = a.Told ? a.Told[e] : 0.0;
+    if (a.Told && a.shift != 0.0) rv -= a.shift * told;
+    const double tn = rv * (-1.0 / (D + a.shift));
+    a.Tnew[e] = tn;
+    a.dT[e] = a.Told ? tn - told : tn;
+  }
+}
+
+struct EnergyArgs {
+  const double* T; const double* Vdr; const double* Vdi; const double* Ver; const double* Vei;
+  int64_t o, v, plane;
+  int planes;
+  double* ws;
+};
+
+__global__ void energy_kernel(EnergyArgs a) {
+  const int64_t n1 = a.v * a.o;
+  const int64_t n2 = n1 * n1;
+  const double* t1r = a.T;
+  const double* t2r = a.T + n1;
+  const double* t1i = a.planes > 1 ? a.T + a.plane : nullptr;
+  const double* t2i = a.planes > 1 ? a.T + a.plane + n1 : nullptr;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n2;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n1, c = e - (e / n1) * n1;
+    if (!t1i) {
+      const double x = t2r[e] + t1r[r] * t1r[c];
+      acc[0] += x * a.Vdr[e];
+      acc[1] += x * a.Ver[e];
+    } else {
+      // X = T2 + T1 T1 (complex);  X * conj(V)
+      const double xr = t2r[e] + t1r[r] * t1r[c] - t1i[r] * t1i[c];
+      const double xi = t2i[e] + t1r[r] * t1i[c] + t1i[r] * t1r[c];
+      const double vdr = a.Vdr[e], vdi = a.Vdi ? a.Vdi[e] : 0.0;
+      const double ver = a.Ver[e], vei = a.Vei ? a.Vei[e] : 0.0;
+      acc[0] += xr * vdr + xi * vdi;
+      acc[1] += xr * ver + xi * vei;
+      acc[2] += xi * vdr - xr * vdi;
+      acc[3] += xi * ver - xr * vei;
+    }
+  }
+  block_sum<4>(acc);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) a.ws[blockIdx.x * 4 + k] = acc[k];
+}
+
+// Fixed-order sum of per-block partials: dst[k] = scale[k] * sum_b ws[b*nvals + k].
+__global__ void finish_kernel(double* dst, const double* ws, int nparts, int nvals,
+                              double s0, double s1, double s2, double s3) {
+  const double sc[4] = {s0, s1, s2, s3};
+  for (int k = 0; k < nvals; ++k) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) v += ws[b * nvals + k];
+    double arr[1] = {v};
+    block_sum<1>(arr);
+    if (threadIdx.x == 0) dst[k] = (k < 4 ? sc[k] : 1.0) * arr[0];
+    __syncthreads();
+  }
+}
+
+struct DotArgs {
+  const double* x;
+  const double* y[8];
+  int ny;
+  int64_t n;
+  double* ws;
+};
+
+__global__ void dots_kernel(DotArgs a) {
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double xv = a.x[e];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k < a.ny) acc[k] += xv * a.y[k][e];
+  }
+  block_sum<8>(acc);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < a.ny; ++k) a.ws[blockIdx.x * a.ny + k] = acc[k];
+}
+
+struct LinArgs {
+  double* out;
+  const double* x[16];
+  const double* y[16];
+  const double* coef;
+  int nx;
+  int64_t n;
+  double* ws;
+};
+
+__global__ void lincomb_kernel(LinArgs a) {
+  double c[16];
+  for (int k = 0; k < 16; ++k) c[k] = k < a.nx ? a.coef[k] : 0.0;
+  double nrm[1] = {0.0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double v = 0.0, w = 0.0;
+    for (int k = 0; k < a.nx; ++k) {
+      v += c[k] * a.x[k][e];
+      if (a.y[0]) w += c[k] * a.y[k][e];
+    }
+    a.out[e] = v;
+    nrm[0] += w * w;
+  }
+  if (a.ws) {
+    block_sum<1>(nrm);
+    if (threadIdx.x == 0) a.ws[blockIdx.x] = nrm[0];
+  }
+}
+
+struct DiisArgs {
+  double* B;
+  const double* dots;
+  int valid[16];
+  int N, next, count;
+  double* coef;
+  int* status;
+};
+
+// Single-thread bordered DIIS solve with partial-pivoting LU (dim <= 17).
+__global__ void diis_solve_kernel(DiisArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int M = a.N + 1;
+  int di = 0;
+  for (int i = 0; i < a.N; ++i) {
+    if (!a.valid[i]) continue;
+    const double ov = 2.0 * a.dots[di++];
+    a.B[(i + 1) * M + (a.next + 1)] = ov;
+    a.B[(a.next + 1) * M + (i + 1)] = ov;
+  }
+  const int dim = a.count + 1;
+  double m[17][17];
+  double x[17];
+  for (int r = 0; r < dim; ++r) {
+    for (int c = 0; c < dim; ++c) m[r][c] = a.B[r * M + c];
+    x[r] = r == 0 ? -1.0 : 0.0;
+  }
+  int singular = 0;
+  for (int k = 0; k < dim; ++k) {
+    int piv = k;
+    double best = fabs(m[k][k]);
+    for (int r = k + 1; r < dim; ++r)
+      if (fabs(m[r][k]) > best) { best = fabs(m[r][k]); piv = r; }
+    if (best == 0.0 || !isfinite(best)) { singular = 1; break; }
+    if (piv != k) {
+      for (int c = 0; c < dim; ++c) { double t = m[k][c]; m[k][c] = m[piv][c]; m[piv][c] = t; }
+      double t = x[k]; x[k] = x[piv]; x[piv] = t;
+    }
+    for (int r = k + 1; r < dim; ++r) {
+      const double f = m[r][k] / m[k][k];
+      for (int c = k; c < dim; ++c) m[r][c] -= f * m[k][c];
+      x[r] -= f * x[k];
+    }
+  }
+  if (!singular) {
+    for (int k = dim - 1; k >= 0; --k) {
+      double s = x[k];
+      for (int c = k + 1; c < dim; ++c) s -= m[k][c] * x[c];
+      x[k] = s / m[k][k];
+    }
+    for (int j = 0; j < a.count; ++j) {
+      const int slot = (a.next + a.N - j) % a.N;
+      a.coef[j] = x[slot + 1];
+    }
+  }
+  a.status[0] = singular;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+double* alloc(size_t elems) {
+  void* p = nullptr;
+  if (elems == 0) elems = 1;
+  cudaError_t e = cudaMalloc(&p, elems * sizeof(double));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(elems * 8) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+  }
+  return static_cast<double*>(p);
+}
+void release(void* p) {
+  if (p) cudaFree(p);
+}
+void zero(double* p, size_t elems, Stream s) {
+  CC_CHECK(cudaMemsetAsync(p, 0, elems * sizeof(double), s));
+}
+void h2d(double* d, const double* h, size_t elems, Stream s) {
+  CC_CHECK(cudaMemcpyAsync(d, h, elems * sizeof(double), cudaMemcpyHostToDevice, s));
+}
+void d2h(double* h, const double* d, size_t elems, Stream s) {
+  CC_CHECK(cudaMemcpyAsync(h, d, elems * sizeof(double), cudaMemcpyDeviceToHost, s));
+}
+void d2d(double* d, const double* src, size_t elems, Stream s) {
+  CC_CHECK(cudaMemcpyAsync(d, src, elems * sizeof(double), cudaMemcpyDeviceToDevice, s));
+}
+void sync(Stream s) { CC_CHECK(cudaStreamSynchronize(s)); }
+Stream stream_create(int device) {
+  CC_CHECK(cudaSetDevice(device));
+  cudaStream_t s;
+  CC_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  return s;
+}
+void stream_destroy(Stream s) {
+  if (s) cudaStreamDestroy(s);
+}
+void* event_create() {
+  cudaEvent_t e;
+  CC_CHECK(cudaEventCreate(&e));
+  return e;
+}
+void event_record(void* e, Stream s) { CC_CHECK(cudaEventRecord(static_cast<cudaEvent_t>(e), s)); }
+float event_ms(void* a, void* b) {
+  CC_CHECK(cudaEventSynchronize(static_cast<cudaEvent_t>(b)));
+  float ms = 0.f;
+  CC_CHECK(cudaEventElapsedTime(&ms, static_cast<cudaEvent_t>(a), static_cast<cudaEvent_t>(b)));
+  return ms;
+}
+void event_destroy(void* e) {
+  if (e) cudaEventDestroy(static_cast<cudaEvent_t>(e));
+}
+
+uint64_t launch_count() { return g_launches.load(); }
+
+void permute4(double* dst, const double* src, const int64_t d[4], const int perm[4],
+              double alpha, double beta, Stream s) {
+  int64_t sstr[4];
+  sstr[3] = 1;
+  for (int k = 2; k >= 0; --k) sstr[k] = sstr[k + 1] * d[k + 1];
+  Perm4 p;
+  for (int k = 0; k < 4; ++k) {
+    p.e[k] = d[perm[k]];
+    p.ss[k] = sstr[perm[k]];
+  }
+  p.ds[3] = 1;
+  for (int k = 2; k >= 0; --k) p.ds[k] = p.ds[k + 1] * p.e[k + 1];
+  const int64_t total = p.e[0] * p.e[1] * p.e[2] * p.e[3];
+  if (total == 0) return;
+  if (perm[3] == 3) {
+    const int64_t rows = p.e[0] * p.e[1] * p.e[2];
+    int threads = p.e[3] >= 256 ? 256 : (p.e[3] >= 128 ? 128 : (p.e[3] >= 64 ? 64 : 32));
+    permute_rows_kernel<<<grid_for(rows, 1, 148 * 64), threads, 0, s>>>(dst, src, p, alpha, beta);
+  } else {
+    int q = 0;
+    for (int k = 0; k < 4; ++k)
+      if (perm[k] == 3) q = k;
+    int b[2], nb = 0;
+    for (int k = 0; k < 3; ++k)
+      if (k != q) b[nb++] = k;
+    const int64_t tiles = ((p.e[3] + 31) / 32) * ((p.e[q] + 31) / 32) * p.e[b[0]] * p.e[b[1]];
+    permute_tiled_kernel<<<grid_for(tiles, 1, 148 * 64), dim3(32, 8), 0, s>>>(
+        dst, src, p, q, b[0], b[1], alpha, beta);
+  }
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void axpby(double* out, double a, const double* x, double b, const double* y, double c,
+           int64_t n, Stream s) {
+  if (n <= 0) return;
+  axpby_kernel<<<grid_for(n, 256), 256, 0, s>>>(out, a, x, b, y, c, n);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void rank1(double* out, double a, const double* A, double b, const double* t, int64_t n,
+           Stream s) {
+  if (n <= 0) return;
+  rank1_kernel<<<grid_for(n * n, 256), 256, 0, s>>>(out, a, A, b, t, n);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void symmetrize(double* R, int64_t n, Stream s) {
+  if (n <= 0) return;
+  const int64_t T = (n + 31) / 32;
+  symmetrize_kernel<<<grid_for(T * (T + 1) / 2, 1, 148 * 64), dim3(32, 8), 0, s>>>(R, n);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void gather_vertex(double* out, const double* in, bool in_complex, int part, int64_t NG,
+                   int64_t Np, int64_t row0, int64_t nx, int64_t col0, int64_t ny, Stream s) {
+  if (NG <= 0 || nx <= 0 || ny <= 0) return;
+  const int64_t tiles = ((NG + 31) / 32) * ((ny + 31) / 32) * nx;
+  gather_vertex_kernel<<<grid_for(tiles, 1, 148 * 64), dim3(32, 8), 0, s>>>(
+      out, in, in_complex ? 1 : 0, part, NG, Np, row0, nx, col0, ny);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const double* eh,
+            const double* ep, const AmpShape& sh, double shift, Stream s) {
+  JacobiArgs a{Tnew, dT, R, Told, eh, ep, sh.o, sh.v, sh.plane(), sh.total(), shift};
+  jacobi_kernel<<<grid_for(sh.total(), 256), 256, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, Stream s) {
+  finish_kernel<<<1, 256, 0, s>>>(dst_dev, ws, nparts, nvals, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
+            const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s) {
+  EnergyArgs a{T, Vd_re, Vd_im, Ve_re, Ve_im, sh.o, sh.v, sh.plane(), (int)sh.planes, ws};
+  energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  // direct = 2 * sum X V_ijab, exchange = -sum X V_ijba  (CoupledCluster.cxx:223-232)
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 4, 2.0, -1.0, 2.0, -1.0);
+  CC_LAUNCH_CHECK();
+  count();
+  count();
+}
+
+void dots(const double* x, const double* const* ys, int ny, int64_t n, double* out_dev,
+          double* ws, Stream s) {
+  if (ny <= 0) return;
+  if (ny > 8) throw Error(ERR_UNSUPPORTED, "dots: at most 8 vectors");
+  DotArgs a{};
+  a.x = x; a.ny = ny; a.n = n; a.ws = ws;
+  for (int k = 0; k < ny; ++k) a.y[k] = ys[k];
+  dots_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, ny, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+  count();
+}
+
+void diis_solve(double* B, const double* dots_dev, const int* valid_host, int N, int next,
+                int count_, double* coef_dev, int* status_dev, Stream s) {
+  if (N > 16) throw Error(ERR_UNSUPPORTED, "DIIS: at most 16 residua");
+  DiisArgs a{};
+  a.B = B; a.dots = dots_dev; a.N = N; a.next = next; a.count = count_;
+  a.coef = coef_dev; a.status = status_dev;
+  for (int i = 0; i < N; ++i) a.valid[i] = valid_host[i];
+  diis_solve_kernel<<<1, 32, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void lincomb(double* out, const double* const* xs, const double* const* ys,
+             const double* coef_dev, int nx, int64_t n, double* norm2_dev, double* ws,
+             Stream s) {
+  if (nx > 16) throw Error(ERR_UNSUPPORTED, "lincomb: at most 16 vectors");
+  LinArgs a{};
+  a.out = out; a.coef = coef_dev; a.nx = nx; a.n = n;
+  a.ws = (ys && norm2_dev) ? ws : nullptr;
+  for (int k = 0; k < nx; ++k) {
+    a.x[k] = xs[k];
+    a.y[k] = ys ? ys[k] : nullptr;
+  }
+  lincomb_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+  if (a.ws) {
+    finish_kernel<<<1, 256, 0, s>>>(norm2_dev, ws, RED_BLOCKS, 1, 1.0, 1.0, 1.0, 1.0);
+    CC_LAUNCH_CHECK();
+    count();
+  }
+}
+
+}  // namespace ops
+}  // namespace cc4s_b200

@@ -1,0 +1,149 @@
+/* C ABI of the B200 CoupledCluster step (methods Ccsd and Ccd).
+ *
+ * Drop-in replacement for the cc4s algorithm step
+ *   - name: CoupledCluster
+ *     in:  {method, slicedEigenEnergies, slicedCoulombVertex, coulombIntegrals,
+ *           mixer: {type, maxResidua | ratio}, maxIterations, energyConvergence,
+ *           amplitudesConvergence, levelShift, initialAmplitudes,
+ *           integralsSliceSize, ppl}
+ *     out: {energy: {correlation, direct, exchange, secondOrder, unit},
+ *           convergenceReached, amplitudes: {ph, pphh}}
+ * The reference binds this step through C++ name registries, not a C ABI:
+ *   AlgorithmRegistrar "CoupledCluster"      src/main/algorithms/CoupledCluster.cxx:34-52
+ *   CoupledClusterMethodRegistrar "Ccsd"     src/main/algorithms/coupledcluster/Ccsd.cxx:25-32
+ *   MixerRegistrar "DiisMixer"/"LinearMixer" src/main/mixers/DiisMixer.cxx:25,
+ *                                            src/main/mixers/LinearMixer.cxx:24
+ * Each entry point below states the reference interface it replaces.
+ *
+ * Conventions: every function returns a status (0 = OK).  No C++ exception
+ * crosses this boundary; the message of the last failure is available from
+ * cc4s_cc_last_error.  Host buffers are owned by the caller and copied; device
+ * memory is owned by the handle.  One handle per host thread; each handle
+ * owns one CUDA stream.  Tensors use the reference's column-major layout
+ * (first index fastest): eps[p], T1[a,i] ("ph"), T2[a,b,i,j] ("pphh"),
+ * Gamma[G,p,q] with the No hole states first.  Complex tensors are
+ * interleaved (re, im) doubles.
+ */
+#ifndef CC4S_CC_H
+#define CC4S_CC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CC4S_OK 0
+#define CC4S_ERR_INVALID_ARGUMENT 1
+#define CC4S_ERR_BAD_SHAPE 2
+#define CC4S_ERR_OUT_OF_MEMORY 3
+#define CC4S_WARN_NOT_CONVERGED 4 /* warning: results are valid */
+#define CC4S_ERR_DIIS_SINGULAR 5
+#define CC4S_ERR_CUDA 6
+#define CC4S_ERR_TIMEOUT 7
+#define CC4S_ERR_STATE 8
+#define CC4S_ERR_NON_FINITE 9
+#define CC4S_ERR_UNSUPPORTED 10
+
+#define CC4S_METHOD_CCSD 0
+#define CC4S_METHOD_CCD 1
+
+#define CC4S_PRECISION_FP64 0
+#define CC4S_PRECISION_SPLIT2 2
+#define CC4S_PRECISION_SPLIT3 3
+
+#define CC4S_MIXER_DIIS 0
+#define CC4S_MIXER_LINEAR 1
+
+#define CC4S_MAX_HISTORY 256
+
+typedef struct cc4s_cc_handle cc4s_cc_handle;
+
+/* Options of the CoupledCluster step; defaults as in
+ * src/main/algorithms/CoupledCluster.hpp:45-49 and the mixers. */
+typedef struct {
+  int method;                   /* "method" (default Ccsd), CoupledCluster.cxx:80 */
+  int precision;                /* FP64 (default) or split-precision tensor-core form */
+  int mixer;                    /* "mixer.type", CoupledCluster.cxx:96 */
+  int max_residua;              /* "mixer.maxResidua" (4), DiisMixer.cxx:33 */
+  double ratio;                 /* "mixer.ratio" (1.0), LinearMixer.cxx:32 */
+  int max_iterations;           /* "maxIterations" (16) */
+  double energy_convergence;    /* "energyConvergence" (1e-7) */
+  double amplitudes_convergence;/* "amplitudesConvergence" (1e-6) */
+  double level_shift;           /* "levelShift" (0) */
+  int64_t integrals_slice_size; /* "integralsSliceSize" (0 = No), Ccsd.cxx:287-289 */
+  int ppl;                      /* "ppl" (1), Ccsd.cxx:95 */
+  int device;                   /* CUDA device ordinal */
+} cc4s_cc_options;
+
+typedef struct {
+  double correlation, direct, exchange, second_order; /* energy.* outputs */
+  double correlation_imag;     /* imaginary part of the complex energy */
+  int iterations;              /* iterations performed */
+  int converged;               /* convergenceReached */
+  int history_len;
+  double energy[CC4S_MAX_HISTORY];        /* per iteration: E */
+  double delta_energy[CC4S_MAX_HISTORY];  /* dE */
+  double residuum_norm[CC4S_MAX_HISTORY]; /* dR (DIIS-extrapolated change norm) */
+  double seconds[CC4S_MAX_HISTORY];       /* device time of the iteration */
+  double flops_per_iteration;  /* FP64-equivalent flops of one residual (this schedule) */
+} cc4s_cc_result;
+
+typedef struct {
+  uint64_t gemm_launches;      /* tensor-core contraction kernels launched so far */
+  uint64_t other_launches;     /* bandwidth kernels launched so far */
+  uint64_t device_bytes;       /* device memory held by the handle */
+  double flops_per_residual;   /* FP64-equivalent flops of one residual */
+} cc4s_cc_stats;
+
+/* Fills the defaults of the reference. */
+void cc4s_cc_default_options(cc4s_cc_options* opt);
+
+/* Replaces the construction of CoupledCluster with its method and mixer
+ * (CoupledCluster.cxx:79-103: CoupledClusterMethodFactory::create,
+ * MixerFactory::create). */
+int cc4s_cc_create(const cc4s_cc_options* opt, cc4s_cc_handle** h);
+
+/* Replaces the inputs slicedEigenEnergies {h, p} and slicedCoulombVertex
+ * (CoupledCluster.cxx:59-66, Ccsd.cxx:110-117).  gamma is Gamma[NG, Np, Np]
+ * with Np = No + Nv, holes first (SliceOperator.cxx:95-131).  half_grid
+ * selects the real integral path V = Re*Re + Im*Im
+ * (VertexCoulombIntegrals.cxx:45-52); otherwise V_pqsr = sum conj(G_sp) G_qr.
+ * The coulombIntegrals input is not needed: the integral slices are formed on
+ * the device from gamma. */
+int cc4s_cc_set_inputs(cc4s_cc_handle* h, const double* eps_h, int64_t No,
+                       const double* eps_p, int64_t Nv, const double* gamma, int64_t NG,
+                       int is_complex, int half_grid);
+
+/* Replaces the "initialAmplitudes" input (CoupledCluster.cxx:70-75).
+ * T1[a,i], T2[a,b,i,j] column-major; complex interleaved on the complex path. */
+int cc4s_cc_set_initial_amplitudes(cc4s_cc_handle* h, const double* T1, const double* T2);
+
+/* Replaces CoupledCluster::run<F,TE> (CoupledCluster.cxx:56-191): the iteration
+ * loop, Jacobi update, mixer and energy.  Returns CC4S_WARN_NOT_CONVERGED when
+ * maxIterations is reached (results are still filled in). */
+int cc4s_cc_run(cc4s_cc_handle* h, cc4s_cc_result* out);
+
+/* Replaces the "amplitudes" output (CoupledCluster.cxx:186-190). */
+int cc4s_cc_get_amplitudes(cc4s_cc_handle* h, double* T1, double* T2);
+
+/* One residual evaluation, Ccsd::getResiduum (Ccsd.cxx:77-378 / 382-633),
+ * on caller amplitudes (T1 == T2 == NULL: first iteration).  Outputs R1[a,i],
+ * R2[a,b,i,j] column-major. */
+int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, double* R1,
+                     double* R2);
+
+int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
+
+/* Releases the handle and its device memory. */
+int cc4s_cc_destroy(cc4s_cc_handle* h);
+
+/* Message of the last failure on this handle (or of the last failed create). */
+const char* cc4s_cc_last_error(const cc4s_cc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CC4S_CC_H */

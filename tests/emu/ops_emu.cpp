@@ -1,0 +1,263 @@
+// TEST INFRASTRUCTURE ONLY: plain-loop CPU emulation of the device operations
+// declared in cc4s_b200/csrc/ops.h and gemm_f64.cuh.
+//
+// It is linked with the product's schedule and driver sources into a separate
+// test library (tests/emu/_build/libcc4s_emu.so) so that the index and stride
+// bookkeeping of every contraction can be checked against the oracle on a
+// machine without a GPU.  The product library never contains this file.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../cc4s_b200/csrc/ops.h"
+
+namespace cc4s_b200 {
+
+namespace {
+struct Ax {
+  int64_t inner, so, si;
+  int64_t off(int64_t x) const { return (x / inner) * so + (x % inner) * si; }
+};
+Ax ax(int64_t inner, int64_t so, int64_t si) { return Ax{inner > 0 ? inner : 1, so, si}; }
+uint64_t g_gemm = 0, g_ops = 0;
+}  // namespace
+
+uint64_t gemm_launch_count() { return g_gemm; }
+
+void gemm(const Contraction& g, cudaStream_t, const GemmScratch&) {
+  ++g_gemm;
+  if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  const int64_t Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1), Bi = g.Bi > 0 ? g.Bi : g.batch;
+  Ax Am = ax(Mi, g.A.s_ro, g.A.s_ri), Ak = ax(Ki, g.A.s_co, g.A.s_ci);
+  Ax Bk = ax(Ki, g.B.s_ro, g.B.s_ri), Bn = ax(Ni, g.B.s_co, g.B.s_ci);
+  Ax Cm = ax(Mi, g.C.s_ro, g.C.s_ri), Cn = ax(Ni, g.C.s_co, g.C.s_ci);
+  Ax C2m = ax(Mi, g.C2.s_ro, g.C2.s_ri), C2n = ax(Ni, g.C2.s_co, g.C2.s_ci);
+  Ax Ab = ax(Bi, g.A.s_bo, g.A.s_bi), Bb = ax(Bi, g.B.s_bo, g.B.s_bi);
+  Ax Cb = ax(Bi, g.C.s_bo, g.C.s_bi), C2b = ax(Bi, g.C2.s_bo, g.C2.s_bi);
+  std::vector<int64_t> ak(g.K), bk(g.K);
+  for (int64_t k = 0; k < g.K; ++k) { ak[k] = Ak.off(k); bk[k] = Bk.off(k); }
+  for (int64_t b = 0; b < g.batch; ++b) {
+    const double* A = g.A.p ? g.A.p + Ab.off(b) : nullptr;
+    const double* B = g.B.p ? g.B.p + Bb.off(b) : nullptr;
+    for (int64_t m = 0; m < g.M; ++m) {
+      const int64_t am = Am.off(m);
+      for (int64_t n = 0; n < g.N; ++n) {
+        const int64_t bn = Bn.off(n);
+        double s = 0.0;
+        for (int64_t k = 0; k < g.K; ++k) s += A[am + ak[k]] * B[bk[k] + bn];
+        const double v = g.alpha * s;
+        double* c = g.C.p + Cb.off(b) + Cm.off(m) + Cn.off(n);
+        *c = g.beta != 0.0 ? v + g.beta * *c : v;
+        if (g.C2.p) {
+          double* c2 = g.C2.p + C2b.off(b) + C2m.off(m) + C2n.off(n);
+          *c2 = g.beta != 0.0 ? v + g.beta * *c2 : v;
+        }
+      }
+    }
+  }
+}
+
+namespace ops {
+
+double* alloc(size_t elems) {
+  void* p = std::calloc(elems ? elems : 1, sizeof(double));
+  if (!p) throw Error(ERR_OUT_OF_MEMORY, "host allocation failed");
+  return static_cast<double*>(p);
+}
+void release(void* p) { std::free(p); }
+void zero(double* p, size_t n, Stream) { std::memset(p, 0, n * sizeof(double)); }
+void h2d(double* d, const double* s, size_t n, Stream) { std::memcpy(d, s, n * sizeof(double)); }
+void d2h(double* d, const double* s, size_t n, Stream) { std::memcpy(d, s, n * sizeof(double)); }
+void d2d(double* d, const double* s, size_t n, Stream) { std::memmove(d, s, n * sizeof(double)); }
+void sync(Stream) {}
+Stream stream_create(int) { return nullptr; }
+void stream_destroy(Stream) {}
+void* event_create() { return nullptr; }
+void event_record(void*, Stream) {}
+float event_ms(void*, void*) { return 0.f; }
+void event_destroy(void*) {}
+uint64_t launch_count() { return g_ops; }
+
+void permute4(double* dst, const double* src, const int64_t d[4], const int perm[4],
+              double alpha, double beta, Stream) {
+  ++g_ops;
+  int64_t ss[4];
+  ss[3] = 1;
+  for (int k = 2; k >= 0; --k) ss[k] = ss[k + 1] * d[k + 1];
+  int64_t e[4], es[4];
+  for (int k = 0; k < 4; ++k) { e[k] = d[perm[k]]; es[k] = ss[perm[k]]; }
+  int64_t o = 0;
+  for (int64_t i0 = 0; i0 < e[0]; ++i0)
+    for (int64_t i1 = 0; i1 < e[1]; ++i1)
+      for (int64_t i2 = 0; i2 < e[2]; ++i2)
+        for (int64_t i3 = 0; i3 < e[3]; ++i3, ++o) {
+          const double v = alpha * src[i0 * es[0] + i1 * es[1] + i2 * es[2] + i3 * es[3]];
+          dst[o] = beta != 0.0 ? v + beta * dst[o] : v;
+        }
+}
+
+void axpby(double* out, double a, const double* x, double b, const double* y, double c,
+           int64_t n, Stream) {
+  ++g_ops;
+  for (int64_t e = 0; e < n; ++e) {
+    double v = a * x[e];
+    if (y) v += b * y[e];
+    if (c != 0.0) v += c * out[e];
+    out[e] = v;
+  }
+}
+
+void rank1(double* out, double a, const double* A, double b, const double* t, int64_t n,
+           Stream) {
+  ++g_ops;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < n; ++c) out[r * n + c] = a * A[r * n + c] + b * t[r] * t[c];
+}
+
+void symmetrize(double* R, int64_t n, Stream) {
+  ++g_ops;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = r; c < n; ++c) {
+      const double s = R[r * n + c] + R[c * n + r];
+      R[r * n + c] = s;
+      R[c * n + r] = s;
+    }
+}
+
+void gather_vertex(double* out, const double* in, bool cplx, int part, int64_t NG, int64_t Np,
+                   int64_t row0, int64_t nx, int64_t col0, int64_t ny, Stream) {
+  ++g_ops;
+  const int64_t es = cplx ? 2 : 1;
+  for (int64_t g = 0; g < NG; ++g)
+    for (int64_t x = 0; x < nx; ++x)
+      for (int64_t y = 0; y < ny; ++y)
+        out[(g * nx + x) * ny + y] = in[(g + NG * ((row0 + x) + Np * (col0 + y))) * es + part];
+}
+
+void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const double* eh,
+            const double* ep, const AmpShape& sh, double shift, Stream) {
+  ++g_ops;
+  const int64_t n1 = sh.n1();
+  for (int64_t e = 0; e < sh.total(); ++e) {
+    const int64_t q = e % sh.plane();
+    double D;
+    if (q < n1) {
+      D = ep[q / sh.o] - eh[q % sh.o];
+    } else {
+      const int64_t r = q - n1, ai = r / n1, bj = r % n1;
+      D = ep[ai / sh.o] - eh[ai % sh.o] + ep[bj / sh.o] - eh[bj % sh.o];
+    }
+    double rv = R[e];
+    const double told = Told ? Told[e] : 0.0;
+    if (Told && shift != 0.0) rv -= shift * told;
+    const double tn = rv * (-1.0 / (D + shift));
+    Tnew[e] = tn;
+    dT[e] = Told ? tn - told : tn;
+  }
+}
+
+void energy(const double* T, const double* Vdr, const double* Vdi, const double* Ver,
+            const double* Vei, const AmpShape& sh, double* out, double*, Stream) {
+  ++g_ops;
+  const int64_t n1 = sh.n1();
+  const double* t1r = T;
+  const double* t2r = T + n1;
+  const double* t1i = sh.planes > 1 ? T + sh.plane() : nullptr;
+  const double* t2i = sh.planes > 1 ? T + sh.plane() + n1 : nullptr;
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t r = 0; r < n1; ++r)
+    for (int64_t c = 0; c < n1; ++c) {
+      const int64_t e = r * n1 + c;
+      if (!t1i) {
+        const double x = t2r[e] + t1r[r] * t1r[c];
+        acc[0] += x * Vdr[e];
+        acc[1] += x * Ver[e];
+      } else {
+        const double xr = t2r[e] + t1r[r] * t1r[c] - t1i[r] * t1i[c];
+        const double xi = t2i[e] + t1r[r] * t1i[c] + t1i[r] * t1r[c];
+        const double vdi = Vdi ? Vdi[e] : 0.0, vei = Vei ? Vei[e] : 0.0;
+        acc[0] += xr * Vdr[e] + xi * vdi;
+        acc[1] += xr * Ver[e] + xi * vei;
+        acc[2] += xi * Vdr[e] - xr * vdi;
+        acc[3] += xi * Ver[e] - xr * vei;
+      }
+    }
+  out[0] = 2.0 * acc[0]; out[1] = -acc[1]; out[2] = 2.0 * acc[2]; out[3] = -acc[3];
+}
+
+void dots(const double* x, const double* const* ys, int ny, int64_t n, double* out, double*,
+          Stream) {
+  ++g_ops;
+  for (int k = 0; k < ny; ++k) {
+    double s = 0.0;
+    for (int64_t e = 0; e < n; ++e) s += x[e] * ys[k][e];
+    out[k] = s;
+  }
+}
+
+void diis_solve(double* B, const double* dots_dev, const int* valid, int N, int next, int count,
+                double* coef, int* status, Stream) {
+  ++g_ops;
+  const int M = N + 1;
+  int di = 0;
+  for (int i = 0; i < N; ++i) {
+    if (!valid[i]) continue;
+    const double ov = 2.0 * dots_dev[di++];
+    B[(i + 1) * M + next + 1] = ov;
+    B[(next + 1) * M + i + 1] = ov;
+  }
+  const int dim = count + 1;
+  std::vector<double> m(dim * dim), x(dim, 0.0);
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) m[r * dim + c] = B[r * M + c];
+  x[0] = -1.0;
+  int singular = 0;
+  for (int k = 0; k < dim; ++k) {
+    int piv = k;
+    double best = std::fabs(m[k * dim + k]);
+    for (int r = k + 1; r < dim; ++r)
+      if (std::fabs(m[r * dim + k]) > best) { best = std::fabs(m[r * dim + k]); piv = r; }
+    if (best == 0.0 || !std::isfinite(best)) { singular = 1; break; }
+    if (piv != k) {
+      for (int c = 0; c < dim; ++c) std::swap(m[k * dim + c], m[piv * dim + c]);
+      std::swap(x[k], x[piv]);
+    }
+    for (int r = k + 1; r < dim; ++r) {
+      const double f = m[r * dim + k] / m[k * dim + k];
+      for (int c = k; c < dim; ++c) m[r * dim + c] -= f * m[k * dim + c];
+      x[r] -= f * x[k];
+    }
+  }
+  if (!singular) {
+    for (int k = dim - 1; k >= 0; --k) {
+      double s = x[k];
+      for (int c = k + 1; c < dim; ++c) s -= m[k * dim + c] * x[c];
+      x[k] = s / m[k * dim + k];
+    }
+    for (int j = 0; j < count; ++j) coef[j] = x[(next + N - j) % N + 1];
+  }
+  status[0] = singular;
+}
+
+void lincomb(double* out, const double* const* xs, const double* const* ys, const double* coef,
+             int nx, int64_t n, double* norm2, double*, Stream) {
+  ++g_ops;
+  double s2 = 0.0;
+  for (int64_t e = 0; e < n; ++e) {
+    double v = 0.0, w = 0.0;
+    for (int k = 0; k < nx; ++k) {
+      v += coef[k] * xs[k][e];
+      if (ys) w += coef[k] * ys[k][e];
+    }
+    out[e] = v;
+    s2 += w * w;
+  }
+  if (ys && norm2) norm2[0] = s2;
+}
+
+void sum_partials_to(double*, const double*, int, int, Stream) {}
+
+}  // namespace ops
+}  // namespace cc4s_b200

@@ -1,0 +1,88 @@
+"""The product's CCSD schedule and driver (C++ sources of cc4s_b200/csrc)
+linked against a plain-loop CPU emulation of the device operations
+(tests/emu/ops_emu.cpp, test-only) and checked against the oracle.  This pins
+every stride of every contraction without a GPU."""
+import os
+import sys
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import ccsd, coupled_cluster, inputs
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
+warnings.simplefilter("ignore")
+
+
+@pytest.fixture(scope="module")
+def emu_lib():
+    import build_emu
+    return build_emu.build()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _rand_T(rng, Nv, No):
+    T1 = rng.standard_normal((Nv, No)) * 0.05
+    T2 = rng.standard_normal((Nv, Nv, No, No)) * 0.05
+    return T1, T2 + T2.transpose(1, 0, 3, 2)
+
+
+@pytest.mark.parametrize("shape", [(3, 7, 5), (4, 10, 12), (2, 5, 3)])
+@pytest.mark.parametrize("method", ["Ccsd", "Ccd"])
+def test_residual_matches_oracle(emu_lib, shape, method):
+    from cc4s_b200 import Solver
+    No, Nv, NG = shape
+    rng = np.random.default_rng(sum(shape))
+    g = (rng.standard_normal((NG, No + Nv, No + Nv)) + 1j * rng.standard_normal((NG, No + Nv, No + Nv))) * 0.1
+    s = inputs.System(np.sort(rng.uniform(-1.5, -.5, No)), np.sort(rng.uniform(.2, 3, Nv)), g, half_grid=True)
+    T = _rand_T(rng, Nv, No)
+    for ppl in (True, False):
+        sol = Solver({"method": method, "ppl": ppl}, lib=emu_lib)
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        R1, R2 = sol.residual(T)
+        Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s), ppl=ppl, ccd=(method == "Ccd"))
+        assert _rel(R2, Q2) < 1e-13
+        if method == "Ccsd":
+            assert _rel(R1, Q1) < 1e-13
+        else:
+            assert np.abs(R1).max() == 0.0
+
+
+@pytest.mark.parametrize("mixer", [dict(type="DiisMixer", maxResidua=5),
+                                   dict(type="DiisMixer", maxResidua=2),
+                                   dict(type="LinearMixer", ratio=0.7)])
+def test_run_matches_oracle(emu_lib, mixer):
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(4, 12, 20, seed=3)
+    opts = dict(maxIterations=30, energyConvergence=1e-10, amplitudesConvergence=1e-8, mixer=mixer,
+                levelShift=0.1 if mixer["type"] == "LinearMixer" else 0.0)
+    r0 = coupled_cluster.run(s, **opts)
+    sol = Solver(opts, lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    r = sol.run()
+    T1, T2 = sol.amplitudes()
+    assert r["iterations"] == r0["iterations"]
+    assert abs(r["correlation"] - r0["energy"]["correlation"]) < 1e-12
+    assert abs(r["secondOrder"] - r0["energy"]["secondOrder"]) < 1e-12
+    assert _rel(T2, r0["amplitudes"][1]) < 1e-12
+
+
+def test_errors_are_reported(emu_lib):
+    from cc4s_b200 import CoupledClusterError, Solver
+    sol = Solver({}, lib=emu_lib)
+    with pytest.raises(CoupledClusterError) as e:
+        sol.run()
+    assert e.value.status == 8  # inputs not set
+    s = inputs.synthetic_system(2, 5, 3, seed=1)
+    g = s.gamma.copy()
+    g[0, 0, 0] = np.nan
+    with pytest.raises(CoupledClusterError) as e:
+        sol.set_inputs(s.eps_h, s.eps_p, g, True)
+    assert e.value.status == 9  # non-finite input
+    with pytest.raises(CoupledClusterError) as e:
+        Solver({"method": "Ccsdt"}, lib=emu_lib)
+    assert e.value.status == 1
