@@ -1,0 +1,313 @@
+"""Benchmark of the CoupledCluster (CCSD) step on B200.
+
+A "step" is one CCSD iteration (residual, Jacobi update, DIIS, energy) on a
+seeded synthetic system.  Default workload: No=32, Nv=256, NG=1024, real,
+FP64 (the FP64 parity case).  T2 (0.54 GB) and the vertex are larger than
+L2, so no flush is needed between iterations.
+
+value: reference-equivalent TFLOP/s = F_ref / (s per iteration), with F_ref
+the flop count of the reference's formulation (cc4s_b200.flops), timed with
+CUDA events on the library's stream inside the library, max over ranks.
+e2e: the same metric through the C ABI from host buffers: set_inputs (vertex
+upload and integral build) + K iterations + amplitude download, wall clock.
+
+Multi-GPU: every rank runs its own replica of the workload (weak scaling, no
+collective on the data path); value is the sum over ranks.
+
+--impl reference: the CPU restatement of the reference (the oracle; the
+reference itself needs MPI and the Cyclops Tensor Framework, which are not
+installed) timed on this host's cores on a bounded sample of the same
+workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+import warnings
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+warnings.simplefilter("ignore")
+
+CONFIG_SHAPES = {
+    "c0": (8, 40, 200), "c1": (32, 256, 1024), "c2": (64, 640, 2560), "c4": (32, 320, 1600),
+}
+METRIC = "CCSD s/iter & TFLOP/s: TC split-precision vs FP64 on 1 B200 at |ΔEc|≤1µEh"
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.stop = threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dgemm_peak(device):
+    """FP64 tensor peak measured here: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    best = 1e30
+    for k in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        if k:
+            best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_sample(cfg):
+    """CPU rate of the oracle on the workload's dominant contractions (bounded sample).
+
+    Times one (vo)^3 ring contraction and one particle-particle-ladder slice pair
+    of the workload with the oracle's numpy/BLAS restatement on all host cores,
+    and converts the measured rate into seconds per iteration of the reference
+    formulation.
+    """
+    import numpy as np
+    from oracle import ccsd as occ, inputs as oin
+    from cc4s_b200.flops import reference_flops
+    o, v, G = CONFIG_SHAPES[cfg]
+    s = oin.config_system(cfg, seed=0)
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((v, v, o, o))
+    Y = rng.standard_normal((v, o, o, v))
+    t0 = time.perf_counter()
+    occ.es("akic,cbkj->abij", Y, X)
+    t1 = time.perf_counter()
+    dG = np.ascontiguousarray(s.gamma[:, o:, o:])
+    sl = o
+    V = occ.es("Gxc,Gyd->xycd", dG[:, :sl, :], dG[:, sl:2 * sl, :])
+    occ.es("xycd,cdij->xyij", V, X)
+    t2 = time.perf_counter()
+    flops = 2.0 * v ** 3 * o ** 3 + 2.0 * sl * sl * v * v * (G + o * o)
+    rate = flops / (t2 - t0)
+    s_iter = reference_flops(o, v, G) / rate
+    return dict(s_per_iter=s_iter, rate_tflops=rate / 1e12, sample_seconds=t2 - t0,
+                cores=os.cpu_count(),
+                sample="oracle numpy/BLAS on one (vo)^3 ring contraction and one ladder slice "
+                       "pair (s=No) of %s; s/iter = reference flops / measured rate" % cfg)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def all_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from cc4s_b200 import Solver, reference_flops
+    from cc4s_b200.synthetic import config
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    eh, ep, g, hg = config(cfg, seed=0)
+    F = reference_flops(o, v, G)
+    K, W = args.steps, args.warmup
+    opts = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
+                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
+    sol = Solver(opts)
+    sol.set_inputs(eh, ep, g, half_grid=hg)
+    st0 = sol.stats()
+    barrier(world)
+    with ClockSampler(local) as clk:
+        r = sol.run()
+    barrier(world)
+    st1 = sol.stats()
+    secs = [h["seconds"] for h in r["history"]]
+    t = all_max(sum(secs[W:W + K]), world)
+    ms = 1e3 * t / K
+    launches_per_it = ((st1["gemm_launches"] - st0["gemm_launches"]) +
+                       (st1["other_launches"] - st0["other_launches"])) / (W + K)
+    T1, T2 = sol.amplitudes()
+    sol.close()
+    # dominant kernel: per-launch CUDA events around every DMMA contraction of one residual
+    prof = Solver(dict(opts, profile=True, maxIterations=1))
+    prof.set_inputs(eh, ep, g, half_grid=hg)
+    prof.residual((T1, T2))
+    ps = prof.stats()
+    prof.close()
+    peak = dgemm_peak(local)
+    achieved = ps["gemm_flops"] / ps["gemm_seconds"] / 1e12
+    # end to end through the C ABI from host buffers
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e = Solver(dict(opts, maxIterations=K))
+    e2e.set_inputs(eh, ep, g, half_grid=hg)
+    re = e2e.run()
+    A1, A2 = e2e.amplitudes()
+    torch.cuda.synchronize()
+    t_e2e = all_max(time.perf_counter() - t0, world)
+    e2e.close()
+    h2d = (g.nbytes + eh.nbytes + ep.nbytes) / K
+    d2h = (A1.nbytes + A2.nbytes) / K + 5 * 8 + 8
+    line = {
+        "metric": METRIC, "value": world * F / (t / K) / 1e12, "unit": "TFLOP/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator of the workload's distributions)",
+        "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d real, DIIS 5" % (cfg, o, v, G),
+                   "precision": "fp64 (DMMA)", "s_per_iter": t / K,
+                   "flops_per_iter_reference_formulation": F,
+                   "flops_per_iter_executed": r["flops_per_iteration"],
+                   "l2": "inputs larger than L2 (T2 %.2f GB)" % ((v * o) ** 2 * 8 / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "energy_after_steps": r["correlation"]},
+        "e2e": {"value": world * F * K / t_e2e / 1e12, "unit": "TFLOP/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "seconds": t_e2e, "iterations": re["iterations"]},
+        "gpu_launches": int(round(launches_per_it * K)),
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "gemm_f64_kernel (mma.sync m16n8k4 f64), all %d contraction "
+                               "launches of one residual" % ps["gemm_profiled_launches"],
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry "
+                                    "in MEASURED_PEAKS.json)",
+                     "top_launch_tflops": ps["top_flops"] / ps["top_seconds"] / 1e12},
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+def run_reference(args, world, rank):
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    from cc4s_b200.flops import reference_flops
+    F = reference_flops(o, v, G)
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    samples = [cpu_sample(cfg) for _ in range(max(1, args.steps))]
+    s_iter = statistics.median(x["s_per_iter"] for x in samples)
+    c = samples[0]
+    val = F / s_iter / 1e12
+    return {"impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * s_iter, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d real" % (cfg, o, v, G),
+                       "implementation": "CPU restatement of the reference (oracle, numpy/BLAS); "
+                                         "the reference build needs MPI + CTF, not installed"},
+            "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": c["cores"],
+                             "kind": "port", "sample": c["sample"]},
+            "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1", choices=sorted(CONFIG_SHAPES))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, world, rank)), flush=True)
+        return
+    world, rank, local = dist_setup()
+    line = run_ours(args, world, rank, local)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            c = cpu_sample(args.config)
+            from cc4s_b200.flops import reference_flops
+            o, v, G = CONFIG_SHAPES[args.config]
+            line["cpu_baseline"] = {"value": reference_flops(o, v, G) / c["s_per_iter"] / 1e12,
+                                    "unit": "TFLOP/s", "cores": c["cores"], "kind": "port",
+                                    "sample": c["sample"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -41,6 +41,7 @@ class Options(ctypes.Structure):
         ("max_iterations", ctypes.c_int), ("energy_convergence", ctypes.c_double),
         ("amplitudes_convergence", ctypes.c_double), ("level_shift", ctypes.c_double),
         ("integrals_slice_size", ctypes.c_int64), ("ppl", ctypes.c_int), ("device", ctypes.c_int),
+        ("profile", ctypes.c_int),
     ]
 
 
@@ -60,6 +61,9 @@ class Stats(ctypes.Structure):
     _fields_ = [
         ("gemm_launches", ctypes.c_uint64), ("other_launches", ctypes.c_uint64),
         ("device_bytes", ctypes.c_uint64), ("flops_per_residual", ctypes.c_double),
+        ("gemm_seconds", ctypes.c_double), ("gemm_flops", ctypes.c_double),
+        ("top_seconds", ctypes.c_double), ("top_flops", ctypes.c_double),
+        ("gemm_profiled_launches", ctypes.c_int),
     ]
 
 

@@ -42,6 +42,7 @@ def _options(lib, arguments):
     o.ppl = 1 if arguments.get("ppl", True) else 0
     o.precision = _abi.PRECISIONS[arguments.get("precision", "fp64")]
     o.device = int(arguments.get("device", 0))
+    o.profile = 1 if arguments.get("profile", False) else 0
     return o
 
 
@@ -141,7 +142,10 @@ class Solver:
         s = _abi.Stats()
         self._check(self.lib.cc4s_cc_get_stats(self.h, ctypes.byref(s)))
         return dict(gemm_launches=s.gemm_launches, other_launches=s.other_launches,
-                    device_bytes=s.device_bytes, flops_per_residual=s.flops_per_residual)
+                    device_bytes=s.device_bytes, flops_per_residual=s.flops_per_residual,
+                    gemm_seconds=s.gemm_seconds, gemm_flops=s.gemm_flops,
+                    top_seconds=s.top_seconds, top_flops=s.top_flops,
+                    gemm_profiled_launches=s.gemm_profiled_launches)
 
 
 def _full_vertex(arguments):

@@ -218,6 +218,7 @@ void cc4s_cc_default_options(cc4s_cc_options* o) {
   o->integrals_slice_size = 0;
   o->ppl = 1;
   o->device = 0;
+  o->profile = 0;
 }
 
 int cc4s_cc_create(const cc4s_cc_options* opt, cc4s_cc_handle** h) {
@@ -275,6 +276,16 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
   if (h->impl->solver) bytes += h->impl->solver->device_bytes();
   out->device_bytes = bytes;
   out->flops_per_residual = h->impl->solver ? h->impl->solver->flops_per_residual() : 0.0;
+  out->gemm_seconds = out->gemm_flops = out->top_seconds = out->top_flops = 0.0;
+  out->gemm_profiled_launches = 0;
+  if (h->impl->solver) {
+    const auto& p = h->impl->solver->profile();
+    out->gemm_seconds = p.gemm_seconds;
+    out->gemm_flops = p.gemm_flops;
+    out->top_seconds = p.top_seconds;
+    out->top_flops = p.top_flops;
+    out->gemm_profiled_launches = p.launches;
+  }
   return 0;
 }
 

@@ -89,12 +89,37 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
 }
 
 CcsdReal::~CcsdReal() {
+  for (void* e : ev_) ops::event_destroy(e);
   for (double* p : owned_) ops::release(p);
 }
 
 void CcsdReal::gemm_(const Contraction& c) {
-  if (count_flops_) flops_ += 2.0 * double(c.M) * double(c.N) * double(c.K) * double(c.batch);
+  const double f = 2.0 * double(c.M) * double(c.N) * double(c.K) * double(c.batch);
+  if (count_flops_) flops_ += f;
+  if (profile_ && count_flops_) {
+    const size_t k = ev_flops_.size();
+    while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
+    ev_flops_.push_back(f);
+    ops::event_record(ev_[2 * k], s_);
+    gemm(c, s_, scratch_);
+    ops::event_record(ev_[2 * k + 1], s_);
+    return;
+  }
   gemm(c, s_, scratch_);
+}
+
+void CcsdReal::profile_finish() {
+  if (!profile_) return;
+  Profile p;
+  for (size_t k = 0; k < ev_flops_.size(); ++k) {
+    const double sec = 1e-3 * ops::event_ms(ev_[2 * k], ev_[2 * k + 1]);
+    p.gemm_seconds += sec;
+    p.gemm_flops += ev_flops_[k];
+    if (ev_flops_[k] > p.top_flops) { p.top_flops = ev_flops_[k]; p.top_seconds = sec; }
+  }
+  p.launches = static_cast<int>(ev_flops_.size());
+  ev_flops_.clear();
+  prof_ = p;
 }
 
 // Iteration-independent integrals (VertexCoulombIntegrals.cxx:87-121).
@@ -397,6 +422,7 @@ void CcsdReal::residual(const double* T, double* R) {
   if (opt_.ppl) ppl(Xp_, R2, dGpp_);
   if (ccd) {
     ops::zero(R1, n1, s_);
+    profile_finish();
     return;
   }
   // ---- singles (Ccsd.cxx:339-375) ------------------------------------------------
@@ -466,6 +492,7 @@ void CcsdReal::residual(const double* T, double* R) {
     c.alpha = -1.0; c.beta = 1.0;
     gemm_(c);
   }
+  profile_finish();
 }
 
 // Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of size s,

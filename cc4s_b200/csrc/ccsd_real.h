@@ -45,6 +45,16 @@ class CcsdReal {
   double flops_per_residual() const { return flops_; }
   size_t device_bytes() const { return bytes_; }
 
+  // Per-launch timing of the tensor-core contractions (CUDA events around each
+  // launch).  Off by default; when on, residual() synchronises at its end.
+  void set_profile(bool on) { profile_ = on; }
+  struct Profile {
+    double gemm_seconds = 0, gemm_flops = 0;      // all contractions of the last residual
+    double top_seconds = 0, top_flops = 0;        // the most expensive single launch
+    int launches = 0;
+  };
+  const Profile& profile() const { return prof_; }
+
  private:
   void gemm_(const Contraction& c);
   double* take(size_t elems);
@@ -59,6 +69,11 @@ class CcsdReal {
   size_t bytes_ = 0;
   double flops_ = 0.0;
   bool count_flops_ = true;
+  bool profile_ = false;
+  Profile prof_;
+  std::vector<void*> ev_;          // event pool: 2 per profiled launch
+  std::vector<double> ev_flops_;
+  void profile_finish();
   // static integrals
   double *Vd_ = nullptr, *Ve_ = nullptr, *Vp_ = nullptr, *Vtp_ = nullptr;
   double *Vhhhh_ = nullptr, *Vhhhp_ = nullptr, *Vh2_ = nullptr;

@@ -114,6 +114,7 @@ void Handle::allocate_state() {
   ro.ccd = opt.method == CC4S_METHOD_CCD;
   ro.ppl = opt.ppl != 0;
   solver.reset(new CcsdReal(sys, ro, stream));
+  solver->set_profile(opt.profile != 0);
   const int64_t n = shape.total();
   Tcur = take(n);
   Rbuf = take(n);

@@ -75,6 +75,7 @@ typedef struct {
   int64_t integrals_slice_size; /* "integralsSliceSize" (0 = No), Ccsd.cxx:287-289 */
   int ppl;                      /* "ppl" (1), Ccsd.cxx:95 */
   int device;                   /* CUDA device ordinal */
+  int profile;                  /* 1: time every contraction launch (CUDA events) */
 } cc4s_cc_options;
 
 typedef struct {
@@ -95,6 +96,10 @@ typedef struct {
   uint64_t other_launches;     /* bandwidth kernels launched so far */
   uint64_t device_bytes;       /* device memory held by the handle */
   double flops_per_residual;   /* FP64-equivalent flops of one residual */
+  /* with options.profile: contraction launches of the last residual */
+  double gemm_seconds, gemm_flops;   /* all launches */
+  double top_seconds, top_flops;     /* the most expensive launch */
+  int gemm_profiled_launches;
 } cc4s_cc_stats;
 
 /* Fills the defaults of the reference. */

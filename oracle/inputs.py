@@ -61,27 +61,11 @@ def synthetic_system(No, Nv, NG, complex=False, seed=0):
     (Gamma_qp = conj(Gamma_pq), complex path, real and imaginary parts each
     N(0, s^2/2)).
     """
-    rng = np.random.default_rng(seed)
-    eps_h = np.sort(rng.uniform(-1.5, -0.5, No))
-    eps_p = np.sort(rng.uniform(0.2, 3.0, Nv))
-    Np = No + Nv
-    s = 0.1 * NG ** (-0.25)
-    iu = np.triu_indices(Np)
-    if not complex:
-        g = np.zeros((NG, Np, Np))
-        vals = rng.standard_normal((NG, iu[0].size)) * s
-        g[:, iu[0], iu[1]] = vals
-        g[:, iu[1], iu[0]] = vals
-        return System(eps_h, eps_p, g, half_grid=True)
-    g = np.zeros((NG, Np, Np), dtype=np.complex128)
-    re = rng.standard_normal((NG, iu[0].size)) * (s / math.sqrt(2.0))
-    im = rng.standard_normal((NG, iu[0].size)) * (s / math.sqrt(2.0))
-    vals = re + 1j * im
-    diag = iu[0] == iu[1]
-    vals[:, diag] = vals[:, diag].real  # Hermitian: real diagonal
-    g[:, iu[0], iu[1]] = vals
-    g[:, iu[1], iu[0]] = np.conj(vals)
-    return System(eps_h, eps_p, g, half_grid=False)
+    # The input generator is shared with the benchmark (inputs only; it
+    # computes nothing that is checked).
+    from cc4s_b200.synthetic import synthetic
+    eps_h, eps_p, g, half_grid = synthetic(No, Nv, NG, complex=complex, seed=seed)
+    return System(eps_h, eps_p, g, half_grid=half_grid)
 
 
 def config_system(name, seed=0):

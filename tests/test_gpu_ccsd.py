@@ -1,0 +1,108 @@
+"""Parity of the CUDA library (through its C ABI) with the oracle on a B200."""
+import json
+import os
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import ccsd, coupled_cluster, inputs, properties
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+warnings.simplefilter("ignore")
+
+# FP64 parity bar: 1e-9 Eh in energies and 1e-9 relative in amplitudes; single
+# residual evaluations agree to rounding (1e-12 relative to the largest element).
+TOL_E = 1e-9
+TOL_AMP = 1e-9
+TOL_RES = 1e-12
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _rand_T(rng, Nv, No, scale=0.02):
+    T1 = rng.standard_normal((Nv, No)) * scale
+    T2 = rng.standard_normal((Nv, Nv, No, No)) * scale
+    return T1, T2 + T2.transpose(1, 0, 3, 2)
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from cc4s_b200 import Solver as S
+    return S
+
+
+@pytest.mark.parametrize("shape,cplx", [((3, 7, 5), True), ((8, 40, 200), False),
+                                        ((5, 33, 70), True), ((16, 128, 256), False)])
+@pytest.mark.parametrize("method", ["Ccsd", "Ccd"])
+def test_residual_parity(Solver, shape, cplx, method):
+    No, Nv, NG = shape
+    rng = np.random.default_rng(No * 1000 + Nv)
+    g = rng.standard_normal((NG, No + Nv, No + Nv)) * 0.1 * NG ** -0.25
+    if cplx:
+        g = g + 1j * rng.standard_normal(g.shape) * 0.1 * NG ** -0.25
+    s = inputs.System(np.sort(rng.uniform(-1.5, -.5, No)), np.sort(rng.uniform(.2, 3, Nv)), g, True)
+    T = _rand_T(rng, Nv, No)
+    sol = Solver({"method": method})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+    R1, R2 = sol.residual(T)
+    Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s), ccd=(method == "Ccd"))
+    assert _rel(R2, Q2) < TOL_RES
+    if method == "Ccsd":
+        assert _rel(R1, Q1) < TOL_RES
+    F1, F2 = sol.residual(None)
+    assert _rel(F2, Q2 * 0 + ccsd.residuum(None, ccsd.CcsdInputs(s))[1]) < TOL_RES
+    sol.close()
+
+
+def test_c0_golden_trajectory(Solver):
+    g = json.load(open(os.path.join(GOLDEN, "c0_seed0.json")))
+    s = inputs.config_system("c0", seed=g["seed"])
+    sol = Solver(g["options"])
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+    r = sol.run()
+    assert r["iterations"] == g["iterations"]
+    assert r["converged"] == g["converged"]
+    for h, e in zip(r["history"], g["history_energy"]):
+        assert abs(h["energy"] - e) < TOL_E
+    assert abs(r["correlation"] - g["energy"]["correlation"]) < TOL_E
+    assert abs(r["secondOrder"] - g["energy"]["secondOrder"]) < TOL_E
+    T1, T2 = sol.amplitudes()
+    ref = coupled_cluster.run(s, **g["options"])
+    assert _rel(T2, ref["amplitudes"][1]) < TOL_AMP
+    assert _rel(T1, ref["amplitudes"][0]) < TOL_AMP
+
+
+@pytest.mark.parametrize("opts", [
+    dict(method="Ccd", mixer=dict(type="DiisMixer", maxResidua=4)),
+    dict(method="Ccsd", mixer=dict(type="LinearMixer", ratio=0.8), levelShift=0.2),
+    dict(method="Ccsd", ppl=False, mixer=dict(type="DiisMixer", maxResidua=3)),
+])
+def test_run_variants(Solver, opts):
+    s = inputs.synthetic_system(6, 30, 60, seed=11)
+    o = dict(maxIterations=40, energyConvergence=1e-10, amplitudesConvergence=1e-8)
+    o.update(opts)
+    ref = coupled_cluster.run(s, **o)
+    sol = Solver(o)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    r = sol.run()
+    assert r["iterations"] == ref["iterations"]
+    assert abs(r["correlation"] - ref["energy"]["correlation"]) < TOL_E
+    T1, T2 = sol.amplitudes()
+    assert _rel(T2, ref["amplitudes"][1]) < TOL_AMP
+
+
+def test_c1_size_independent_properties(Solver):
+    """At the FP64 parity size (No=32, Nv=256, NG=1024): the first iteration gives
+    the MP2 energy, and the amplitudes keep the pair symmetry T_abij = T_baji."""
+    s = inputs.config_system("c1", seed=0)
+    sol = Solver(dict(maxIterations=3, energyConvergence=0.0))
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    r = sol.run()
+    assert abs(r["secondOrder"] - properties.mp2(s)[0]) < TOL_E
+    T1, T2 = sol.amplitudes()
+    assert _rel(T2.transpose(1, 0, 3, 2), T2) < 1e-12
+    assert all(np.isfinite(h["energy"]) for h in r["history"])
