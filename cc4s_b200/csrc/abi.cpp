@@ -3,46 +3,75 @@
 #include <complex>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "driver.h"
 
 namespace cc4s_b200 {
 
 // Reference layout T1[a,i], T2[a,b,i,j] (first index fastest) -> amplitude vector.
+// Complex host buffers are interleaved (re, im); device vectors are planar.
 void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2) {
-  const int64_t o = shape.o, v = shape.v, n1 = v * o;
+  const int64_t o = shape.o, v = shape.v, n1 = v * o, pl = shape.plane();
   double* st = Rs[0];
-  ops::h2d(st, T1, n1, stream);
-  ops::h2d(st + n1, T2, n1 * n1, stream);
-  const int64_t d1[4] = {1, 1, o, v};
-  const int p1[4] = {0, 1, 3, 2};
-  ops::permute4(dst, st, d1, p1, 1.0, 0.0, stream);
-  const int64_t d2[4] = {o, o, v, v};  // [j][i][b][a]
-  const int p2[4] = {3, 1, 2, 0};      // -> [a][i][b][j]
-  ops::permute4(dst + n1, st + n1, d2, p2, 1.0, 0.0, stream);
+  std::vector<double> h1, h2;
+  for (int64_t p = 0; p < shape.planes; ++p) {
+    const double* s1 = T1;
+    const double* s2 = T2;
+    if (shape.planes > 1) {
+      h1.resize(n1);
+      h2.resize(n1 * n1);
+      for (int64_t k = 0; k < n1; ++k) h1[k] = T1[2 * k + p];
+      for (int64_t k = 0; k < n1 * n1; ++k) h2[k] = T2[2 * k + p];
+      s1 = h1.data();
+      s2 = h2.data();
+    }
+    ops::h2d(st, s1, n1, stream);
+    ops::h2d(st + n1, s2, n1 * n1, stream);
+    const int64_t d1[4] = {1, 1, o, v};
+    const int p1[4] = {0, 1, 3, 2};
+    ops::permute4(dst + p * pl, st, d1, p1, 1.0, 0.0, stream);
+    const int64_t d2[4] = {o, o, v, v};  // [j][i][b][a]
+    const int p2[4] = {3, 1, 2, 0};      // -> [a][i][b][j]
+    ops::permute4(dst + p * pl + n1, st + n1, d2, p2, 1.0, 0.0, stream);
+    ops::sync(stream);
+  }
 }
 
 void Handle::download_amplitudes(const double* src, double* T1, double* T2) {
-  const int64_t o = shape.o, v = shape.v, n1 = v * o;
+  const int64_t o = shape.o, v = shape.v, n1 = v * o, pl = shape.plane();
   double* st = Rs[0];
-  const int64_t d1[4] = {1, 1, v, o};
-  const int p1[4] = {0, 1, 3, 2};
-  ops::permute4(st, src, d1, p1, 1.0, 0.0, stream);
-  const int64_t d2[4] = {v, o, v, o};  // [a][i][b][j]
-  const int p2[4] = {3, 1, 2, 0};      // -> [j][i][b][a]
-  ops::permute4(st + n1, src + n1, d2, p2, 1.0, 0.0, stream);
-  if (T1) ops::d2h(T1, st, n1, stream);
-  if (T2) ops::d2h(T2, st + n1, n1 * n1, stream);
-  ops::sync(stream);
+  std::vector<double> h1, h2;
+  for (int64_t p = 0; p < shape.planes; ++p) {
+    const int64_t d1[4] = {1, 1, v, o};
+    const int p1[4] = {0, 1, 3, 2};
+    ops::permute4(st, src + p * pl, d1, p1, 1.0, 0.0, stream);
+    const int64_t d2[4] = {v, o, v, o};  // [a][i][b][j]
+    const int p2[4] = {3, 1, 2, 0};      // -> [j][i][b][a]
+    ops::permute4(st + n1, src + p * pl + n1, d2, p2, 1.0, 0.0, stream);
+    if (shape.planes == 1) {
+      if (T1) ops::d2h(T1, st, n1, stream);
+      if (T2) ops::d2h(T2, st + n1, n1 * n1, stream);
+      ops::sync(stream);
+    } else {
+      h1.resize(n1);
+      h2.resize(n1 * n1);
+      ops::d2h(h1.data(), st, n1, stream);
+      ops::d2h(h2.data(), st + n1, n1 * n1, stream);
+      ops::sync(stream);
+      if (T1) for (int64_t k = 0; k < n1; ++k) T1[2 * k + p] = h1[k];
+      if (T2) for (int64_t k = 0; k < n1 * n1; ++k) T2[2 * k + p] = h2[k];
+    }
+  }
 }
 
 void Handle::set_initial(const double* T1, const double* T2) {
   require_inputs();
   if (!T1 || !T2) throw Error(ERR_INVALID_ARGUMENT, "null amplitudes");
-  const int64_t n1 = shape.n1();
-  for (int64_t k = 0; k < n1; ++k)
+  const int64_t n1 = shape.n1(), np = shape.planes;
+  for (int64_t k = 0; k < n1 * np; ++k)
     if (!std::isfinite(T1[k])) throw Error(ERR_NON_FINITE, "non-finite T1");
-  for (int64_t k = 0; k < n1 * n1; ++k)
+  for (int64_t k = 0; k < n1 * n1 * np; ++k)
     if (!std::isfinite(T2[k])) throw Error(ERR_NON_FINITE, "non-finite T2");
   upload_amplitudes(Tcur, T1, T2);
   ops::sync(stream);
@@ -107,7 +136,7 @@ int Handle::run(cc4s_cc_result* out) {
     const bool second = !have_T;
     mix(A[slot], Rs[slot], scal + 4);
     have_T = true;
-    ops::energy(Tcur, solver->Vd(), nullptr, solver->Ve(), nullptr, shape, scal, ws, stream);
+    ops::energy(Tcur, solver->Vd(), solver->Vd_im(), solver->Ve(), solver->Ve_im(), shape, scal, ws, stream);
     ops::event_record(ev1, stream);
     ops::d2h(host, scal, 5, stream);
     double st = 0.0;
@@ -137,7 +166,7 @@ int Handle::run(cc4s_cc_result* out) {
   (void)N;
   if (maxIt == 0) {
     if (!have_T) throw Error(ERR_STATE, "maxIterations = 0 needs initial amplitudes");
-    ops::energy(Tcur, solver->Vd(), nullptr, solver->Ve(), nullptr, shape, scal, ws, stream);
+    ops::energy(Tcur, solver->Vd(), solver->Vd_im(), solver->Ve(), solver->Ve_im(), shape, scal, ws, stream);
     ops::d2h(host, scal, 4, stream);
     ops::sync(stream);
     Dr = host[0]; Xr = host[1];

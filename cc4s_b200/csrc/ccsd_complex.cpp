@@ -1,0 +1,492 @@
+// Complex-path CCSD / CCD residual, restated from cc4s Ccsd<Complex>::getResiduum
+// (src/main/algorithms/coupledcluster/Ccsd.cxx:382-633) as FP64 tensor-core
+// contractions on planar complex tensors.
+//
+// Integrals follow VertexCoulombIntegrals.cxx:143-190:
+//   V_pqsr = sum_G conj(Gamma_G,s,p) Gamma_G,q,r.
+// Layouts as on the real path (pair [a][i][b][j], exchange, pp).  Exact
+// rearrangements relative to the reference:
+//   * Vphhh T1 and Vphhp T1 T1 (Ccsd.cxx:490-491) are contracted through the
+//     vertex: sum_G conj(Gamma_G,i,a) sum_k T_bk (Gamma_G,k,j + sum_c Gamma_G,k,c T_cj);
+//   * Vphhp T1 and Vphph T1 in the singles (Ccsd.cxx:620-621) likewise;
+//   * the ring (Ccsd.cxx:494-502) contracts the vertex part as
+//     cTdGamma^T (Gamma (2T - T^x)) without forming Xakic;
+//   * the crossed ring's second term is written into the exchange pairing;
+//   * the ladder runs on a >= b slabs as on the real path.
+#include "ccsd_complex.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace cc4s_b200 {
+
+CcsdComplex::CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Stream s)
+    : Schedule(s), sys_(sys), opt_(opt) {
+  const int64_t o = sys.o, v = sys.v, G = sys.G, n1 = v * o, D2 = n1 * n1;
+  if (o <= 0 || v <= 0 || G <= 0) throw Error(ERR_BAD_SHAPE, "CcsdComplex: empty dimension");
+  D2_ = D2;
+  try {
+    scratch_.elems = static_cast<size_t>(std::max<int64_t>(int64_t(1) << 22,
+                                                           std::min<int64_t>(64 * v * v, int64_t(1) << 25)));
+    scratch_.p = take(scratch_.elems);
+    auto z = [&](int64_t n) { return take(2 * n); };
+    Vd_ = z(D2); Ven_ = z(D2); Vh4_ = z(D2); Vtc_ = z(D2); M2_ = z(D2); M3_ = z(D2);
+    Vhhhh_ = z(o * o * o * o); Vhhhp_ = z(o * o * o * v); Vh2_ = z(o * o * o * v);
+    Xd_ = z(D2); Xp_ = z(D2); Te_ = z(D2); Y_ = z(D2); W8_ = z(D2); Tp_ = z(D2); EX_ = z(D2);
+    Kki_ = z(o * o); Kac_ = z(v * v); Lac_ = z(v * v); Lki_ = z(o * o); jG_ = z(G);
+    U_ = z(G * n1); cTdGph_ = z(G * n1); W_ = z(G * n1); SQ_ = z(G * n1); W1_ = z(G * n1);
+    F_ = z(G * n1); cTdGpp_ = z(G * v * v); dGpp_ = z(G * v * v); dGhh_ = z(G * o * o);
+    Xkl1_ = z(o * o * o * o); Xkl2_ = z(o * o * o * o); kck_ = z(n1); P1_ = z(o * o);
+    P_ = z(G * o * v);
+    // The ladder slices follow integralsSliceSize (default No) exactly: the
+    // reference mirrors each a > b slice pair into (b,a,j,i), which equals the
+    // directly computed block only for a Hermitian vertex, so for a general
+    // complex vertex the result depends on the slicing (Ccsd.cxx:553-598).
+    const int64_t sl = opt.slab > 0 ? opt.slab : o;
+    slab_rows_ = std::min(sl, v);
+    if (opt.ppl) slab_ = z(slab_rows_ * slab_rows_ * v * v);
+  } catch (...) {
+    release_all();
+    throw;
+  }
+  count_flops_ = false;
+  build_integrals();
+  count_flops_ = true;
+}
+
+void CcsdComplex::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA,
+                        bool conjB) {
+  const double sA = conjA ? -1.0 : 1.0, sB = conjB ? -1.0 : 1.0;
+  const double al = c.alpha, be = c.beta;
+  double* Ar = c.A.p;
+  double* Br = c.B.p;
+  double* Cr = c.C.p;
+  double* C2r = c.C2.p;
+  // real plane: Re(A) Re(B) - sA sB Im(A) Im(B)
+  gemm_(c);
+  if (a_im && b_im) {
+    Contraction r = c;
+    r.A.p = Ar + a_im; r.B.p = Br + b_im; r.alpha = -al * sA * sB; r.beta = 1.0;
+    gemm_(r);
+  }
+  // imaginary plane: sB Re(A) Im(B) + sA Im(A) Re(B)
+  Contraction i = c;
+  i.C.p = Cr + c_im;
+  if (C2r) i.C2.p = C2r + c_im;
+  bool wrote = false;
+  if (b_im) {
+    i.B.p = Br + b_im; i.alpha = al * sB; i.beta = be;
+    gemm_(i);
+    wrote = true;
+  }
+  if (a_im) {
+    i.A.p = Ar + a_im; i.B.p = Br; i.alpha = al * sA; i.beta = wrote ? 1.0 : be;
+    gemm_(i);
+    wrote = true;
+  }
+  if (!wrote) throw Error(ERR_STATE, "zgemm: both operands real");
+}
+
+void CcsdComplex::zperm(double* dst, int64_t dst_im, const double* src, int64_t src_im,
+                        const int64_t d[4], const int p[4], double alpha, double beta,
+                        bool conj) {
+  ops::permute4(dst, src, d, p, alpha, beta, s_);
+  ops::permute4(dst + dst_im, src + src_im, d, p, conj ? -alpha : alpha, beta, s_);
+}
+
+// out = a x + b y on both planes; every operand has its imaginary plane at +n.
+void CcsdComplex::zaxpby(double* out, double a, const double* x, double b, const double* y,
+                         int64_t n) {
+  ops::axpby(out, a, x, b, y, 0.0, n, s_);
+  ops::axpby(out + n, a, x + n, b, y ? y + n : nullptr, 0.0, n, s_);
+}
+
+// Iteration-independent integrals (VertexCoulombIntegrals.cxx:143-190).
+void CcsdComplex::build_integrals() {
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o, D2 = D2_;
+  const int64_t gpp = G * v * v, gph = G * n1, ghh = G * o * o;
+  double *Gpp = sys_.Gpp, *Gph = sys_.Gph, *Ghh = sys_.Ghh, *Ghp = sys_.Ghp;
+  (void)Gpp; (void)ghh; (void)gpp;
+  {  // Vd[(a,i),(b,j)] = V_abij = sum_G conj(Ghp[G][i][a]) Gph[G][b][j]
+    Contraction c; c.M = n1; c.N = n1; c.K = G; c.Mi = o;
+    c.A = vw(Ghp, 1, v, 0, n1);
+    c.B = rm(Gph, n1);
+    c.C = vw(Vd_, o * n1, n1, 0, 1);
+    zgemm(c, gph, gph, D2, true, false);
+  }
+  const int64_t d4[4] = {v, o, v, o};
+  { const int pm[4] = {2, 1, 0, 3}; zperm(Ven_, D2, Vd_, D2, d4, pm, 1.0, 0.0); }  // V_baij
+  {  // Vh4[k][l][c][d] = V_klcd = sum_G conj(Gph[G][c][k]) Ghp[G][l][d]
+    Contraction c; c.M = o * v; c.N = o * v; c.K = G; c.Mi = v; c.Ni = v;
+    c.A = vw(Gph, 1, o, 0, n1);
+    c.B = vw(Ghp, 0, n1, v, 1);
+    c.C = vw(Vh4_, o * v * v, v, v * v, 1);
+    zgemm(c, gph, gph, D2, true, false);
+  }
+  const int64_t dh[4] = {o, o, v, v};  // Vh4 [k][l][c][d]
+  {  // Vtc[c][d][k][l] = 2 V_klcd - V_kldc
+    const int pa[4] = {2, 3, 0, 1}, pb[4] = {3, 2, 0, 1};
+    zperm(Vtc_, D2, Vh4_, D2, dh, pa, 2.0, 0.0);
+    zperm(Vtc_, D2, Vh4_, D2, dh, pb, -1.0, 1.0);
+  }
+  {  // M2[(c,k),(d,l)] = V_lkdc - V_lkcd / 2 ;  M3[(c,k),(d,l)] = V_lkcd
+    const int pa[4] = {3, 1, 2, 0}, pb[4] = {2, 1, 3, 0};
+    zperm(M2_, D2, Vh4_, D2, dh, pa, 1.0, 0.0);
+    zperm(M2_, D2, Vh4_, D2, dh, pb, -0.5, 1.0);
+    zperm(M3_, D2, Vh4_, D2, dh, pb, 1.0, 0.0);
+  }
+  const int64_t o4 = o * o * o * o, o3v = o * o * o * v;
+  {  // Vhhhh[k][l][i][j] = sum_G conj(Ghh[G][i][k]) Ghh[G][l][j]
+    Contraction c; c.M = o * o; c.N = o * o; c.K = G; c.Mi = o; c.Ni = o;
+    c.A = vw(Ghh, 1, o, 0, o * o);
+    c.B = vw(Ghh, 0, o * o, o, 1);
+    c.C = vw(Vhhhh_, o * o * o, o, o * o, 1);
+    zgemm(c, G * o * o, G * o * o, o4, true, false);
+  }
+  {  // Vhhhp[k][l][i][c] = sum_G conj(Ghh[G][i][k]) Ghp[G][l][c]
+    Contraction c; c.M = o * o; c.N = o * v; c.K = G; c.Mi = o; c.Ni = v;
+    c.A = vw(Ghh, 1, o, 0, o * o);
+    c.B = vw(Ghp, 0, o * v, v, 1);
+    c.C = vw(Vhhhp_, o * o * v, v, o * v, 1);
+    zgemm(c, G * o * o, gph, o3v, true, false);
+  }
+  {  // Vh2[i][c][k][l] = 2 V_klic - V_lkic
+    const int64_t dv[4] = {o, o, o, v};
+    const int pa[4] = {2, 3, 0, 1}, pb[4] = {2, 3, 1, 0};
+    zperm(Vh2_, o3v, Vhhhp_, o3v, dv, pa, 2.0, 0.0);
+    zperm(Vh2_, o3v, Vhhhp_, o3v, dv, pb, -1.0, 1.0);
+  }
+}
+
+void CcsdComplex::residual(const double* T, double* R) {
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o, D2 = D2_;
+  const int64_t pl = n1 + D2;  // imaginary plane of amplitude vectors
+  double* R1 = R;
+  double* R2 = R + n1;
+  if (!T) {  // Ccsd.cxx:404-409
+    ops::zero(R1, n1, s_);
+    ops::zero(R1 + pl, n1, s_);
+    ops::d2d(R2, Vd_, D2, s_);
+    ops::d2d(R2 + pl, Vd_ + D2, D2, s_);
+    return;
+  }
+  const bool ccd = opt_.ccd;
+  flops_ = 0.0;
+  double* t = cp(T);
+  double* Td = cp(T + n1);
+  double *Gpp = sys_.Gpp, *Gph = sys_.Gph, *Ghh = sys_.Ghh, *Ghp = sys_.Ghp;
+  const int64_t gpp = G * v * v, gph = G * n1, ghh = G * o * o, o4 = o * o * o * o,
+                o3v = o * o * o * v, gov = G * o * v;
+  const int64_t d4[4] = {v, o, v, o};
+  const int p_pp[4] = {0, 2, 1, 3};
+  const int p_ex[4] = {0, 3, 2, 1};
+
+  // ---- X = T2 + T1 T1 (Ccsd.cxx:460-461) ----------------------------------------
+  if (ccd) { ops::d2d(Xd_, Td, D2, s_); ops::d2d(Xd_ + D2, Td + pl, D2, s_); }
+  else ops::zrank1(Xd_, Xd_ + D2, Td, Td + pl, t, t + pl, 1.0, n1, s_);
+  zperm(Xp_, D2, Xd_, D2, d4, p_pp, 1.0, 0.0);
+  // ---- Kac, Kki (Ccsd.cxx:465-473) ---------------------------------------------
+  {
+    Contraction c; c.M = o; c.N = o; c.K = v * v * o; c.Ki = o;
+    c.A = vw(Vtc_, 0, o, o * o, 1); c.B = vw(Xp_, o * o, 1, 0, o); c.C = rm(Kki_, o);
+    zgemm(c, D2, D2, o * o);
+  }
+  {
+    Contraction c; c.M = v; c.N = v; c.K = v * o * o;
+    c.A = rm(Xp_, v * o * o); c.B = tr(Vtc_, v * o * o); c.C = rm(Kac_, v); c.alpha = -1.0;
+    zgemm(c, D2, D2, v * v);
+  }
+  // ---- Lac (Ccsd.cxx:468-470) ----------------------------------------------------
+  ops::d2d(Lac_, Kac_, 2 * v * v, s_);
+  if (!ccd) {
+    {  // jG[G] = sum_{k,d} Ghp[G][k][d] t[d][k]
+      Contraction c; c.M = G; c.N = 1; c.K = n1; c.Ki = v;
+      c.A = vw(Ghp, 0, n1, v, 1); c.B = vw(t, 1, o, 0, 0); c.C = vw(jG_, 0, 1, 0, 0);
+      zgemm(c, gph, pl, G);
+    }
+    {  // Lac[a][c] += 2 sum_G conj(Gpp[G][c][a]) jG[G]
+      Contraction c; c.M = v * v; c.N = 1; c.K = G; c.Mi = v;
+      c.A = vw(Gpp, v, 1, 0, v * v); c.B = vw(jG_, 0, 1, 0, 0); c.C = vw(Lac_, 1, v, 0, 0);
+      c.alpha = 2.0; c.beta = 1.0;
+      zgemm(c, gpp, G, v * v, true, false);
+    }
+    {  // U[G][a][k] = sum_d conj(Gpp[G][d][a]) t[d][k]
+      Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(tr(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(U_, o), n1);
+      zgemm(c, gpp, pl, gph, true, false);
+    }
+    {  // Lac[a][c] -= sum_{G,k} U[G][a][k] Ghp[G][k][c]
+      Contraction c; c.M = v; c.N = v; c.K = G * o; c.Ki = o;
+      c.A = vw(U_, 0, o, n1, 1); c.B = vw(Ghp, o * v, v, 0, 1); c.C = rm(Lac_, v);
+      c.alpha = -1.0; c.beta = 1.0;
+      zgemm(c, gph, gph, v * v);
+    }
+  }
+  // ---- Lki (Ccsd.cxx:476-478) ----------------------------------------------------
+  ops::d2d(Lki_, Kki_, 2 * o * o, s_);
+  if (!ccd) {
+    Contraction c; c.M = o * o; c.N = 1; c.K = v * o; c.Mi = o; c.Ki = o;
+    c.A = vw(Vh2_, v * o * o, o, o * o, 1); c.B = vw(t, o, 1, 0, 0); c.C = vw(Lki_, 1, o, 0, 0);
+    c.beta = 1.0;
+    zgemm(c, o3v, pl, o * o);
+  }
+  // ---- R2 = Lac T2 - Lki T2 (Ccsd.cxx:481-484) ------------------------------------
+  {
+    Contraction c; c.M = v; c.N = o * n1; c.K = v;
+    c.A = rm(Lac_, v); c.B = rm(Td, o * n1); c.C = rm(R2, o * n1);
+    zgemm(c, v * v, pl, pl);
+  }
+  {
+    Contraction c; c.M = o; c.N = n1; c.K = o; c.batch = v;
+    c.A = tr(Lki_, o); c.B = with_batch(rm(Td, n1), o * n1); c.C = with_batch(rm(R2, n1), o * n1);
+    c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, o * o, pl, pl);
+  }
+  // ---- T1-dressed vertex terms (Ccsd.cxx:487-491) -------------------------------
+  {
+    const int64_t dg[4] = {1, G, o, v};
+    const int pt[4] = {0, 1, 3, 2};
+    zperm(cTdGph_, gph, Ghp, gph, dg, pt, 1.0, 0.0, true);  // conj(Ghp[G][i][a]) -> [G][a][i]
+  }
+  ops::d2d(dGhh_, Ghh, 2 * ghh, s_);
+  if (!ccd) {
+    {  // cTdGph[G][a][i] -= sum_k t[a][k] conj(Ghh[G][i][k])
+      Contraction c; c.M = v; c.N = o; c.K = o; c.batch = G;
+      c.A = rm(t, o); c.B = with_batch(tr(Ghh, o), o * o); c.C = with_batch(rm(cTdGph_, o), n1);
+      c.alpha = -1.0; c.beta = 1.0;
+      zgemm(c, pl, ghh, gph, false, true);
+    }
+    {  // W[G][b][j] = sum_c Gpp[G][b][c] t[c][j]
+      Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(rm(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(W_, o), n1);
+      zgemm(c, gpp, pl, gph);
+    }
+    {  // R2 += cTdGph^T W
+      Contraction c; c.M = n1; c.N = n1; c.K = G;
+      c.A = tr(cTdGph_, n1); c.B = rm(W_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+      zgemm(c, gph, gph, pl);
+    }
+    {  // dGhh[G][k][i] += sum_d Ghp[G][k][d] t[d][i]
+      Contraction c; c.M = o; c.N = o; c.K = v; c.batch = G;
+      c.A = with_batch(rm(Ghp, v), o * v); c.B = rm(t, o); c.C = with_batch(rm(dGhh_, o), o * o);
+      c.beta = 1.0;
+      zgemm(c, gph, pl, ghh);
+    }
+    {  // SQ[G][b][j] = sum_k t[b][k] dGhh[G][k][j]
+      Contraction c; c.M = v; c.N = o; c.K = o; c.batch = G;
+      c.A = rm(t, o); c.B = with_batch(rm(dGhh_, o), o * o); c.C = with_batch(rm(SQ_, o), n1);
+      zgemm(c, pl, ghh, gph);
+    }
+    {  // R2 -= sum_G conj(Ghp[G][i][a]) SQ[G][b][j]   (Vphhh T1 + Vphhp T1 T1)
+      Contraction c; c.M = n1; c.N = n1; c.K = G; c.Mi = o;
+      c.A = vw(Ghp, 1, v, 0, n1); c.B = rm(SQ_, n1); c.C = vw(R2, o * n1, n1, 0, 1);
+      c.alpha = -1.0; c.beta = 1.0;
+      zgemm(c, gph, gph, pl, true, false);
+    }
+  }
+  // ---- ring Xakic (Ccsd.cxx:494-502) -----------------------------------------------
+  zperm(Te_, D2, Td, pl, d4, p_ex, 1.0, 0.0);
+  if (ccd) { ops::d2d(W8_, Td, D2, s_); ops::d2d(W8_ + D2, Td + pl, D2, s_); }
+  else ops::zrank1(W8_, W8_ + D2, Td, Td + pl, t, t + pl, 2.0, n1, s_);
+  zperm(Y_, D2, W8_, D2, d4, p_ex, 1.0, 0.0);  // (T2 + 2 T1 T1)^x
+  if (!ccd) {  // cTdGph[G][a][i] += sum_d conj(Gpp[G][d][a]) t[d][i]
+    Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
+    c.A = with_batch(tr(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(cTdGph_, o), n1);
+    c.beta = 1.0;
+    zgemm(c, gpp, pl, gph, true, false);
+  }
+  {  // cTdGph -= 1/2 sum_{dl} conj(Gph[G][d][l]) Y_dail
+    Contraction c; c.M = G; c.N = n1; c.K = n1;
+    c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(cTdGph_, n1); c.alpha = -0.5; c.beta = 1.0;
+    zgemm(c, gph, D2, gph, true, false);
+  }
+  ops::axpby(Y_, 2.0, Td, -1.0, Te_, 0.0, D2, s_);            // Y = 2T - T^x
+  ops::axpby(Y_ + D2, 2.0, Td + pl, -1.0, Te_ + D2, 0.0, D2, s_);
+  {  // W1[G][(b,j)] = sum_{c,k} Ghp[G][k][c] Y[(c,k),(b,j)]
+    Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
+    c.A = vw(Ghp, 0, n1, 1, v); c.B = vw(Y_, o * n1, n1, 0, 1); c.C = rm(W1_, n1);
+    zgemm(c, gph, D2, gph);
+  }
+  {  // R2 += cTdGph^T W1
+    Contraction c; c.M = n1; c.N = n1; c.K = G;
+    c.A = tr(cTdGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+    zgemm(c, gph, gph, pl);
+  }
+  {  // EX = T M2^T ;  R2 += EX Y
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(Td, n1); c.B = tr(M2_, n1); c.C = rm(EX_, n1);
+    zgemm(c, pl, D2, D2);
+    Contraction d; d.M = n1; d.N = n1; d.K = n1;
+    d.A = rm(EX_, n1); d.B = rm(Y_, n1); d.C = rm(R2, n1); d.beta = 1.0;
+    zgemm(d, D2, D2, pl);
+  }
+  // ---- crossed ring Xakci (Ccsd.cxx:509-517) ----------------------------------------
+  {
+    const int64_t dg[4] = {1, G, v, v};
+    const int pt[4] = {0, 1, 3, 2};
+    zperm(cTdGpp_, gpp, Gpp, gpp, dg, pt, 1.0, 0.0, true);  // conj(Gpp[G][c][a]) -> [G][a][c]
+  }
+  if (!ccd) {  // cTdGpp[G][a][c] -= sum_l t[a][l] conj(Gph[G][c][l])
+    Contraction c; c.M = v; c.N = v; c.K = o; c.batch = G;
+    c.A = rm(t, o); c.B = with_batch(tr(Gph, o), n1); c.C = with_batch(rm(cTdGpp_, v), v * v);
+    c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, pl, gph, gpp, false, true);
+  }
+  {  // EX = -1/2 T^x M3^T
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(Te_, n1); c.B = tr(M3_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
+    zgemm(c, D2, D2, D2);
+  }
+  {  // EX[a][i][c][k] += sum_G cTdGpp[G][a][c] dGhh[G][k][i]
+    Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
+    c.A = vw(cTdGpp_, v, 1, 0, v * v); c.B = vw(dGhh_, 0, o * o, o, 1);
+    c.C = vw(EX_, o * n1, o, 1, n1); c.beta = 1.0;
+    zgemm(c, gpp, ghh, D2);
+  }
+  {  // R2 -= EX T
+    Contraction c; c.M = n1; c.N = n1; c.K = n1;
+    c.A = rm(EX_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1); c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, D2, pl, pl);
+  }
+  {  // R2_abij -= sum_ck T_ackj X_bkci   (exchange pairing)
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
+    c.A = vw(Te_, o * n1, n1, 0, 1); c.B = vw(EX_, 0, 1, o * n1, n1);
+    c.C = vw(R2, o * n1, 1, o, n1); c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, D2, D2, pl);
+  }
+  // ---- symmetrisation, +V (Ccsd.cxx:520,529) -----------------------------------
+  ops::symmetrize(R2, n1, s_);
+  ops::symmetrize(R2 + pl, n1, s_);
+  ops::axpby(R2, 1.0, R2, 1.0, Vd_, 0.0, D2, s_);
+  ops::axpby(R2 + pl, 1.0, R2 + pl, 1.0, Vd_ + D2, 0.0, D2, s_);
+  // ---- hole-hole ladder (Ccsd.cxx:534-546) ----------------------------------------
+  ops::d2d(Xkl1_, Vhhhh_, 2 * o4, s_);
+  if (!ccd) {
+    {
+      Contraction c; c.M = o * o * o; c.N = o; c.K = v;
+      c.A = rm(Vhhhp_, v); c.B = rm(t, o); c.C = rm(Xkl1_, o); c.beta = 1.0;
+      zgemm(c, o3v, pl, o4);
+    }
+    {
+      Contraction c; c.M = o * o; c.N = o; c.K = v; c.batch = o; c.Mi = o;
+      c.A = vw(Vhhhp_, o * v, v, 0, 1, 0, o * o * v); c.B = rm(t, o);
+      c.C = vw(Xkl1_, o * o * o, 1, 0, o, 0, o * o); c.beta = 1.0;
+      zgemm(c, o3v, pl, o4);
+    }
+  }
+  zperm(Tp_, D2, Td, pl, d4, p_pp, 1.0, 0.0);
+  {  // Xkl2[kl][ij] = sum_cd V_klcd X_cdij
+    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
+    c.A = rm(Vh4_, v * v); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
+    zgemm(c, D2, D2, o4);
+  }
+  {
+    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
+    c.A = vw(Xp_, v * o * o, o * o, 0, 1); c.B = vw(Xkl1_, 0, o * o, o, 1);
+    c.C = vw(R2, o * n1, o, n1, 1); c.beta = 1.0;
+    zgemm(c, D2, o4, pl);
+    c.A.p = opt_.ppl ? Tp_ : Xp_;
+    c.B.p = Xkl2_;
+    zgemm(c, D2, o4, pl);
+  }
+  // ---- particle-particle ladder (Ccsd.cxx:549-601) ---------------------------------
+  if (opt_.ppl) {
+    ops::d2d(dGpp_, Gpp, 2 * gpp, s_);
+    if (!ccd) {  // dGpp[G][a][b] -= sum_k t[a][k] Ghp[G][k][b]
+      Contraction c; c.M = v; c.N = v; c.K = o; c.batch = G;
+      c.A = rm(t, o); c.B = with_batch(rm(Ghp, v), o * v); c.C = with_batch(rm(dGpp_, v), v * v);
+      c.alpha = -1.0; c.beta = 1.0;
+      zgemm(c, pl, gph, gpp);
+    }
+    const int64_t s = slab_rows_, nb = (v + s - 1) / s, sz = s * s * v * v;
+    for (int64_t X = 0; X < nb; ++X)
+      for (int64_t Yb = 0; Yb <= X; ++Yb) {
+        const int64_t x0 = X * s, sx = std::min(s, v - x0);
+        const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
+        {
+          Contraction c; c.M = sx * v; c.N = sy * v; c.K = G; c.Mi = v; c.Ni = v;
+          c.A = vw(cTdGpp_ + x0 * v, v, 1, 0, v * v);
+          c.B = vw(dGpp_ + y0 * v, 0, v * v, v, 1);
+          c.C = vw(slab_, sy * v * v, v, v * v, 1);
+          zgemm(c, gpp, gpp, sz);
+        }
+        {
+          Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
+          c.A = vw(slab_, sy * v * v, v * v, 0, 1);
+          c.B = vw(Xp_, 0, o * o, o, 1);
+          c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
+          if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
+          c.beta = 1.0;
+          zgemm(c, sz, D2, pl);
+        }
+      }
+  }
+  if (ccd) {
+    ops::zero(R1, n1, s_);
+    ops::zero(R1 + pl, n1, s_);
+    profile_finish();
+    return;
+  }
+  // ---- singles (Ccsd.cxx:607-629) ------------------------------------------------------
+  {
+    Contraction c; c.M = v; c.N = o; c.K = v;
+    c.A = rm(Kac_, v); c.B = rm(t, o); c.C = rm(R1, o);
+    zgemm(c, v * v, pl, pl);
+    Contraction d; d.M = v; d.N = o; d.K = o;
+    d.A = rm(t, o); d.B = rm(Kki_, o); d.C = rm(R1, o); d.alpha = -1.0; d.beta = 1.0;
+    zgemm(d, pl, o * o, pl);
+  }
+  {  // kck[(c,k)] = sum_{d,l} Vtc[c][d][k][l] t[d][l]
+    Contraction c; c.M = n1; c.N = 1; c.K = n1; c.Mi = o; c.Ki = o;
+    c.A = vw(Vtc_, v * o * o, o, o * o, 1); c.B = vw(t, o, 1, 0, 0); c.C = vw(kck_, o, 1, 0, 0);
+    zgemm(c, D2, pl, n1);
+  }
+  {  // R1 += (2T - T^x) kck
+    Contraction c; c.M = n1; c.N = 1; c.K = n1;
+    c.A = rm(Y_, n1); c.B = vw(kck_, 0, 1, 0, 0); c.C = vw(R1, 0, 1, 0, 0); c.beta = 1.0;
+    zgemm(c, D2, n1, pl);
+  }
+  {  // R1 += t (kck^T t)
+    Contraction c; c.M = o; c.N = o; c.K = v;
+    c.A = tr(kck_, o); c.B = rm(t, o); c.C = rm(P1_, o);
+    zgemm(c, n1, pl, o * o);
+    Contraction d; d.M = v; d.N = o; d.K = o;
+    d.A = rm(t, o); d.B = rm(P1_, o); d.C = rm(R1, o); d.beta = 1.0;
+    zgemm(d, pl, o * o, pl);
+  }
+  {  // R1 += 2 sum_G conj(Ghp[G][i][a]) jG[G]   (2 Vphhp T1)
+    Contraction c; c.M = n1; c.N = 1; c.K = G; c.Mi = o;
+    c.A = vw(Ghp, 1, v, 0, n1); c.B = vw(jG_, 0, 1, 0, 0); c.C = vw(R1, o, 1, 0, 0);
+    c.alpha = 2.0; c.beta = 1.0;
+    zgemm(c, gph, G, pl, true, false);
+  }
+  {  // P[G][i][c] = sum_k Ghh[G][k][i] t[c][k];  R1[a][i] -= sum_{G,c} conj(Gpp[G][c][a]) P[G][i][c]
+    Contraction c; c.M = o; c.N = v; c.K = o; c.batch = G;
+    c.A = with_batch(tr(Ghh, o), o * o); c.B = tr(t, o); c.C = with_batch(rm(P_, v), o * v);
+    zgemm(c, ghh, pl, gov);
+    Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
+    d.A = vw(Gpp, 0, 1, v * v, v); d.B = vw(P_, o * v, 1, 0, v); d.C = rm(R1, o);
+    d.alpha = -1.0; d.beta = 1.0;
+    zgemm(d, gpp, gov, pl, true, false);
+  }
+  {  // F = Ghp' (2X - X^x);  R1[a][i] += sum_{G,x} conj(Gpp[G][x][a]) F[G][x][i]
+    zperm(W8_, D2, Xd_, D2, d4, p_ex, 1.0, 0.0);
+    ops::axpby(W8_, 2.0, Xd_, -1.0, W8_, 0.0, D2, s_);
+    ops::axpby(W8_ + D2, 2.0, Xd_ + D2, -1.0, W8_ + D2, 0.0, D2, s_);
+    Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
+    c.A = vw(Ghp, 0, n1, 1, v); c.B = vw(W8_, o * n1, n1, 0, 1); c.C = rm(F_, n1);
+    zgemm(c, gph, D2, gph);
+    Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
+    d.A = vw(Gpp, 0, 1, v * v, v); d.B = vw(F_, n1, o, 0, 1); d.C = rm(R1, o); d.beta = 1.0;
+    zgemm(d, gpp, gph, pl, true, false);
+  }
+  {  // R1 -= Xp Vh2^T
+    Contraction c; c.M = v; c.N = o; c.K = v * o * o;
+    c.A = rm(Xp_, v * o * o); c.B = tr(Vh2_, v * o * o); c.C = rm(R1, o);
+    c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, D2, o3v, pl);
+  }
+  profile_finish();
+}
+
+}  // namespace cc4s_b200

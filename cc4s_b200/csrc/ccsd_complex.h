@@ -1,0 +1,60 @@
+// Complex-path CCSD / CCD residual (cc4s Ccsd<Complex>::getResiduum) on one B200.
+//
+// Complex tensors are stored as two planes (real plane, then imaginary plane);
+// every complex contraction runs as four real FP64 tensor-core contractions,
+// with conjugation folded into the sign of the imaginary-plane terms.
+#pragma once
+
+#include "ccsd_real.h"
+#include "schedule.h"
+
+namespace cc4s_b200 {
+
+// Device-resident inputs of the complex path (planar complex, im plane at +size).
+struct ComplexSystem {
+  int64_t o = 0, v = 0, G = 0;
+  double* eh = nullptr;
+  double* ep = nullptr;
+  double* Gpp = nullptr;  // [G][v][v]
+  double* Gph = nullptr;  // [G][v][o]
+  double* Ghh = nullptr;  // [G][o][o]
+  double* Ghp = nullptr;  // [G][o][v]
+};
+
+class CcsdComplex : public Schedule {
+ public:
+  CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Stream s);
+
+  void residual(const double* T, double* R) override;
+  const double* Vd() const override { return Vd_; }
+  const double* Ve() const override { return Ven_; }
+  const double* Vd_im() const override { return Vd_ + D2_; }
+  const double* Ve_im() const override { return Ven_ + D2_; }
+
+ private:
+  // C = alpha * op(A) op(B) + beta * C on complex planar operands; the
+  // imaginary plane of each operand sits at the given element offset
+  // (0: the operand is real).  conjA/conjB conjugate the operand.
+  void zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA = false,
+             bool conjB = false);
+  void zperm(double* dst, int64_t dst_im, const double* src, int64_t src_im, const int64_t d[4],
+             const int p[4], double alpha, double beta, bool conj = false);
+  void zaxpby(double* out, double a, const double* x, double b, const double* y, int64_t n);
+  void build_integrals();
+
+  ComplexSystem sys_;
+  RealOptions opt_;
+  int64_t D2_ = 0;
+  double *Vd_ = nullptr, *Ven_ = nullptr, *Vh4_ = nullptr, *Vtc_ = nullptr, *M2_ = nullptr,
+         *M3_ = nullptr, *Vhhhh_ = nullptr, *Vhhhp_ = nullptr, *Vh2_ = nullptr;
+  double *Xd_ = nullptr, *Xp_ = nullptr, *Te_ = nullptr, *Y_ = nullptr, *W8_ = nullptr,
+         *Tp_ = nullptr, *EX_ = nullptr;
+  double *Kki_ = nullptr, *Kac_ = nullptr, *Lac_ = nullptr, *Lki_ = nullptr, *jG_ = nullptr,
+         *U_ = nullptr, *cTdGph_ = nullptr, *W_ = nullptr, *SQ_ = nullptr, *W1_ = nullptr,
+         *F_ = nullptr, *cTdGpp_ = nullptr, *dGpp_ = nullptr, *dGhh_ = nullptr,
+         *Xkl1_ = nullptr, *Xkl2_ = nullptr, *kck_ = nullptr, *P1_ = nullptr, *P_ = nullptr,
+         *slab_ = nullptr;
+  int64_t slab_rows_ = 0;
+};
+
+}  // namespace cc4s_b200

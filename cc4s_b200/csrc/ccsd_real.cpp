@@ -30,26 +30,8 @@
 
 namespace cc4s_b200 {
 
-namespace {
-View vw(double* p, int64_t s_ro, int64_t s_ri, int64_t s_co, int64_t s_ci, int64_t s_bo = 0,
-        int64_t s_bi = 0) {
-  View v;
-  v.p = p; v.s_ro = s_ro; v.s_ri = s_ri; v.s_co = s_co; v.s_ci = s_ci; v.s_bo = s_bo;
-  v.s_bi = s_bi;
-  return v;
-}
-inline double* cp(const double* p) { return const_cast<double*>(p); }
-}  // namespace
-
-double* CcsdReal::take(size_t elems) {
-  double* p = ops::alloc(elems);
-  owned_.push_back(p);
-  bytes_ += elems * sizeof(double);
-  return p;
-}
-
 CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
-    : sys_(sys), opt_(opt), s_(s) {
+    : Schedule(s), sys_(sys), opt_(opt) {
   const int64_t o = sys.o, v = sys.v, G = sys.G, n1 = v * o, D2 = n1 * n1;
   if (o <= 0 || v <= 0 || G <= 0) throw Error(ERR_BAD_SHAPE, "CcsdReal: empty dimension");
   try {
@@ -79,47 +61,12 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
     slab_rows_ = std::min(sl, v);
     if (opt.ppl) slab_ = take(slab_rows_ * slab_rows_ * v * v);
   } catch (...) {
-    for (double* p : owned_) ops::release(p);
-    owned_.clear();
+    release_all();
     throw;
   }
   count_flops_ = false;
   build_integrals();
   count_flops_ = true;
-}
-
-CcsdReal::~CcsdReal() {
-  for (void* e : ev_) ops::event_destroy(e);
-  for (double* p : owned_) ops::release(p);
-}
-
-void CcsdReal::gemm_(const Contraction& c) {
-  const double f = 2.0 * double(c.M) * double(c.N) * double(c.K) * double(c.batch);
-  if (count_flops_) flops_ += f;
-  if (profile_ && count_flops_) {
-    const size_t k = ev_flops_.size();
-    while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
-    ev_flops_.push_back(f);
-    ops::event_record(ev_[2 * k], s_);
-    gemm(c, s_, scratch_);
-    ops::event_record(ev_[2 * k + 1], s_);
-    return;
-  }
-  gemm(c, s_, scratch_);
-}
-
-void CcsdReal::profile_finish() {
-  if (!profile_) return;
-  Profile p;
-  for (size_t k = 0; k < ev_flops_.size(); ++k) {
-    const double sec = 1e-3 * ops::event_ms(ev_[2 * k], ev_[2 * k + 1]);
-    p.gemm_seconds += sec;
-    p.gemm_flops += ev_flops_[k];
-    if (ev_flops_[k] > p.top_flops) { p.top_flops = ev_flops_[k]; p.top_seconds = sec; }
-  }
-  p.launches = static_cast<int>(ev_flops_.size());
-  ev_flops_.clear();
-  prof_ = p;
 }
 
 // Iteration-independent integrals (VertexCoulombIntegrals.cxx:87-121).

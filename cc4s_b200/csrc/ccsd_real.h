@@ -1,9 +1,7 @@
 // Real-path CCSD / CCD residual (cc4s Ccsd<Real>::getResiduum) on one B200.
 #pragma once
 
-#include "ops.h"
-
-#include <vector>
+#include "schedule.h"
 
 namespace cc4s_b200 {
 
@@ -26,54 +24,20 @@ struct RealSystem {
   double* Ghp = nullptr;  // [G][o][v]  Gamma_G,i,a
 };
 
-class CcsdReal {
+class CcsdReal : public Schedule {
  public:
   CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s);
-  ~CcsdReal();
-  CcsdReal(const CcsdReal&) = delete;
-  CcsdReal& operator=(const CcsdReal&) = delete;
 
-  // R = residual(T).  T, R are amplitude vectors (ops::AmpShape, one plane);
-  // T == nullptr is the first iteration (R1 = 0, R2 = V_abij).
-  void residual(const double* T, double* R);
-
-  // Pair-layout integrals used by the energy: Vd = V_abij, Ve = V_baij.
-  const double* Vd() const { return Vd_; }
-  const double* Ve() const { return Ve_; }
-
-  // FP64-equivalent flops of one residual evaluation (this schedule).
-  double flops_per_residual() const { return flops_; }
-  size_t device_bytes() const { return bytes_; }
-
-  // Per-launch timing of the tensor-core contractions (CUDA events around each
-  // launch).  Off by default; when on, residual() synchronises at its end.
-  void set_profile(bool on) { profile_ = on; }
-  struct Profile {
-    double gemm_seconds = 0, gemm_flops = 0;      // all contractions of the last residual
-    double top_seconds = 0, top_flops = 0;        // the most expensive single launch
-    int launches = 0;
-  };
-  const Profile& profile() const { return prof_; }
+  void residual(const double* T, double* R) override;
+  const double* Vd() const override { return Vd_; }
+  const double* Ve() const override { return Ve_; }
 
  private:
-  void gemm_(const Contraction& c);
-  double* take(size_t elems);
   void build_integrals();
   void ppl(const double* Xp, double* R2, const double* dGpp);
 
   RealSystem sys_;
   RealOptions opt_;
-  Stream s_;
-  GemmScratch scratch_;
-  std::vector<double*> owned_;
-  size_t bytes_ = 0;
-  double flops_ = 0.0;
-  bool count_flops_ = true;
-  bool profile_ = false;
-  Profile prof_;
-  std::vector<void*> ev_;          // event pool: 2 per profiled launch
-  std::vector<double> ev_flops_;
-  void profile_finish();
   // static integrals
   double *Vd_ = nullptr, *Ve_ = nullptr, *Vp_ = nullptr, *Vtp_ = nullptr;
   double *Vhhhh_ = nullptr, *Vhhhp_ = nullptr, *Vh2_ = nullptr;

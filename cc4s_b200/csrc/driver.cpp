@@ -69,15 +69,51 @@ void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, in
     if (!std::isfinite(gamma[k])) throw Error(ERR_NON_FINITE, "non-finite Coulomb vertex");
     if (is_complex && (k & 1) && gamma[k] != 0.0) has_imag = true;
   }
-  if (!half_grid)
-    throw Error(ERR_UNSUPPORTED, "the complex integral path is not available in this build");
   free_state();
   for (double* p : vertex) ops::release(p);
   vertex.clear();
+  auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
+  if (!half_grid) {
+    // Complex path: planar complex slices (imaginary plane at +size, zero for real input).
+    ComplexSystem cs;
+    cs.o = No; cs.v = Nv; cs.G = NG;
+    cs.eh = vtake(No); cs.ep = vtake(Nv);
+    const int64_t spp = NG * Nv * Nv, sph = NG * Nv * No, shh = NG * No * No;
+    cs.Gpp = vtake(2 * spp); cs.Gph = vtake(2 * sph); cs.Ghh = vtake(2 * shh); cs.Ghp = vtake(2 * sph);
+    ops::h2d(cs.eh, eps_h, No, stream);
+    ops::h2d(cs.ep, eps_p, Nv, stream);
+    double* staging = ops::alloc(nin);
+    try {
+      ops::h2d(staging, gamma, nin, stream);
+      const int parts = is_complex ? 2 : 1;
+      for (int part = 0; part < 2; ++part) {
+        if (part >= parts) {
+          ops::zero(cs.Gpp + spp, spp, stream); ops::zero(cs.Gph + sph, sph, stream);
+          ops::zero(cs.Ghh + shh, shh, stream); ops::zero(cs.Ghp + sph, sph, stream);
+          break;
+        }
+        ops::gather_vertex(cs.Gpp + part * spp, staging, is_complex, part, NG, Np, No, Nv, No, Nv, stream);
+        ops::gather_vertex(cs.Gph + part * sph, staging, is_complex, part, NG, Np, No, Nv, 0, No, stream);
+        ops::gather_vertex(cs.Ghh + part * shh, staging, is_complex, part, NG, Np, 0, No, 0, No, stream);
+        ops::gather_vertex(cs.Ghp + part * sph, staging, is_complex, part, NG, Np, 0, No, No, Nv, stream);
+      }
+      ops::sync(stream);
+    } catch (...) {
+      ops::release(staging);
+      throw;
+    }
+    ops::release(staging);
+    csys = cs;
+    sys = RealSystem();
+    sys.o = No; sys.v = Nv; sys.G = NG; sys.eh = cs.eh; sys.ep = cs.ep;
+    shape = ops::AmpShape{No, Nv, 2};
+    complex_path = true;
+    allocate_state();
+    return;
+  }
   // Real path: stack Re and (if present) Im rows into one real auxiliary index.
   const int64_t parts = has_imag ? 2 : 1;
   const int64_t G = NG * parts;
-  auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
   RealSystem rs;
   rs.o = No; rs.v = Nv; rs.G = G;
   rs.eh = vtake(No); rs.ep = vtake(Nv);
@@ -113,7 +149,11 @@ void Handle::allocate_state() {
   RealOptions ro;
   ro.ccd = opt.method == CC4S_METHOD_CCD;
   ro.ppl = opt.ppl != 0;
-  solver.reset(new CcsdReal(sys, ro, stream));
+  // Real path: the ladder is symmetric under (a,c) <-> (b,d), so its slab size is a
+  // free memory/performance choice.  Complex path: slices follow integralsSliceSize.
+  if (complex_path) ro.slab = opt.integrals_slice_size;
+  if (complex_path) solver.reset(new CcsdComplex(csys, ro, stream));
+  else solver.reset(new CcsdReal(sys, ro, stream));
   solver->set_profile(opt.profile != 0);
   const int64_t n = shape.total();
   Tcur = take(n);

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/cc4s_cc.h"
+#include "ccsd_complex.h"
 #include "ccsd_real.h"
 #include "ops.h"
 
@@ -39,11 +40,12 @@ struct Handle {
   std::string error;
 
   RealSystem sys;
+  ComplexSystem csys;
   ops::AmpShape shape{0, 0, 1};
   bool complex_path = false;
   std::vector<double*> vertex;  // device inputs (vertex slices, energies)
   std::vector<double*> state;   // amplitudes, DIIS history, scalars
-  std::unique_ptr<CcsdReal> solver;
+  std::unique_ptr<Schedule> solver;
 
   double* Tcur = nullptr;   // current amplitudes (mixer output)
   double* Rbuf = nullptr;   // residual

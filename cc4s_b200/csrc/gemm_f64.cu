@@ -1,10 +1,13 @@
-// FP64 DMMA contraction kernel (mma.sync.m16n8k4.f64) with cp.async staging.
+// FP64 DMMA contraction kernel (mma.sync.m16n8k16.f64) with cp.async staging.
 //
-// Tile 128 (m) x 128 (n) x 16 (k), 256 threads = 8 warps in a 2 x 4 grid,
-// each warp owns a 64 x 32 sub-tile = 4 x 4 MMA tiles of 16 x 8.
-// Operand tiles are staged through a 3-stage cp.async ring in shared memory.
+// Tile 128 (m) x 128 (n) x 32 (k), 256 threads = 8 warps in a 2 x 4 grid,
+// each warp owns a 64 x 32 sub-tile = 4 x 4 MMA tiles of 16 x 8.  Operand
+// tiles are staged through a 3-stage cp.async ring in shared memory (212 KB).
 // Shared-memory rows are padded by 4 doubles so that the fragment reads of
 // both storage orders ([m][k] and [k][m]) are free of bank conflicts.
+// Address arithmetic is kept off the critical path: offsets of the m / n
+// tile rows are computed once per tile, k offsets with 32-bit division once
+// per thread and k-tile, then stepped incrementally.
 #include "gemm_f64.cuh"
 
 #include <algorithm>
@@ -14,16 +17,17 @@ namespace cc4s_b200 {
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 256;
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
 
 static std::atomic<uint64_t> g_launches{0};
 
+// One index of an operand, split as x = (x / inner) * s_o + (x % inner) * s_i.
 struct Axis {
-  int64_t inner;   // inner extent of the two-level split
+  uint32_t inner;
   int64_t s_o, s_i;
-  __device__ __forceinline__ int64_t off(int64_t x) const {
-    int64_t o = x / inner;
-    return o * s_o + (x - o * inner) * s_i;
+  __device__ __forceinline__ int64_t off(uint32_t x) const {
+    const uint32_t o = x / inner;
+    return static_cast<int64_t>(o) * s_o + static_cast<int64_t>(x - o * inner) * s_i;
   }
 };
 
@@ -50,49 +54,90 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// A tile stored S[u][w] (w contiguous in shared memory, row length W + 4).
-// u runs over the operand's strided tile axis, w over its contiguous one.
-template <int U, int W, int V>
-__device__ __forceinline__ void load_tile(double* S, const double* base, int tid,
-                                          int64_t u0, int64_t uext, const Axis& au,
-                                          int64_t w0, int64_t wext, const Axis& aw) {
-  constexpr int LD = W + 4;
-  constexpr int WCH = W / V;              // chunks per smem row
-  constexpr int PER = (U * W / V) / THREADS;
-  static_assert((U * W / V) % THREADS == 0, "tile/threads");
-  static_assert(THREADS % WCH == 0, "row split");
-  const int wl = (tid % WCH) * V;
-  const int64_t w = w0 + wl;
-  const bool wok = w < wext;
-  const int64_t woff = wok ? aw.off(w) : 0;
-#pragma unroll
-  for (int r = 0; r < PER; ++r) {
-    const int ul = tid / WCH + r * (THREADS / WCH);
-    const int64_t u = u0 + ul;
-    const bool ok = wok && (u < uext);
-    const double* g = ok ? base + au.off(u) + woff : base;
-    double* sp = S + ul * LD + wl;
-    if (V == 2) cp_async16(sp, g, ok); else cp_async8(sp, g, ok);
-  }
-}
+// Loader of one operand tile stored S[u][w] (w contiguous in shared memory,
+// row length W + 4).  One of (u, w) is the k index, the other is m or n.
+// KU: the strided tile axis u is k; otherwise w is k.
+template <int U, int W, int V, bool KU>
+struct Loader {
+  static constexpr int LD = W + 4;
+  static constexpr int WCH = W / V;               // chunks per smem row
+  static constexpr int RP = THREADS / WCH;        // rows per pass
+  static constexpr int PER = U / RP;              // passes
+  static_assert((U * W / V) % THREADS == 0 && THREADS % WCH == 0, "tile split");
+  // fixed part (the m / n index)
+  int64_t fix[KU ? 1 : PER];
+  bool fok[KU ? 1 : PER];
+  int wl, ul0;
 
-__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  __device__ __forceinline__ void init(int tid, int64_t f0, int64_t fext, const Axis& af) {
+    wl = (tid % WCH) * V;
+    ul0 = tid / WCH;
+    if (KU) {
+      const int64_t x = f0 + wl;
+      fok[0] = x < fext;
+      fix[0] = fok[0] ? af.off(static_cast<uint32_t>(x)) : 0;
+    } else {
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const int64_t x = f0 + ul0 + r * RP;
+        fok[r] = x < fext;
+        fix[r] = fok[r] ? af.off(static_cast<uint32_t>(x)) : 0;
+      }
+    }
+  }
+
+  __device__ __forceinline__ void load(double* S, const double* base, int64_t k0, int64_t kend,
+                                       const Axis& ak) const {
+    if (KU) {
+      // u = k varies with r: step (ko, ki) incrementally by RP
+      uint32_t k = static_cast<uint32_t>(k0 + ul0);
+      uint32_t ko = k / ak.inner, ki = k - ko * ak.inner;
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const bool ok = fok[0] && (static_cast<int64_t>(k) < kend);
+        const double* g = ok ? base + static_cast<int64_t>(ko) * ak.s_o +
+                                   static_cast<int64_t>(ki) * ak.s_i + fix[0]
+                             : base;
+        double* sp = S + (ul0 + r * RP) * LD + wl;
+        if (V == 2) cp_async16(sp, g, ok); else cp_async8(sp, g, ok);
+        k += RP;
+        ki += RP;
+        while (ki >= ak.inner) { ki -= ak.inner; ++ko; }
+      }
+    } else {
+      const int64_t k = k0 + wl;
+      const bool kok = k < kend;
+      const int64_t koff = kok ? ak.off(static_cast<uint32_t>(k)) : 0;
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const bool ok = kok && fok[r];
+        const double* g = ok ? base + fix[r] + koff : base;
+        double* sp = S + (ul0 + r * RP) * LD + wl;
+        if (V == 2) cp_async16(sp, g, ok); else cp_async8(sp, g, ok);
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
-      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-      "{%0,%1,%2,%3};\n"
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-      : "d"(a0), "d"(a1), "d"(b0));
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 // A_KC: A tile stored [m][k]; otherwise [k][m].  B_NC: B tile stored [k][n]; otherwise [n][k].
 template <bool A_KC, bool B_NC, int VA, int VB>
 __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
   extern __shared__ __align__(16) double smem[];
-  constexpr int A_SIZE = A_KC ? BM * (BK + 4) : BK * (BM + 4);
-  constexpr int B_SIZE = B_NC ? BK * (BN + 4) : BN * (BK + 4);
+  using LA = Loader<A_KC ? BM : BK, A_KC ? BK : BM, VA, !A_KC>;
+  using LB = Loader<B_NC ? BK : BN, B_NC ? BN : BK, VB, B_NC>;
+  constexpr int A_SIZE = (A_KC ? BM : BK) * LA::LD;
+  constexpr int B_SIZE = (B_NC ? BK : BN) * LB::LD;
   constexpr int STAGE = A_SIZE + B_SIZE;
-  constexpr int ALD = A_KC ? (BK + 4) : (BM + 4);
-  constexpr int BLD = B_NC ? (BN + 4) : (BK + 4);
+  constexpr int ALD = LA::LD, BLD = LB::LD;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -107,8 +152,13 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
   const int64_t kbeg = split * p.ksplit_len;
   const int64_t kend = min(p.K, kbeg + p.ksplit_len);
 
-  const double* Ab = p.A + p.Ab.off(b);
-  const double* Bb = p.B + p.Bb.off(b);
+  const double* Ab = p.A + p.Ab.off(static_cast<uint32_t>(b));
+  const double* Bb = p.B + p.Bb.off(static_cast<uint32_t>(b));
+
+  LA la;
+  LB lb;
+  la.init(tid, m0, p.M, p.Am);
+  lb.init(tid, n0, p.N, p.Bn);
 
   double acc[4][4][4];
 #pragma unroll
@@ -124,11 +174,8 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
     double* As = smem + stage * STAGE;
     double* Bs = As + A_SIZE;
     const int64_t k0 = kbeg + kt * BK;
-    // Tiles never read past kend: the k extent passed is kend.
-    if (A_KC) load_tile<BM, BK, VA>(As, Ab, tid, m0, p.M, p.Am, k0, kend, p.Ak);
-    else      load_tile<BK, BM, VA>(As, Ab, tid, k0, kend, p.Ak, m0, p.M, p.Am);
-    if (B_NC) load_tile<BK, BN, VB>(Bs, Bb, tid, k0, kend, p.Bk, n0, p.N, p.Bn);
-    else      load_tile<BN, BK, VB>(Bs, Bb, tid, n0, p.N, p.Bn, k0, kend, p.Bk);
+    la.load(As, Ab, k0, kend, p.Ak);
+    lb.load(Bs, Bb, k0, kend, p.Bk);
   };
 
 #pragma unroll
@@ -148,28 +195,28 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
     const double* As = smem + (kt % STAGES) * STAGE;
     const double* Bs = As + A_SIZE;
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double a[4][2], bf[4];
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const int mr = wm + mt * 16 + g;
-        if (A_KC) {
-          a[mt][0] = As[mr * ALD + kk + t];
-          a[mt][1] = As[(mr + 8) * ALD + kk + t];
-        } else {
-          a[mt][0] = As[(kk + t) * ALD + mr];
-          a[mt][1] = As[(kk + t) * ALD + mr + 8];
-        }
-      }
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int nc = wn + nt * 8 + g;
-        bf[nt] = B_NC ? Bs[(kk + t) * BLD + nc] : Bs[nc * BLD + kk + t];
-      }
+    for (int kk = 0; kk < BK; kk += 16) {
+      double a[4][8], bf[4][4];
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt][0], a[mt][1], bf[nt]);
+        for (int q = 0; q < 8; ++q) {
+          const int mr = wm + mt * 16 + g + ((q & 1) << 3);
+          const int kc = kk + t + (q >> 1) * 4;
+          a[mt][q] = A_KC ? As[mr * ALD + kc] : As[kc * ALD + mr];
+        }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int nc = wn + nt * 8 + g;
+          const int kc = kk + t + q * 4;
+          bf[nt][q] = B_NC ? Bs[kc * BLD + nc] : Bs[nc * BLD + kc];
+        }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma16(acc[mt][nt], a[mt], bf[nt]);
     }
   }
   cp_wait<0>();
@@ -189,26 +236,38 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
         }
     return;
   }
-  double* Cb = p.C + p.Cb.off(b);
-  double* C2b = p.C2 ? p.C2 + p.C2b.off(b) : nullptr;
+  double* Cb = p.C + p.Cb.off(static_cast<uint32_t>(b));
+  double* C2b = p.C2 ? p.C2 + p.C2b.off(static_cast<uint32_t>(b)) : nullptr;
+  int64_t co[8], co2[8];
+#pragma unroll
+  for (int h = 0; h < 8; ++h) {  // column offsets: nt = h >> 1, parity h & 1
+    const int64_t n = n0 + wn + (h >> 1) * 8 + 2 * t + (h & 1);
+    co[h] = n < p.N ? p.Cn.off(static_cast<uint32_t>(n)) : 0;
+    co2[h] = (C2b && n < p.N) ? p.C2n.off(static_cast<uint32_t>(n)) : 0;
+  }
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
+    for (int hh = 0; hh < 2; ++hh) {
+      const int64_t m = m0 + wm + mt * 16 + g + hh * 8;
+      if (m >= p.M) continue;
+      const int64_t ro = p.Cm.off(static_cast<uint32_t>(m));
+      const int64_t ro2 = C2b ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t m = m0 + wm + mt * 16 + g + ((q >> 1) << 3);
-        const int64_t n = n0 + wn + nt * 8 + 2 * t + (q & 1);
-        if (m < p.M && n < p.N) {
-          const double v = p.alpha * acc[mt][nt][q];
-          double* c = Cb + p.Cm.off(m) + p.Cn.off(n);
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int par = 0; par < 2; ++par) {
+          const int64_t n = n0 + wn + nt * 8 + 2 * t + par;
+          if (n >= p.N) continue;
+          const double v = p.alpha * acc[mt][nt][hh * 2 + par];
+          double* c = Cb + ro + co[nt * 2 + par];
           *c = (p.beta != 0.0) ? v + p.beta * *c : v;
           if (C2b) {
-            double* c2 = C2b + p.C2m.off(m) + p.C2n.off(n);
+            double* c2 = C2b + ro2 + co2[nt * 2 + par];
             *c2 = (p.beta != 0.0) ? v + p.beta * *c2 : v;
           }
         }
-      }
+    }
 }
 
 // Fixed-order reduction of split-K partials, then the alpha/beta epilogue.
@@ -223,17 +282,23 @@ __global__ void splitk_reduce_kernel(KParams p) {
     const int64_t r = e - b * p.M * p.N;
     const int64_t m = r / p.N, n = r - (r / p.N) * p.N;
     const double v = p.alpha * s;
-    double* c = p.C + p.Cb.off(b) + p.Cm.off(m) + p.Cn.off(n);
+    double* c = p.C + p.Cb.off(static_cast<uint32_t>(b)) + p.Cm.off(static_cast<uint32_t>(m)) +
+                p.Cn.off(static_cast<uint32_t>(n));
     *c = (p.beta != 0.0) ? v + p.beta * *c : v;
     if (p.C2) {
-      double* c2 = p.C2 + p.C2b.off(b) + p.C2m.off(m) + p.C2n.off(n);
+      double* c2 = p.C2 + p.C2b.off(static_cast<uint32_t>(b)) +
+                   p.C2m.off(static_cast<uint32_t>(m)) + p.C2n.off(static_cast<uint32_t>(n));
       *c2 = (p.beta != 0.0) ? v + p.beta * *c2 : v;
     }
   }
 }
 
 inline Axis axis(int64_t inner, int64_t s_o, int64_t s_i) {
-  Axis a; a.inner = inner > 0 ? inner : 1; a.s_o = s_o; a.s_i = s_i; return a;
+  Axis a;
+  a.inner = static_cast<uint32_t>(inner > 0 ? inner : 1);
+  a.s_o = s_o;
+  a.s_i = s_i;
+  return a;
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
@@ -261,6 +326,9 @@ void gemm(const Contraction& g0, cudaStream_t s, const GemmScratch& ws) {
   Contraction g = g0;
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
   if (g.K < 0) throw Error(ERR_INVALID_ARGUMENT, "gemm: negative K");
+  const int64_t lim = int64_t(1) << 31;
+  if (g.M >= lim || g.N >= lim || g.K >= lim || g.batch >= lim)
+    throw Error(ERR_BAD_SHAPE, "gemm: extent beyond 2^31");
   const int64_t Mi = g.Mi > 0 ? g.Mi : g.M;
   const int64_t Ni = g.Ni > 0 ? g.Ni : g.N;
   const int64_t Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);

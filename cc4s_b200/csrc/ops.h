@@ -39,6 +39,9 @@ void axpby(double* out, double a, const double* x, double b, const double* y, do
 // out[r][c] = a*A[r][c] + b*t[r]*t[c] for an n x n matrix (A may alias out).
 void rank1(double* out, double a, const double* A, double b, const double* t, int64_t n,
            Stream s);
+// Complex planar version: out = A + b * t t^T (no conjugation); out may alias A.
+void zrank1(double* out_re, double* out_im, const double* A_re, const double* A_im,
+            const double* t_re, const double* t_im, double b, int64_t n, Stream s);
 // R <- R + R^T for an n x n matrix, in place.
 void symmetrize(double* R, int64_t n, Stream s);
 

@@ -127,6 +127,19 @@ __global__ void rank1_kernel(double* out, double a, const double* A, double b, c
   }
 }
 
+__global__ void zrank1_kernel(double* ore, double* oim, const double* are, const double* aim,
+                              const double* tre, const double* tim, double b, int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n, c = e - (e / n) * n;
+    const double xr = tre[r] * tre[c] - tim[r] * tim[c];
+    const double xi = tre[r] * tim[c] + tim[r] * tre[c];
+    ore[e] = are[e] + b * xr;
+    oim[e] = aim[e] + b * xi;
+  }
+}
+
 // R <- R + R^T on 32 x 32 tile pairs (I <= J).
 __global__ void symmetrize_kernel(double* R, int64_t n) {
   __shared__ double t1[32][33];
@@ -483,6 +496,14 @@ void rank1(double* out, double a, const double* A, double b, const double* t, in
            Stream s) {
   if (n <= 0) return;
   rank1_kernel<<<grid_for(n * n, 256), 256, 0, s>>>(out, a, A, b, t, n);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void zrank1(double* out_re, double* out_im, const double* A_re, const double* A_im,
+            const double* t_re, const double* t_im, double b, int64_t n, Stream s) {
+  if (n <= 0) return;
+  zrank1_kernel<<<grid_for(n * n, 256), 256, 0, s>>>(out_re, out_im, A_re, A_im, t_re, t_im, b, n);
   CC_LAUNCH_CHECK();
   count();
 }

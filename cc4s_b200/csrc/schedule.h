@@ -1,0 +1,66 @@
+// Common machinery of the residual schedules: device allocations, flop
+// accounting, split-K scratch and optional per-launch timing of contractions.
+#pragma once
+
+#include <vector>
+
+#include "ops.h"
+
+namespace cc4s_b200 {
+
+inline View vw(double* p, int64_t s_ro, int64_t s_ri, int64_t s_co, int64_t s_ci,
+               int64_t s_bo = 0, int64_t s_bi = 0) {
+  View v;
+  v.p = p; v.s_ro = s_ro; v.s_ri = s_ri; v.s_co = s_co; v.s_ci = s_ci; v.s_bo = s_bo;
+  v.s_bi = s_bi;
+  return v;
+}
+inline double* cp(const double* p) { return const_cast<double*>(p); }
+
+class Schedule {
+ public:
+  explicit Schedule(Stream s) : s_(s) {}
+  virtual ~Schedule();
+  Schedule(const Schedule&) = delete;
+  Schedule& operator=(const Schedule&) = delete;
+
+  // R = residual(T) on amplitude vectors (ops::AmpShape layout); T == nullptr is
+  // the first iteration (R1 = 0, R2 = V_abij).
+  virtual void residual(const double* T, double* R) = 0;
+  // Pair-layout integrals of the energy: Vd = V_abij, Ve = V_baij (imaginary
+  // planes null on the real path).
+  virtual const double* Vd() const = 0;
+  virtual const double* Ve() const = 0;
+  virtual const double* Vd_im() const { return nullptr; }
+  virtual const double* Ve_im() const { return nullptr; }
+
+  double flops_per_residual() const { return flops_; }
+  size_t device_bytes() const { return bytes_; }
+
+  void set_profile(bool on) { profile_ = on; }
+  struct Profile {
+    double gemm_seconds = 0, gemm_flops = 0;  // all contractions of the last residual
+    double top_seconds = 0, top_flops = 0;    // the most expensive single launch
+    int launches = 0;
+  };
+  const Profile& profile() const { return prof_; }
+
+ protected:
+  double* take(size_t elems);
+  void gemm_(const Contraction& c);
+  void profile_finish();
+  void release_all();
+
+  Stream s_;
+  GemmScratch scratch_;
+  std::vector<double*> owned_;
+  size_t bytes_ = 0;
+  double flops_ = 0.0;
+  bool count_flops_ = true;
+  bool profile_ = false;
+  Profile prof_;
+  std::vector<void*> ev_;
+  std::vector<double> ev_flops_;
+};
+
+}  // namespace cc4s_b200

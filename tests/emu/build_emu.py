@@ -6,12 +6,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 CSRC = os.path.join(ROOT, "cc4s_b200", "csrc")
 OUT = os.path.join(HERE, "_build", "libcc4s_emu.so")
+SCHEDULE_SOURCES = ("schedule.cpp", "ccsd_real.cpp", "ccsd_complex.cpp", "driver.cpp", "abi.cpp")
 
 
 def build():
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    srcs = [os.path.join(HERE, "ops_emu.cpp")] + [
-        os.path.join(CSRC, f) for f in ("ccsd_real.cpp", "driver.cpp", "abi.cpp")]
+    srcs = [os.path.join(HERE, "ops_emu.cpp")] + [os.path.join(CSRC, f) for f in SCHEDULE_SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "cc4s_cc.h"))
     if os.path.exists(OUT) and os.path.getmtime(OUT) > max(os.path.getmtime(d) for d in deps):

@@ -116,6 +116,19 @@ void rank1(double* out, double a, const double* A, double b, const double* t, in
     for (int64_t c = 0; c < n; ++c) out[r * n + c] = a * A[r * n + c] + b * t[r] * t[c];
 }
 
+void zrank1(double* ore, double* oim, const double* are, const double* aim, const double* tre,
+            const double* tim, double b, int64_t n, Stream) {
+  ++g_ops;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < n; ++c) {
+      const int64_t e = r * n + c;
+      const double xr = tre[r] * tre[c] - tim[r] * tim[c];
+      const double xi = tre[r] * tim[c] + tim[r] * tre[c];
+      ore[e] = are[e] + b * xr;
+      oim[e] = aim[e] + b * xi;
+    }
+}
+
 void symmetrize(double* R, int64_t n, Stream) {
   ++g_ops;
   for (int64_t r = 0; r < n; ++r)

@@ -86,3 +86,39 @@ def test_errors_are_reported(emu_lib):
     with pytest.raises(CoupledClusterError) as e:
         Solver({"method": "Ccsdt"}, lib=emu_lib)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("shape", [(3, 7, 5), (4, 9, 11)])
+@pytest.mark.parametrize("method", ["Ccsd", "Ccd"])
+def test_complex_residual_matches_oracle(emu_lib, shape, method):
+    """Complex integral path with a non-Hermitian vertex."""
+    from cc4s_b200 import Solver
+    No, Nv, NG = shape
+    rng = np.random.default_rng(100 + sum(shape))
+    g = (rng.standard_normal((NG, No + Nv, No + Nv)) + 1j * rng.standard_normal((NG, No + Nv, No + Nv))) * 0.1
+    s = inputs.System(np.sort(rng.uniform(-1.5, -.5, No)), np.sort(rng.uniform(.2, 3, Nv)), g, half_grid=False)
+    T1 = (rng.standard_normal((Nv, No)) + 1j * rng.standard_normal((Nv, No))) * 0.05
+    T2 = (rng.standard_normal((Nv, Nv, No, No)) + 1j * rng.standard_normal((Nv, Nv, No, No))) * 0.05
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    sol = Solver({"method": method}, lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    R1, R2 = sol.residual((T1, T2))
+    Q1, Q2 = ccsd.residuum((T1, T2), ccsd.CcsdInputs(s), ccd=(method == "Ccd"))
+    assert _rel(R2, Q2) < 1e-13
+    if method == "Ccsd":
+        assert _rel(R1, Q1) < 1e-13
+
+
+def test_ueg_reference_energies_through_product_schedule(emu_lib):
+    """The product's complex schedule and driver reproduce cc4s's own expected
+    UEG (rs=1, No=7, Nv=26) CCSD energies."""
+    import json
+    from cc4s_b200 import Solver
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ueg_rs1.0_7occ_26virt.json")))
+    s = inputs.ueg_system(7, 26, 1.0)
+    sol = Solver(g["ccsd"]["options"], lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    r = sol.run()
+    assert r["converged"]
+    for k, ref in g["ccsd"]["energy"].items():
+        assert abs(r[k] - ref) < 1e-10, (k, r[k], ref)

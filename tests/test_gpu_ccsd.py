@@ -106,3 +106,49 @@ def test_c1_size_independent_properties(Solver):
     T1, T2 = sol.amplitudes()
     assert _rel(T2.transpose(1, 0, 3, 2), T2) < 1e-12
     assert all(np.isfinite(h["energy"]) for h in r["history"])
+
+
+def test_ueg_reference_energies(Solver):
+    """cc4s's own expected CCSD energies of its UEG regression test
+    (test/tests/ueg/rs1.0-7occ-26virt), reproduced on the GPU."""
+    g = json.load(open(os.path.join(GOLDEN, "ueg_rs1.0_7occ_26virt.json")))
+    s = inputs.ueg_system(7, 26, 1.0)
+    sol = Solver(g["ccsd"]["options"])
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    r = sol.run()
+    assert r["converged"]
+    for k, ref in g["ccsd"]["energy"].items():
+        assert abs(r[k] - ref) < TOL_E, (k, r[k], ref)
+
+
+@pytest.mark.parametrize("shape,hermitian", [((3, 7, 5), False), ((6, 30, 40), True),
+                                             ((10, 64, 90), True)])
+def test_complex_residual_parity(Solver, shape, hermitian):
+    No, Nv, NG = shape
+    rng = np.random.default_rng(7 * No + Nv)
+    if hermitian:
+        s = inputs.synthetic_system(No, Nv, NG, complex=True, seed=No)
+    else:
+        g = (rng.standard_normal((NG, No + Nv, No + Nv)) + 1j * rng.standard_normal((NG, No + Nv, No + Nv))) * 0.1
+        s = inputs.System(np.sort(rng.uniform(-1.5, -.5, No)), np.sort(rng.uniform(.2, 3, Nv)), g, False)
+    T1 = (rng.standard_normal((Nv, No)) + 1j * rng.standard_normal((Nv, No))) * 0.02
+    T2 = (rng.standard_normal((Nv, Nv, No, No)) + 1j * rng.standard_normal((Nv, Nv, No, No))) * 0.02
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    sol = Solver({})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    R1, R2 = sol.residual((T1, T2))
+    Q1, Q2 = ccsd.residuum((T1, T2), ccsd.CcsdInputs(s))
+    assert _rel(R1, Q1) < TOL_RES and _rel(R2, Q2) < TOL_RES
+
+
+def test_complex_run(Solver):
+    s = inputs.synthetic_system(6, 30, 60, complex=True, seed=5)
+    o = dict(maxIterations=30, energyConvergence=1e-10, amplitudesConvergence=1e-8)
+    ref = coupled_cluster.run(s, **o)
+    sol = Solver(o)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    r = sol.run()
+    assert r["iterations"] == ref["iterations"]
+    assert abs(r["correlation"] - ref["energy"]["correlation"]) < TOL_E
+    T1, T2 = sol.amplitudes()
+    assert _rel(T2, ref["amplitudes"][1]) < TOL_AMP
