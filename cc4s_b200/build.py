@@ -7,7 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcc4s_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["gemm_f64.cu", "ops_cuda.cu", "schedule.cpp", "ccsd_real.cpp", "driver.cpp", "abi.cpp"]
+SOURCES = ["gemm_f64.cu", "split_gemm.cu", "ops_cuda.cu", "schedule.cpp", "ccsd_real.cpp",
+           "ccsd_complex.cpp", "driver.cpp", "abi.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]

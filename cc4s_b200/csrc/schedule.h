@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "ops.h"
+#include "split_gemm.cuh"
 
 namespace cc4s_b200 {
 
@@ -38,6 +39,11 @@ class Schedule {
   size_t device_bytes() const { return bytes_; }
 
   void set_profile(bool on) { profile_ = on; }
+  // 0: FP64 throughout; 3: the large ladder / ring / vertex contractions run as
+  // three-slice split-precision products on the tcgen05 tensor cores.
+  void set_precision(int slices) { precision_ = slices; }
+  // Non-zero if a bounded wait inside a tensor-core kernel expired (synchronises).
+  int device_error();
   struct Profile {
     double gemm_seconds = 0, gemm_flops = 0;  // all contractions of the last residual
     double top_seconds = 0, top_flops = 0;    // the most expensive single launch
@@ -48,7 +54,12 @@ class Schedule {
  protected:
   double* take(size_t elems);
   void gemm_(const Contraction& c);
+  // A large contraction: split precision when enabled (batch 1), else FP64.
+  void tc_(const Contraction& c);
   void profile_finish();
+  int precision_ = 0;
+  SplitScratch split_;
+  double* split_mem_ = nullptr;
   void release_all();
 
   Stream s_;

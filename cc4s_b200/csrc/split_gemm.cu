@@ -1,0 +1,486 @@
+// Split-precision FP64 contraction: FP16 integer slices on tcgen05 tensor cores.
+//
+// Kernel layout (one 128 x 128 output tile per CTA, 192 threads):
+//   warp 0      TMA producer: per k-block of 32, three A-slice and three
+//               B-slice tiles (128 x 32 FP16, 64-byte swizzle) into a 4-stage
+//               shared-memory ring, completion tracked by mbarriers;
+//   warp 1      allocates 512 TMEM columns; one thread issues tcgen05.mma
+//               (M=128, N=128, K=16) for the six slice products into three
+//               FP32 accumulators (TMEM columns 0, 128, 256) and commits to
+//               mbarriers that release smem stages and publish K chunks;
+//   warps 2..5  epilogue: after each K chunk, tcgen05.ld the three groups,
+//               recombine in FP64 with the row/column scales and add into C.
+// Every mbarrier wait is bounded; on expiry the kernel records an error flag
+// and every role leaves its loop, so the kernel always terminates.
+#include "split_gemm.cuh"
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <mutex>
+
+namespace cc4s_b200 {
+
+namespace {
+
+constexpr int TM = 128, TN = 128, TK = 32, NST = 4, NSLICE = 3;
+constexpr int KCHUNK = 4096;                      // exact FP32 span of the leading group
+constexpr int TILE_BYTES = TM * TK * 2;           // 8 KB per slice tile
+constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;
+constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t WAIT_LIMIT = 1u << 28;         // bounded mbarrier waits
+
+std::atomic<uint64_t> g_split_launches{0};
+
+struct Ax {
+  uint32_t inner;
+  int64_t s_o, s_i;
+  __host__ __device__ __forceinline__ int64_t off(uint32_t x) const {
+    const uint32_t o = x / inner;
+    return static_cast<int64_t>(o) * s_o + static_cast<int64_t>(x - o * inner) * s_i;
+  }
+};
+Ax mkax(int64_t inner, int64_t s_o, int64_t s_i) {
+  Ax a; a.inner = static_cast<uint32_t>(inner > 0 ? inner : 1); a.s_o = s_o; a.s_i = s_i; return a;
+}
+
+// ---------------------------------------------------------------------------
+// Packing: operand element (r, k) -> three FP16 integer slices P[q][r][k]
+// (row-padded to Rp, k-padded to Kp) and a per-row exponent.
+struct PackArgs {
+  const double* src;
+  Ax ar, ak;              // two-level index maps of the row and k indices
+  int64_t R, K, Rp, Kp;
+  unsigned long long* rmax;  // per-row max |x| as IEEE bits (non-negative doubles)
+  int* rexp;              // per-row exponent
+  __half* dst;            // [3][Rp][Kp]
+  int r_contig;           // 1: the row index is the contiguous one in memory
+};
+
+// Tile 32 rows x 32 k through shared memory; mode 0: row maxima, mode 1: slices.
+template <int MODE>
+__global__ void pack_kernel(PackArgs a) {
+  __shared__ double tile[32][33];
+  const int64_t tr = (a.Rp + 31) / 32, tk = (a.Kp + 31) / 32;
+  for (int64_t blk = blockIdx.x; blk < tr * tk; blk += gridDim.x) {
+    const int64_t r0 = (blk / tk) * 32, k0 = (blk % tk) * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+      // read: lanes along the contiguous index
+      int64_t r, k;
+      if (a.r_contig) { r = r0 + threadIdx.x; k = k0 + yy; }
+      else { r = r0 + yy; k = k0 + threadIdx.x; }
+      double v = 0.0;
+      if (r < a.R && k < a.K) v = a.src[a.ar.off(static_cast<uint32_t>(r)) + a.ak.off(static_cast<uint32_t>(k))];
+      if (a.r_contig) tile[threadIdx.x][yy] = v; else tile[yy][threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (MODE == 0) {
+      // row maxima: threads (x = k lane, y = row) reduce over k with warp shuffles
+      for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        double m = fabs(tile[rr][threadIdx.x]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        const int64_t r = r0 + rr;
+        if (threadIdx.x == 0 && r < a.R && m > 0.0)
+          atomicMax(&a.rmax[r], static_cast<unsigned long long>(__double_as_longlong(m)));
+      }
+    } else {
+      for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        const int64_t r = r0 + rr, k = k0 + threadIdx.x;
+        if (r >= a.Rp || k >= a.Kp) continue;
+        double x = tile[rr][threadIdx.x];
+        int e = 0;
+        if (r < a.R) {
+          const double m = __longlong_as_double(static_cast<long long>(a.rmax[r]));
+          if (m > 0.0) frexp(m, &e);
+          if (k == 0) a.rexp[r] = e;
+        }
+        x = ldexp(x, -e) * 64.0;                 // |x| <= 64
+        const double s1 = rint(x);
+        double t = (x - s1) * 2048.0;            // |t| <= 1024
+        const double s2 = rint(t);
+        t = (t - s2) * 2048.0;
+        const double s3 = rint(t);
+        const int64_t o = r * a.Kp + k, pl = a.Rp * a.Kp;
+        // integers of at most 11 bits: exact in FP32 and FP16
+        a.dst[o] = __float2half_rn(static_cast<float>(s1));
+        a.dst[o + pl] = __float2half_rn(static_cast<float>(s2));
+        a.dst[o + 2 * pl] = __float2half_rn(static_cast<float>(s3));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers (inline PTX for sm_100a).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar));
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Bounded wait for the phase with the given parity: gives up after
+// WAIT_LIMIT polls or 2 seconds, whichever comes first; returns false then.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    if (ok) return true;
+    if ((it & 1023) == 1023 && global_ns() - t0 > 2000000000ull) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];\n"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);        // start address
+  d |= static_cast<uint64_t>(1) << 16;                       // leading byte offset (16 B)
+  d |= static_cast<uint64_t>(512 >> 4) << 32;                // stride byte offset
+  d |= static_cast<uint64_t>(1) << 46;                       // descriptor version (sm100)
+  d |= static_cast<uint64_t>(4) << 61;                       // SWIZZLE_64B
+  return d;
+}
+// Instruction descriptor: D = F32, A = B = F16, both K-major, N = 128, M = 128.
+constexpr uint32_t IDESC = (1u << 4) | ((TN >> 3) << 17) | ((TM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+               ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+struct SplitParams {
+  int64_t M, N, K;                 // logical extents
+  int64_t Mp, Np;                  // padded row counts of the packed operands
+  int nkb;                         // k-blocks of TK
+  Ax Cm, Cn, C2m, C2n;
+  double* C; double* C2;
+  double alpha, beta;
+  const int* ea; const int* eb;    // row exponents of A (m) and of B (n)
+  int* error;
+};
+
+__global__ void __launch_bounds__(192, 1)
+split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+             SplitParams p) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned stage buffers, then barriers
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NST * STAGE_BYTES);
+  // bars[0..NST): full, [NST..2NST): empty, [2NST]: acc_full, [2NST+1]: acc_empty
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NST + 2);
+  __shared__ int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * TM, n0 = static_cast<int64_t>(blockIdx.x) * TN;
+  const int nchunks = (p.nkb * TK + KCHUNK - 1) / KCHUNK;
+  constexpr int KB_PER_CHUNK = KCHUNK / TK;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(smem_u32(&bars[s]), 1);
+      mbar_init(smem_u32(&bars[NST + s]), 1);
+    }
+    mbar_init(smem_u32(&bars[2 * NST]), 1);
+    mbar_init(smem_u32(&bars[2 * NST + 1]), 128);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_u32(tmem_slot)), "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    for (int kb = 0; kb < p.nkb; ++kb) {
+      const int s = kb % NST;
+      if (kb >= NST && !mbar_wait(smem_u32(&bars[NST + s]), ((kb / NST) - 1) & 1)) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      if (abort_flag) break;
+      const uint32_t full = smem_u32(&bars[s]);
+      mbar_expect_tx(full, STAGE_BYTES);
+      unsigned char* st = base + s * STAGE_BYTES;
+      for (int q = 0; q < NSLICE; ++q) {
+        tma_load_2d(smem_u32(st + q * TILE_BYTES), &tmA, full, kb * TK, static_cast<int>(q * p.Mp + m0));
+        tma_load_2d(smem_u32(st + (NSLICE + q) * TILE_BYTES), &tmB, full, kb * TK,
+                    static_cast<int>(q * p.Np + n0));
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    int kb = 0;
+    for (int c = 0; c < nchunks && !abort_flag; ++c) {
+      if (c > 0 && !mbar_wait(smem_u32(&bars[2 * NST + 1]), (c - 1) & 1)) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      const int kb_end = min(p.nkb, (c + 1) * KB_PER_CHUNK);
+      bool first = true;
+      for (; kb < kb_end; ++kb) {
+        const int s = kb % NST;
+        if (!mbar_wait(smem_u32(&bars[s]), (kb / NST) & 1)) { atomicExch(&abort_flag, 1); break; }
+        tc_fence_after();
+        const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < TK / 16; ++kk) {
+          // 32 bytes per 16-element K step inside the 64-byte swizzled rows
+          const uint32_t koff = kk * 32;
+          // group 0: (1,1); group 1: (1,2),(2,1); group 2: (1,3),(2,2),(3,1)
+#pragma unroll
+          for (int pa = 0; pa < NSLICE; ++pa)
+#pragma unroll
+            for (int pb = 0; pb < NSLICE; ++pb) {
+              if (pa + pb > NSLICE - 1) continue;
+              const int grp = pa + pb;
+              const uint64_t da = sdesc(st + pa * TILE_BYTES + koff);
+              const uint64_t db = sdesc(st + (NSLICE + pb) * TILE_BYTES + koff);
+              // the first product of each group in a chunk overwrites the accumulator
+              const bool init = first && kk == 0 && (pa == 0);
+              umma(tmem + grp * TN, da, db, init ? 0u : 1u);
+            }
+        }
+        umma_commit(smem_u32(&bars[NST + s]));  // stage free once these MMAs retire
+        first = false;
+      }
+      umma_commit(smem_u32(&bars[2 * NST]));    // chunk accumulators ready
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM -> FP64 recombination -> C ----
+    const int quad = warp & 3;                  // TMEM lanes 32*quad .. 32*quad+31
+    const int row = quad * 32 + lane;
+    const int64_t m = m0 + row;
+    const bool mok = m < p.M;
+    const double sa = mok ? ldexp(1.0, p.ea[m]) : 0.0;
+    const int64_t ro = mok ? p.Cm.off(static_cast<uint32_t>(m)) : 0;
+    const int64_t ro2 = (mok && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
+    for (int c = 0; c < nchunks; ++c) {
+      if (!mbar_wait(smem_u32(&bars[2 * NST]), c & 1)) { atomicExch(&abort_flag, 1); break; }
+      tc_fence_after();
+      const double w0 = 0x1p-12, w1 = 0x1p-23, w2 = 0x1p-34;
+      for (int cb = 0; cb < TN; cb += 32) {
+        uint32_t g0[32], g1[32], g2[32];
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + cb;
+        tmem_ld32(lane_addr, g0);
+        tmem_ld32(lane_addr + TN, g1);
+        tmem_ld32(lane_addr + 2 * TN, g2);
+        tmem_wait_ld();
+        if (mok) {
+#pragma unroll 4
+          for (int j = 0; j < 32; ++j) {
+            const int64_t n = n0 + cb + j;
+            if (n >= p.N) break;
+            const double v = (static_cast<double>(__uint_as_float(g0[j])) * w0 +
+                              static_cast<double>(__uint_as_float(g1[j])) * w1 +
+                              static_cast<double>(__uint_as_float(g2[j])) * w2) *
+                             sa * ldexp(1.0, p.eb[n]) * p.alpha;
+            const int64_t co = p.Cn.off(static_cast<uint32_t>(n));
+            double* cptr = p.C + ro + co;
+            const double prev = (c == 0) ? (p.beta != 0.0 ? p.beta * *cptr : 0.0) : *cptr;
+            *cptr = prev + v;
+            if (p.C2) {
+              double* c2 = p.C2 + ro2 + p.C2n.off(static_cast<uint32_t>(n));
+              const double prev2 = (c == 0) ? (p.beta != 0.0 ? p.beta * *c2 : 0.0) : *c2;
+              *c2 = prev2 + v;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(smem_u32(&bars[2 * NST + 1]));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicExch(p.error, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ---------------------------------------------------------------------------
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+  static EncodeFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeFn>(p);
+  });
+  if (!fn) throw Error(ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  return fn;
+}
+
+// 2-D map over packed slices [3*Rp][Kp] FP16, box 32 (k) x 128 (rows), 64-byte swizzle.
+CUtensorMap make_map(void* base, int64_t rows, int64_t Kp) {
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(Kp * 2)};
+  const cuuint32_t box[2] = {TK, 128};
+  const cuuint32_t es[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  return m;
+}
+
+inline int64_t rup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+struct Layout2 {
+  int64_t Mp, Np, Kp;
+  size_t a_bytes, b_bytes, meta_bytes;
+};
+Layout2 layout_of(const Contraction& g) {
+  Layout2 L;
+  L.Mp = rup(g.M, TM);
+  L.Np = rup(g.N, TN);
+  L.Kp = rup(std::max<int64_t>(g.K, 1), TK);
+  L.a_bytes = rup(static_cast<int64_t>(NSLICE * L.Mp * L.Kp * 2), 1024);
+  L.b_bytes = rup(static_cast<int64_t>(NSLICE * L.Np * L.Kp * 2), 1024);
+  L.meta_bytes = rup((L.Mp + L.Np) * (8 + 4), 1024);
+  return L;
+}
+
+void pack(const View& v, bool rows_are_m, const Contraction& g, int64_t R, int64_t Rp,
+          int64_t Kp, __half* dst, unsigned long long* rmax, int* rexp, cudaStream_t s) {
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  const int64_t Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);
+  PackArgs a;
+  a.src = v.p;
+  if (rows_are_m) {  // A(m, k): rows = m (s_ro, s_ri), k = cols (s_co, s_ci)
+    a.ar = mkax(Mi, v.s_ro, v.s_ri);
+    a.ak = mkax(Ki, v.s_co, v.s_ci);
+    a.r_contig = (v.s_ri == 1 && v.s_ci != 1) ? 1 : 0;
+  } else {           // B(k, n): rows of the packed operand = n (s_co, s_ci), k = (s_ro, s_ri)
+    a.ar = mkax(Ni, v.s_co, v.s_ci);
+    a.ak = mkax(Ki, v.s_ro, v.s_ri);
+    a.r_contig = (v.s_ci == 1 && v.s_ri != 1) ? 1 : 0;
+  }
+  a.R = R; a.K = g.K; a.Rp = Rp; a.Kp = Kp;
+  a.rmax = rmax; a.rexp = rexp; a.dst = dst;
+  CC_CHECK(cudaMemsetAsync(rmax, 0, R * sizeof(unsigned long long), s));
+  const int64_t tiles = ((Rp + 31) / 32) * ((Kp + 31) / 32);
+  const unsigned grid = static_cast<unsigned>(std::min<int64_t>(tiles, 148 * 64));
+  pack_kernel<0><<<grid, dim3(32, 8), 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  pack_kernel<1><<<grid, dim3(32, 8), 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+uint64_t split_launch_count() { return g_split_launches.load(); }
+
+size_t gemm_split_scratch_bytes(const Contraction& g) {
+  const Layout2 L = layout_of(g);
+  return L.a_bytes + L.b_bytes + L.meta_bytes;
+}
+
+void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
+  if (g.M <= 0 || g.N <= 0) return;
+  if (g.batch != 1) throw Error(ERR_UNSUPPORTED, "gemm_split: batched contraction");
+  if (g.K <= 0) throw Error(ERR_UNSUPPORTED, "gemm_split: empty K");
+  const Layout2 L = layout_of(g);
+  if (L.a_bytes + L.b_bytes + L.meta_bytes > ws.bytes) throw Error(ERR_OUT_OF_MEMORY, "gemm_split: scratch too small");
+  if (L.Mp * NSLICE >= (int64_t(1) << 31) || L.Np * NSLICE >= (int64_t(1) << 31) || L.Kp >= (int64_t(1) << 31))
+    throw Error(ERR_BAD_SHAPE, "gemm_split: extent too large");
+  unsigned char* p = static_cast<unsigned char*>(ws.p);
+  __half* Apk = reinterpret_cast<__half*>(p);
+  __half* Bpk = reinterpret_cast<__half*>(p + L.a_bytes);
+  unsigned char* meta = p + L.a_bytes + L.b_bytes;
+  auto* amax = reinterpret_cast<unsigned long long*>(meta);
+  auto* bmax = amax + L.Mp;
+  int* aexp = reinterpret_cast<int*>(bmax + L.Np);
+  int* bexp = aexp + L.Mp;
+  pack(g.A, true, g, g.M, L.Mp, L.Kp, Apk, amax, aexp, s);
+  pack(g.B, false, g, g.N, L.Np, L.Kp, Bpk, bmax, bexp, s);
+  const CUtensorMap ta = make_map(Apk, NSLICE * L.Mp, L.Kp);
+  const CUtensorMap tb = make_map(Bpk, NSLICE * L.Np, L.Kp);
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  SplitParams sp;
+  sp.M = g.M; sp.N = g.N; sp.K = g.K; sp.Mp = L.Mp; sp.Np = L.Np;
+  sp.nkb = static_cast<int>(L.Kp / TK);
+  sp.Cm = mkax(Mi, g.C.s_ro, g.C.s_ri);
+  sp.Cn = mkax(Ni, g.C.s_co, g.C.s_ci);
+  sp.C2m = mkax(Mi, g.C2.s_ro, g.C2.s_ri);
+  sp.C2n = mkax(Ni, g.C2.s_co, g.C2.s_ci);
+  sp.C = g.C.p; sp.C2 = g.C2.p;
+  sp.alpha = g.alpha; sp.beta = g.beta;
+  sp.ea = aexp; sp.eb = bexp;
+  sp.error = ws.error;
+  static bool configured = false;
+  if (!configured) {
+    CC_CHECK(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    configured = true;
+  }
+  dim3 grid(static_cast<unsigned>(L.Np / TN), static_cast<unsigned>(L.Mp / TM));
+  split_kernel<<<grid, 192, SMEM_BYTES, s>>>(ta, tb, sp);
+  CC_LAUNCH_CHECK();
+  g_split_launches.fetch_add(1);
+}
+
+}  // namespace cc4s_b200
