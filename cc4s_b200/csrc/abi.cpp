@@ -147,6 +147,8 @@ int Handle::run(cc4s_cc_result* out) {
     std::memcpy(&status_int, &st, sizeof(int));
     if (opt.mixer == CC4S_MIXER_DIIS && status_int != 0)
       throw Error(ERR_DIIS_SINGULAR, "Diagonalization failed (singular DIIS system)");
+    if (opt.precision != CC4S_PRECISION_FP64 && solver->device_error())
+      throw Error(ERR_TIMEOUT, "a tensor-core kernel gave up a bounded wait");
     Dr = host[0]; Xr = host[1];
     e = std::complex<double>(host[0] + host[1], host[2] + host[3]);
     const double norm = std::sqrt(host[4]);

@@ -223,7 +223,7 @@ void CcsdReal::residual(const double* T, double* R) {
     {  // R2 += dGph^T W
       Contraction c; c.M = n1; c.N = n1; c.K = G;
       c.A = tr(dGph_, n1); c.B = rm(W_, n1); c.C = rm(R2, n1); c.beta = 1.0;
-      gemm_(c);
+      tc_(c);
     }
     {  // R2[a][i][b][j] -= sum_k Vhhhp[j][i][k][a] t[b][k]      (batch j, m = (a,i))
       Contraction c; c.M = n1; c.N = v; c.K = o; c.batch = o; c.Mi = o;
@@ -255,7 +255,7 @@ void CcsdReal::residual(const double* T, double* R) {
   {  // Z = Gph M1
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(Z_, n1);
-    gemm_(c);
+    tc_(c);
   }
   if (!ccd) {  // dGph[G][a][i] += sum_d Gpp[G][a][d] t[d][i]
     Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
@@ -267,22 +267,22 @@ void CcsdReal::residual(const double* T, double* R) {
   {  // W1 = Gph Y
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(W1_, n1);
-    gemm_(c);
+    tc_(c);
   }
   {  // R2 += A2^T W1
     Contraction c; c.M = n1; c.N = n1; c.K = G;
     c.A = tr(dGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
   }
   {  // EX = -1/2 T Ve
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(Td, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
-    gemm_(c);
+    tc_(c);
   }
   {  // R2 += EX Y
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(EX_, n1); c.B = rm(Y_, n1); c.C = rm(R2, n1); c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
   }
   // ---- crossed ring Xakci (Ccsd.cxx:233-253) ------------------------------------
   ops::d2d(dGpp_, Gpp, G * v * v, s_);
@@ -304,7 +304,7 @@ void CcsdReal::residual(const double* T, double* R) {
   {  // EX = -1/2 T^x Ve
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(Te_, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
-    gemm_(c);
+    tc_(c);
   }
   {  // EX[a][i][c][k] += sum_G dGpp[G][a][c] dGhh[G][k][i]      (m = (a,c), n = (k,i))
     Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
@@ -312,13 +312,13 @@ void CcsdReal::residual(const double* T, double* R) {
     c.B = vw(dGhh_, 0, o * o, o, 1);
     c.C = vw(EX_, o * n1, o, 1, n1);
     c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
   }
   {  // R2 -= EX T
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(EX_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1);
     c.alpha = -1.0; c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
   }
   {  // R2_abij -= sum_ck T_ackj X_bkci : exchange pairing m = (a,j), n = (b,i)
     Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
@@ -326,7 +326,7 @@ void CcsdReal::residual(const double* T, double* R) {
     c.B = vw(EX_, 0, 1, o * n1, n1);
     c.C = vw(R2, o * n1, 1, o, n1);
     c.alpha = -1.0; c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
   }
   // ---- P(ab,ij) symmetrisation and +V (Ccsd.cxx:256,263) ----------------------
   ops::symmetrize(R2, n1, s_);
@@ -352,7 +352,7 @@ void CcsdReal::residual(const double* T, double* R) {
   {  // Xkl2[kl][ij] = sum_cd V_cdkl X_cdij
     Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
     c.A = tr(Vp_, o * o); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
-    gemm_(c);
+    tc_(c);
   }
   {  // R2 += Xkl1 X_abkl  (m = (a,b), n = (i,j))
     Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
@@ -360,10 +360,10 @@ void CcsdReal::residual(const double* T, double* R) {
     c.B = vw(Xkl1_, 0, o * o, o, 1);
     c.C = vw(R2, o * n1, o, n1, 1);
     c.beta = 1.0;
-    gemm_(c);
+    tc_(c);
     c.A.p = opt_.ppl ? Tp_ : Xp_;
     c.B.p = Xkl2_;
-    gemm_(c);
+    tc_(c);
   }
   // ---- particle-particle ladder (Ccsd.cxx:283-333) ------------------------------
   if (opt_.ppl) ppl(Xp_, R2, dGpp_);
@@ -425,7 +425,7 @@ void CcsdReal::residual(const double* T, double* R) {
     ops::axpby(W8_, 2.0, Xd_, -1.0, W8_, 0.0, D2, s_);
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(F_, n1);
-    gemm_(c);
+    tc_(c);
     Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
     d.A = vw(Gpp, 0, 1, v * v, v);
     d.B = vw(F_, n1, o, 0, 1);
@@ -458,7 +458,7 @@ void CcsdReal::ppl(const double* Xp, double* R2, const double* dGpp) {
         c.A = vw(cp(dGpp) + x0 * v, v, 1, 0, v * v);
         c.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
         c.C = vw(slab_, sy * v * v, v, v * v, 1);
-        gemm_(c);
+        tc_(c);
       }
       {
         Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
@@ -467,7 +467,7 @@ void CcsdReal::ppl(const double* Xp, double* R2, const double* dGpp) {
         c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
         if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
         c.beta = 1.0;
-        gemm_(c);
+        tc_(c);
       }
     }
   }

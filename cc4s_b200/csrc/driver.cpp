@@ -22,8 +22,8 @@ Handle::Handle(const cc4s_cc_options& o) : opt(o) {
     throw Error(ERR_INVALID_ARGUMENT, "Unknown mixer type");
   if (opt.mixer == CC4S_MIXER_DIIS && (opt.max_residua < 1 || opt.max_residua > 8))
     throw Error(ERR_UNSUPPORTED, "maxResidua must be in [1, 8]");
-  if (opt.precision != CC4S_PRECISION_FP64)
-    throw Error(ERR_UNSUPPORTED, "only the FP64 form is available in this build");
+  if (opt.precision != CC4S_PRECISION_FP64 && opt.precision != CC4S_PRECISION_SPLIT3)
+    throw Error(ERR_UNSUPPORTED, "precision must be FP64 or the three-slice split form");
   if (opt.max_iterations < 0) throw Error(ERR_INVALID_ARGUMENT, "maxIterations < 0");
   stream = ops::stream_create(opt.device);
   ev0 = ops::event_create();
@@ -155,6 +155,7 @@ void Handle::allocate_state() {
   if (complex_path) solver.reset(new CcsdComplex(csys, ro, stream));
   else solver.reset(new CcsdReal(sys, ro, stream));
   solver->set_profile(opt.profile != 0);
+  solver->set_precision(opt.precision == CC4S_PRECISION_SPLIT3 ? 3 : 0);
   const int64_t n = shape.total();
   Tcur = take(n);
   Rbuf = take(n);

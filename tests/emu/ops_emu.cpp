@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../cc4s_b200/csrc/ops.h"
+#include "../../cc4s_b200/csrc/split_gemm.cuh"
 
 namespace cc4s_b200 {
 
@@ -57,6 +58,76 @@ void gemm(const Contraction& g, cudaStream_t, const GemmScratch&) {
       }
     }
   }
+}
+
+// Emulation of the split-precision contraction: the same row/column scaling,
+// integer slices (6, 11, 11 bits) and the six slice products p + q <= 2
+// (0-based), summed exactly in FP64 (the device sums the leading group exactly
+// in FP32 per 4096-wide chunk; the lower groups differ only below 2^-50 relative).
+static uint64_t g_split = 0;
+uint64_t split_launch_count() { return g_split; }
+size_t gemm_split_scratch_bytes(const Contraction&) { return 64; }
+
+void gemm_split(const Contraction& g, cudaStream_t, SplitScratch&) {
+  ++g_split;
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  const int64_t Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);
+  Ax Am = ax(Mi, g.A.s_ro, g.A.s_ri), Ak = ax(Ki, g.A.s_co, g.A.s_ci);
+  Ax Bk = ax(Ki, g.B.s_ro, g.B.s_ri), Bn = ax(Ni, g.B.s_co, g.B.s_ci);
+  Ax Cm = ax(Mi, g.C.s_ro, g.C.s_ri), Cn = ax(Ni, g.C.s_co, g.C.s_ci);
+  Ax C2m = ax(Mi, g.C2.s_ro, g.C2.s_ri), C2n = ax(Ni, g.C2.s_co, g.C2.s_ci);
+  auto split = [](const std::vector<double>& x, std::vector<double> (&s)[3], int& e) {
+    double m = 0.0;
+    for (double v : x) m = std::max(m, std::fabs(v));
+    e = 0;
+    if (m > 0.0) std::frexp(m, &e);
+    for (auto& v : s) v.assign(x.size(), 0.0);
+    for (size_t k = 0; k < x.size(); ++k) {
+      double y = std::ldexp(x[k], -e) * 64.0;
+      const double s1 = std::nearbyint(y);
+      double t = (y - s1) * 2048.0;
+      const double s2 = std::nearbyint(t);
+      t = (t - s2) * 2048.0;
+      s[0][k] = s1; s[1][k] = s2; s[2][k] = std::nearbyint(t);
+    }
+  };
+  std::vector<std::vector<double>> as[3], bs[3];
+  std::vector<int> ea(g.M), eb(g.N);
+  for (auto& v : as) v.resize(g.M);
+  for (auto& v : bs) v.resize(g.N);
+  std::vector<double> row(g.K);
+  for (int64_t m = 0; m < g.M; ++m) {
+    for (int64_t k = 0; k < g.K; ++k) row[k] = g.A.p[Am.off(m) + Ak.off(k)];
+    std::vector<double> s[3];
+    split(row, s, ea[m]);
+    for (int q = 0; q < 3; ++q) as[q][m] = s[q];
+  }
+  for (int64_t n = 0; n < g.N; ++n) {
+    for (int64_t k = 0; k < g.K; ++k) row[k] = g.B.p[Bk.off(k) + Bn.off(n)];
+    std::vector<double> s[3];
+    split(row, s, eb[n]);
+    for (int q = 0; q < 3; ++q) bs[q][n] = s[q];
+  }
+  const double w[3] = {0x1p-12, 0x1p-23, 0x1p-34};
+  for (int64_t m = 0; m < g.M; ++m)
+    for (int64_t n = 0; n < g.N; ++n) {
+      double acc[3] = {0, 0, 0};
+      for (int pa = 0; pa < 3; ++pa)
+        for (int pb = 0; pb + pa < 3; ++pb) {
+          double s = 0.0;
+          const auto& x = as[pa][m];
+          const auto& y = bs[pb][n];
+          for (int64_t k = 0; k < g.K; ++k) s += x[k] * y[k];
+          acc[pa + pb] += s;
+        }
+      const double v = g.alpha * std::ldexp(acc[0] * w[0] + acc[1] * w[1] + acc[2] * w[2], ea[m] + eb[n]);
+      double* c = g.C.p + Cm.off(m) + Cn.off(n);
+      *c = g.beta != 0.0 ? v + g.beta * *c : v;
+      if (g.C2.p) {
+        double* c2 = g.C2.p + C2m.off(m) + C2n.off(n);
+        *c2 = g.beta != 0.0 ? v + g.beta * *c2 : v;
+      }
+    }
 }
 
 namespace ops {
