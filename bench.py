@@ -177,19 +177,10 @@ def barrier(world):
         dist.barrier()
 
 
-def run_ours(args, world, rank, local):
-    import numpy as np
-    import torch
-    from cc4s_b200 import Solver, reference_flops
-    from cc4s_b200.synthetic import config
-    torch.cuda.set_device(local)
-    cfg = args.config
-    o, v, G = CONFIG_SHAPES[cfg]
-    eh, ep, g, hg = config(cfg, seed=0)
-    F = reference_flops(o, v, G)
-    K, W = args.steps, args.warmup
-    opts = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
-                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
+def timed_run(opts, inputs, W, K, world, local):
+    """W + K iterations; the last K are timed (CUDA events on the library stream)."""
+    from cc4s_b200 import Solver
+    eh, ep, g, hg = inputs
     sol = Solver(opts)
     sol.set_inputs(eh, ep, g, half_grid=hg)
     st0 = sol.stats()
@@ -200,23 +191,62 @@ def run_ours(args, world, rank, local):
     st1 = sol.stats()
     secs = [h["seconds"] for h in r["history"]]
     t = all_max(sum(secs[W:W + K]), world)
-    ms = 1e3 * t / K
-    launches_per_it = ((st1["gemm_launches"] - st0["gemm_launches"]) +
-                       (st1["other_launches"] - st0["other_launches"])) / (W + K)
-    T1, T2 = sol.amplitudes()
+    launches = ((st1["gemm_launches"] - st0["gemm_launches"]) +
+                (st1["other_launches"] - st0["other_launches"])) / (W + K)
+    T = sol.amplitudes()
     sol.close()
-    # dominant kernel: per-launch CUDA events around every DMMA contraction of one residual
-    prof = Solver(dict(opts, profile=True, maxIterations=1))
+    return dict(t=t, r=r, launches=launches, T=T, clocks=clk.summary())
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from cc4s_b200 import Solver, reference_flops
+    from cc4s_b200.synthetic import config
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    inputs = config(cfg, seed=0)
+    eh, ep, g, hg = inputs
+    F = reference_flops(o, v, G)
+    K, W = args.steps, args.warmup
+    base = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
+                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
+    forms = ["fp64", "split3"] if args.precision == "both" else [args.precision]
+    runs = {p: timed_run(dict(base, precision=p), inputs, W, K, world, local) for p in forms}
+    head = "split3" if "split3" in runs else "fp64"
+    hr = runs[head]
+    t = hr["t"]
+    # dominant kernel: per-launch CUDA events around every contraction of one residual
+    prof = Solver(dict(base, precision=head, profile=True, maxIterations=1))
     prof.set_inputs(eh, ep, g, half_grid=hg)
-    prof.residual((T1, T2))
+    prof.residual(hr["T"])
     ps = prof.stats()
     prof.close()
-    peak = dgemm_peak(local)
-    achieved = ps["gemm_flops"] / ps["gemm_seconds"] / 1e12
+    pk = peaks()
+    dpeak = dgemm_peak(local)
+    if head == "split3":
+        # executed FP16 tensor work: six slice products per FP64-equivalent multiply-add
+        achieved = 6.0 * ps["split_flops"] / ps["split_seconds"] / 1e12
+        peak = pk.get("bf16_tflops_sustained", 1405.3)
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "split_kernel (tcgen05.mma kind::f16, TMEM, TMA) incl. operand slicing, "
+                          "%d launches of one residual" % ps["split_launches"],
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+                "fp64_equivalent_tflops": ps["split_flops"] / ps["split_seconds"] / 1e12}
+    else:
+        achieved = ps["gemm_flops"] / ps["gemm_seconds"] / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
+                "frac": achieved / dpeak, "traffic": None,
+                "kernel": "gemm_f64_kernel (mma.sync m16n8k16 f64), all %d contraction launches "
+                          "of one residual" % ps["gemm_profiled_launches"],
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured; no FP64 "
+                               "entry in MEASURED_PEAKS.json)",
+                "top_launch_tflops": ps["top_flops"] / ps["top_seconds"] / 1e12}
     # end to end through the C ABI from host buffers
     barrier(world)
     t0 = time.perf_counter()
-    e2e = Solver(dict(opts, maxIterations=K))
+    e2e = Solver(dict(base, precision=head, maxIterations=K))
     e2e.set_inputs(eh, ep, g, half_grid=hg)
     re = e2e.run()
     A1, A2 = e2e.amplitudes()
@@ -225,30 +255,32 @@ def run_ours(args, world, rank, local):
     e2e.close()
     h2d = (g.nbytes + eh.nbytes + ep.nbytes) / K
     d2h = (A1.nbytes + A2.nbytes) / K + 5 * 8 + 8
+    conf = {"workload": "CCSD %s: No=%d Nv=%d NG=%d real, DIIS 5, %s" % (cfg, o, v, G, head),
+            "precision": head, "s_per_iter": t / K,
+            "flops_per_iter_reference_formulation": F,
+            "flops_per_iter_executed": hr["r"]["flops_per_iteration"],
+            "l2": "inputs larger than L2 (T2 %.2f GB)" % ((v * o) ** 2 * 8 / 1e9),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "energy_after_steps": hr["r"]["correlation"],
+            "fp64_dgemm_peak_tflops": dpeak}
+    if "fp64" in runs and "split3" in runs:
+        t64 = runs["fp64"]["t"]
+        conf.update({"fp64_s_per_iter": t64 / K, "fp64_tflops": world * F / (t64 / K) / 1e12,
+                     "split_speedup_vs_fp64": t64 / t,
+                     "abs_dE_after_steps_split_vs_fp64":
+                         abs(runs["split3"]["r"]["correlation"] - runs["fp64"]["r"]["correlation"])})
     line = {
         "metric": METRIC, "value": world * F / (t / K) / 1e12, "unit": "TFLOP/s",
-        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms,
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": 1e3 * t / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the workload's distributions)",
-        "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d real, DIIS 5" % (cfg, o, v, G),
-                   "precision": "fp64 (DMMA)", "s_per_iter": t / K,
-                   "flops_per_iter_reference_formulation": F,
-                   "flops_per_iter_executed": r["flops_per_iteration"],
-                   "l2": "inputs larger than L2 (T2 %.2f GB)" % ((v * o) ** 2 * 8 / 1e9),
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "energy_after_steps": r["correlation"]},
+        "config": conf,
         "e2e": {"value": world * F * K / t_e2e / 1e12, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "seconds": t_e2e, "iterations": re["iterations"]},
-        "gpu_launches": int(round(launches_per_it * K)),
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "kernel": "gemm_f64_kernel (mma.sync m16n8k4 f64), all %d contraction "
-                               "launches of one residual" % ps["gemm_profiled_launches"],
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry "
-                                    "in MEASURED_PEAKS.json)",
-                     "top_launch_tflops": ps["top_flops"] / ps["top_seconds"] / 1e12},
-        "clocks": clk.summary(),
+        "gpu_launches": int(round(hr["launches"] * K)),
+        "roofline": roof,
+        "clocks": hr["clocks"],
     }
     return line
 
@@ -285,6 +317,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(CONFIG_SHAPES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "split3"])
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

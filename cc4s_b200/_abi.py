@@ -22,7 +22,7 @@ ERR_STATE = 8
 ERR_NON_FINITE = 9
 ERR_UNSUPPORTED = 10
 
-METHODS = {"Ccsd": 0, "Ccd": 1}
+METHODS = {"Ccsd": 0, "Ccd": 1, "Drccd": 2}
 PRECISIONS = {"fp64": 0, "split2": 2, "split3": 3}
 MIXERS = {"DiisMixer": 0, "LinearMixer": 1}
 
@@ -30,7 +30,8 @@ MIXERS = {"DiisMixer": 0, "LinearMixer": 1}
 EXPORTS = [
     "cc4s_cc_default_options", "cc4s_cc_create", "cc4s_cc_set_inputs",
     "cc4s_cc_set_initial_amplitudes", "cc4s_cc_run", "cc4s_cc_get_amplitudes",
-    "cc4s_cc_residual", "cc4s_cc_get_stats", "cc4s_cc_destroy", "cc4s_cc_last_error",
+    "cc4s_cc_residual", "cc4s_cc_get_stats", "cc4s_cc_destroy",
+    "cc4s_cc_last_error",
 ]
 
 
@@ -41,7 +42,8 @@ class Options(ctypes.Structure):
         ("max_iterations", ctypes.c_int), ("energy_convergence", ctypes.c_double),
         ("amplitudes_convergence", ctypes.c_double), ("level_shift", ctypes.c_double),
         ("integrals_slice_size", ctypes.c_int64), ("ppl", ctypes.c_int), ("device", ctypes.c_int),
-        ("profile", ctypes.c_int),
+        ("profile", ctypes.c_int), ("linearized", ctypes.c_int),
+        ("adjacent_pairs_exchange", ctypes.c_int),
     ]
 
 
@@ -64,6 +66,8 @@ class Stats(ctypes.Structure):
         ("gemm_seconds", ctypes.c_double), ("gemm_flops", ctypes.c_double),
         ("top_seconds", ctypes.c_double), ("top_flops", ctypes.c_double),
         ("gemm_profiled_launches", ctypes.c_int),
+        ("split_seconds", ctypes.c_double), ("split_flops", ctypes.c_double),
+        ("split_launches", ctypes.c_int),
     ]
 
 

@@ -43,6 +43,8 @@ def _options(lib, arguments):
     o.precision = _abi.PRECISIONS[arguments.get("precision", "fp64")]
     o.device = int(arguments.get("device", 0))
     o.profile = 1 if arguments.get("profile", False) else 0
+    o.linearized = 1 if arguments.get("linearized", False) else 0
+    o.adjacent_pairs_exchange = 1 if arguments.get("adjacentPairsExchange", False) else 0
     return o
 
 
@@ -145,7 +147,9 @@ class Solver:
                     device_bytes=s.device_bytes, flops_per_residual=s.flops_per_residual,
                     gemm_seconds=s.gemm_seconds, gemm_flops=s.gemm_flops,
                     top_seconds=s.top_seconds, top_flops=s.top_flops,
-                    gemm_profiled_launches=s.gemm_profiled_launches)
+                    gemm_profiled_launches=s.gemm_profiled_launches,
+                    split_seconds=s.split_seconds, split_flops=s.split_flops,
+                    split_launches=s.split_launches)
 
 
 def _full_vertex(arguments):

@@ -250,6 +250,8 @@ void cc4s_cc_default_options(cc4s_cc_options* o) {
   o->ppl = 1;
   o->device = 0;
   o->profile = 0;
+  o->linearized = 0;
+  o->adjacent_pairs_exchange = 0;
 }
 
 int cc4s_cc_create(const cc4s_cc_options* opt, cc4s_cc_handle** h) {
@@ -301,7 +303,8 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
   if (!h || !h->impl || !out) return CC4S_ERR_INVALID_ARGUMENT;
-  out->gemm_launches = cc4s_b200::gemm_launch_count();
+  // each split-precision contraction is two slicing launches plus the tensor-core kernel
+  out->gemm_launches = cc4s_b200::gemm_launch_count() + 3 * cc4s_b200::split_launch_count();
   out->other_launches = cc4s_b200::ops::launch_count();
   size_t bytes = 0;
   if (h->impl->solver) bytes += h->impl->solver->device_bytes();
@@ -309,6 +312,8 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
   out->flops_per_residual = h->impl->solver ? h->impl->solver->flops_per_residual() : 0.0;
   out->gemm_seconds = out->gemm_flops = out->top_seconds = out->top_flops = 0.0;
   out->gemm_profiled_launches = 0;
+  out->split_seconds = out->split_flops = 0.0;
+  out->split_launches = 0;
   if (h->impl->solver) {
     const auto& p = h->impl->solver->profile();
     out->gemm_seconds = p.gemm_seconds;
@@ -316,6 +321,9 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
     out->top_seconds = p.top_seconds;
     out->top_flops = p.top_flops;
     out->gemm_profiled_launches = p.launches;
+    out->split_seconds = p.split_seconds;
+    out->split_flops = p.split_flops;
+    out->split_launches = p.split_launches;
   }
   return 0;
 }

@@ -54,39 +54,6 @@ CcsdComplex::CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Strea
   count_flops_ = true;
 }
 
-void CcsdComplex::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA,
-                        bool conjB) {
-  const double sA = conjA ? -1.0 : 1.0, sB = conjB ? -1.0 : 1.0;
-  const double al = c.alpha, be = c.beta;
-  double* Ar = c.A.p;
-  double* Br = c.B.p;
-  double* Cr = c.C.p;
-  double* C2r = c.C2.p;
-  // real plane: Re(A) Re(B) - sA sB Im(A) Im(B)
-  gemm_(c);
-  if (a_im && b_im) {
-    Contraction r = c;
-    r.A.p = Ar + a_im; r.B.p = Br + b_im; r.alpha = -al * sA * sB; r.beta = 1.0;
-    gemm_(r);
-  }
-  // imaginary plane: sB Re(A) Im(B) + sA Im(A) Re(B)
-  Contraction i = c;
-  i.C.p = Cr + c_im;
-  if (C2r) i.C2.p = C2r + c_im;
-  bool wrote = false;
-  if (b_im) {
-    i.B.p = Br + b_im; i.alpha = al * sB; i.beta = be;
-    gemm_(i);
-    wrote = true;
-  }
-  if (a_im) {
-    i.A.p = Ar + a_im; i.B.p = Br; i.alpha = al * sA; i.beta = wrote ? 1.0 : be;
-    gemm_(i);
-    wrote = true;
-  }
-  if (!wrote) throw Error(ERR_STATE, "zgemm: both operands real");
-}
-
 void CcsdComplex::zperm(double* dst, int64_t dst_im, const double* src, int64_t src_im,
                         const int64_t d[4], const int p[4], double alpha, double beta,
                         bool conj) {

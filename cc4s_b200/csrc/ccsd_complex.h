@@ -32,11 +32,6 @@ class CcsdComplex : public Schedule {
   const double* Ve_im() const override { return Ven_ + D2_; }
 
  private:
-  // C = alpha * op(A) op(B) + beta * C on complex planar operands; the
-  // imaginary plane of each operand sits at the given element offset
-  // (0: the operand is real).  conjA/conjB conjugate the operand.
-  void zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA = false,
-             bool conjB = false);
   void zperm(double* dst, int64_t dst_im, const double* src, int64_t src_im, const int64_t d[4],
              const int p[4], double alpha, double beta, bool conj = false);
   void zaxpby(double* out, double a, const double* x, double b, const double* y, int64_t n);

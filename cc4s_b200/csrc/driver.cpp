@@ -16,7 +16,8 @@
 namespace cc4s_b200 {
 
 Handle::Handle(const cc4s_cc_options& o) : opt(o) {
-  if (opt.method != CC4S_METHOD_CCSD && opt.method != CC4S_METHOD_CCD)
+  if (opt.method != CC4S_METHOD_CCSD && opt.method != CC4S_METHOD_CCD &&
+      opt.method != CC4S_METHOD_DRCCD)
     throw Error(ERR_INVALID_ARGUMENT, "Unknown method");
   if (opt.mixer != CC4S_MIXER_DIIS && opt.mixer != CC4S_MIXER_LINEAR)
     throw Error(ERR_INVALID_ARGUMENT, "Unknown mixer type");
@@ -152,8 +153,19 @@ void Handle::allocate_state() {
   // Real path: the ladder is symmetric under (a,c) <-> (b,d), so its slab size is a
   // free memory/performance choice.  Complex path: slices follow integralsSliceSize.
   if (complex_path) ro.slab = opt.integrals_slice_size;
-  if (complex_path) solver.reset(new CcsdComplex(csys, ro, stream));
-  else solver.reset(new CcsdReal(sys, ro, stream));
+  if (opt.method == CC4S_METHOD_DRCCD) {
+    DrccdOptions dro;
+    dro.linearized = opt.linearized != 0;
+    dro.adjacent_pairs_exchange = opt.adjacent_pairs_exchange != 0;
+    if (complex_path)
+      solver.reset(new Drccd(csys.o, csys.v, csys.G, true, csys.Gph, csys.Ghp, dro, stream));
+    else
+      solver.reset(new Drccd(sys.o, sys.v, sys.G, false, sys.Gph, sys.Ghp, dro, stream));
+  } else if (complex_path) {
+    solver.reset(new CcsdComplex(csys, ro, stream));
+  } else {
+    solver.reset(new CcsdReal(sys, ro, stream));
+  }
   solver->set_profile(opt.profile != 0);
   solver->set_precision(opt.precision == CC4S_PRECISION_SPLIT3 ? 3 : 0);
   const int64_t n = shape.total();

@@ -7,6 +7,7 @@
 
 #include "../../include/cc4s_cc.h"
 #include "ccsd_complex.h"
+#include "drccd.h"
 #include "ccsd_real.h"
 #include "ops.h"
 

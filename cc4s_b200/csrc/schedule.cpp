@@ -30,6 +30,7 @@ void Schedule::gemm_(const Contraction& c) {
     const size_t k = ev_flops_.size();
     while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
     ev_flops_.push_back(f);
+    ev_split_.push_back(0);
     ops::event_record(ev_[2 * k], s_);
     gemm(c, s_, scratch_);
     ops::event_record(ev_[2 * k + 1], s_);
@@ -61,12 +62,48 @@ void Schedule::tc_(const Contraction& c) {
     const size_t k = ev_flops_.size();
     while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
     ev_flops_.push_back(f);
+    ev_split_.push_back(1);
     ops::event_record(ev_[2 * k], s_);
     gemm_split(c, s_, split_);
     ops::event_record(ev_[2 * k + 1], s_);
     return;
   }
   gemm_split(c, s_, split_);
+}
+
+void Schedule::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA,
+                     bool conjB, bool big) {
+  auto run = [&](const Contraction& x) { if (big) tc_(x); else gemm_(x); };
+  const double sA = conjA ? -1.0 : 1.0, sB = conjB ? -1.0 : 1.0;
+  const double al = c.alpha, be = c.beta;
+  double* Ar = c.A.p;
+  double* Br = c.B.p;
+  double* Cr = c.C.p;
+  double* C2r = c.C2.p;
+  // real plane: Re(A) Re(B) - sA sB Im(A) Im(B)
+  run(c);
+  if (a_im && b_im) {
+    Contraction r = c;
+    r.A.p = Ar + a_im; r.B.p = Br + b_im; r.alpha = -al * sA * sB; r.beta = 1.0;
+    run(r);
+  }
+  if (!c_im) return;  // real result (both operands real)
+  // imaginary plane: sB Re(A) Im(B) + sA Im(A) Re(B)
+  Contraction i = c;
+  i.C.p = Cr + c_im;
+  if (C2r) i.C2.p = C2r + c_im;
+  bool wrote = false;
+  if (b_im) {
+    i.B.p = Br + b_im; i.alpha = al * sB; i.beta = be;
+    run(i);
+    wrote = true;
+  }
+  if (a_im) {
+    i.A.p = Ar + a_im; i.B.p = Br; i.alpha = al * sA; i.beta = wrote ? 1.0 : be;
+    run(i);
+    wrote = true;
+  }
+  if (!wrote) throw Error(ERR_STATE, "zgemm: complex result from real operands");
 }
 
 int Schedule::device_error() {
@@ -87,8 +124,14 @@ void Schedule::profile_finish() {
     p.gemm_seconds += sec;
     p.gemm_flops += ev_flops_[k];
     if (ev_flops_[k] > p.top_flops) { p.top_flops = ev_flops_[k]; p.top_seconds = sec; }
+    if (ev_split_[k]) {
+      p.split_seconds += sec;
+      p.split_flops += ev_flops_[k];
+      ++p.split_launches;
+    }
   }
   p.launches = static_cast<int>(ev_flops_.size());
+  ev_split_.clear();
   ev_flops_.clear();
   prof_ = p;
 }

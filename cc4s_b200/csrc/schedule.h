@@ -48,6 +48,9 @@ class Schedule {
     double gemm_seconds = 0, gemm_flops = 0;  // all contractions of the last residual
     double top_seconds = 0, top_flops = 0;    // the most expensive single launch
     int launches = 0;
+    // split-precision launches only (FP64-equivalent flops; 6 FP16 products each)
+    double split_seconds = 0, split_flops = 0;
+    int split_launches = 0;
   };
   const Profile& profile() const { return prof_; }
 
@@ -56,6 +59,12 @@ class Schedule {
   void gemm_(const Contraction& c);
   // A large contraction: split precision when enabled (batch 1), else FP64.
   void tc_(const Contraction& c);
+  // C = alpha * op(A) op(B) + beta * C on planar complex operands: the
+  // imaginary plane of each operand sits at the given element offset (0: the
+  // operand is real); conjA / conjB conjugate an operand.  Four real
+  // contractions; `big` routes them through tc_.
+  void zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA = false,
+             bool conjB = false, bool big = false);
   void profile_finish();
   int precision_ = 0;
   SplitScratch split_;
@@ -72,6 +81,7 @@ class Schedule {
   Profile prof_;
   std::vector<void*> ev_;
   std::vector<double> ev_flops_;
+  std::vector<char> ev_split_;
 };
 
 }  // namespace cc4s_b200

@@ -48,6 +48,7 @@ extern "C" {
 
 #define CC4S_METHOD_CCSD 0
 #define CC4S_METHOD_CCD 1
+#define CC4S_METHOD_DRCCD 2
 
 #define CC4S_PRECISION_FP64 0
 #define CC4S_PRECISION_SPLIT2 2
@@ -76,6 +77,8 @@ typedef struct {
   int ppl;                      /* "ppl" (1), Ccsd.cxx:95 */
   int device;                   /* CUDA device ordinal */
   int profile;                  /* 1: time every contraction launch (CUDA events) */
+  int linearized;               /* "linearized" (0), Drccd only, Drccd.cxx:53-55 */
+  int adjacent_pairs_exchange;  /* "adjacentPairsExchange" (0), Drccd only, Drccd.cxx:56-58 */
 } cc4s_cc_options;
 
 typedef struct {
@@ -100,6 +103,8 @@ typedef struct {
   double gemm_seconds, gemm_flops;   /* all launches */
   double top_seconds, top_flops;     /* the most expensive launch */
   int gemm_profiled_launches;
+  double split_seconds, split_flops;  /* the split-precision launches among them */
+  int split_launches;
 } cc4s_cc_stats;
 
 /* Fills the defaults of the reference. */
@@ -140,6 +145,7 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
                      double* R2);
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
+
 
 /* Releases the handle and its device memory. */
 int cc4s_cc_destroy(cc4s_cc_handle* h);

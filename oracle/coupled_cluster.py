@@ -77,6 +77,11 @@ def run(sys: System, initial_amplitudes=None, **opts):
     if method == "Ccsd" or method == "Ccd":
         kw = dict(ppl=bool(o["ppl"]), slice_size=o["integralsSliceSize"], ccd=(method == "Ccd"))
         res_fn = lambda T: ccsd_mod.residuum(T, inp, **kw)
+    elif method == "Drccd":
+        from . import drccd
+        dr_inp = drccd.DrccdInputs(sys)
+        res_fn = lambda T: drccd.residuum(T, dr_inp, linearized=bool(o.get("linearized", False)),
+                                          adjacent_pairs_exchange=bool(o.get("adjacentPairsExchange", False)))
     elif method == "CcsdReference":
         ref_inp = ccsd_reference.ReferenceInputs(sys)
         res_fn = lambda T: ccsd_reference.residuum(T, ref_inp)

@@ -6,7 +6,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 CSRC = os.path.join(ROOT, "cc4s_b200", "csrc")
 OUT = os.path.join(HERE, "_build", "libcc4s_emu.so")
-SCHEDULE_SOURCES = ("schedule.cpp", "ccsd_real.cpp", "ccsd_complex.cpp", "driver.cpp", "abi.cpp")
+SCHEDULE_SOURCES = ("schedule.cpp", "ccsd_real.cpp", "ccsd_complex.cpp", "drccd.cpp",
+                    "driver.cpp", "abi.cpp")
 
 
 def build():

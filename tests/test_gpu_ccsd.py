@@ -141,6 +141,38 @@ def test_complex_residual_parity(Solver, shape, hermitian):
     assert _rel(R1, Q1) < TOL_RES and _rel(R2, Q2) < TOL_RES
 
 
+def test_split_precision_residual(Solver):
+    """Three-slice tensor-core form of the residual vs the FP64 oracle: the split
+    products carry 28 bits of each operand row/column, so the residual agrees to
+    ~1e-7 of its largest element (tolerance 1e-5)."""
+    s = inputs.synthetic_system(16, 128, 256, seed=2)
+    rng = np.random.default_rng(3)
+    T = _rand_T(rng, 128, 16)
+    sol = Solver({"precision": "split3"})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    R1, R2 = sol.residual(T)
+    Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s))
+    assert _rel(R2, Q2) < 1e-5 and _rel(R1, Q1) < 1e-5
+    assert _rel(R2, Q2) > 1e-14  # the tensor-core path really ran
+
+
+@pytest.mark.parametrize("shape", [(8, 40, 200), (10, 64, 150)])
+def test_split_precision_energy_within_1ueh(Solver, shape):
+    """Converged CCSD energy of the split-precision form within 1 uEh of FP64."""
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, seed=0)
+    o = dict(maxIterations=80, energyConvergence=1e-10, amplitudesConvergence=1e-7,
+             mixer=dict(type="DiisMixer", maxResidua=5))
+    a = Solver(o)
+    a.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    ra = a.run()
+    b = Solver(dict(o, precision="split3"))
+    b.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    rb = b.run()
+    assert ra["converged"] and rb["converged"]
+    assert abs(ra["correlation"] - rb["correlation"]) < 1e-6
+
+
 def test_complex_run(Solver):
     s = inputs.synthetic_system(6, 30, 60, complex=True, seed=5)
     o = dict(maxIterations=30, energyConvergence=1e-10, amplitudesConvergence=1e-8)

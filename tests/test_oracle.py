@@ -33,6 +33,16 @@ def test_ueg_pinned_to_reference_expected_output():
         assert abs(r["energy"][k] - ref) < 1e-10, (k, r["energy"][k], ref)
 
 
+def test_ueg_drccd_pinned_to_reference_expected_output():
+    """Restated Drccd reproduces the reference's expected UEG Drccd energies."""
+    g = json.load(open(os.path.join(GOLDEN, "ueg_rs1.0_7occ_26virt.json")))
+    s = inputs.ueg_system(7, 26, 1.0)
+    r = coupled_cluster.run(s, **g["drccd"]["options"])
+    assert r["convergenceReached"]
+    for k, ref in g["drccd"]["energy"].items():
+        assert abs(r["energy"][k] - ref) < 1e-10, (k, r["energy"][k], ref)
+
+
 def test_ueg_mp2_matches_second_order():
     g = json.load(open(os.path.join(GOLDEN, "ueg_rs1.0_7occ_26virt.json")))
     s = inputs.ueg_system(7, 26, 1.0)
