@@ -9,6 +9,9 @@
 
 namespace cc4s_b200 {
 
+int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t No, int64_t Nv,
+                   int is_complex, double* out, cudaStream_t stream, const char** err);
+
 // Reference layout T1[a,i], T2[a,b,i,j] (first index fastest) -> amplitude vector.
 // Complex host buffers are interleaved (re, im); device vectors are planar.
 void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2) {
@@ -326,6 +329,15 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
     out->split_launches = p.split_launches;
   }
   return 0;
+}
+
+int cc4s_cc_energy_noalloc(const double* T1, const double* T2, const double* Vpphh, int64_t No,
+                           int64_t Nv, int is_complex, double* energy, void* stream) {
+  const char* err = "";
+  const int st = cc4s_b200::energy_noalloc(T1, T2, Vpphh, No, Nv, is_complex, energy,
+                                            static_cast<cudaStream_t>(stream), &err);
+  if (st) g_create_error = err;
+  return st;
 }
 
 int cc4s_cc_destroy(cc4s_cc_handle* h) {

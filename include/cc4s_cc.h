@@ -146,6 +146,25 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
 
+/* Correlation energy of amplitudes that already live in device memory, computed
+ * without allocating any device memory.  No counterpart in the reference: this
+ * is for callers that cannot allocate at the point of the call (hosts whose
+ * device memory is entirely owned by their own pool, or loops that must not
+ * pay for the device synchronisation a cudaFree implies).
+ * Inputs (device pointers, reference column-major layout, complex interleaved
+ * when is_complex): T1[a,i], T2[a,b,i,j] and V_abij (the "pphh" integrals).
+ * Output: energy[0..3] (device) = direct, exchange, and their imaginary parts,
+ * with correlation = direct + exchange as in CoupledCluster::getEnergy.
+ * Temporary data lives in a fixed 2 MiB device array (nothing in it, nor in
+ * energy, has to start at zero), so No <= 256
+ * (larger systems are rejected with CC4S_ERR_BAD_SHAPE).  The first call on a
+ * device looks up that array's device address; make that first call before
+ * any stream capture.  Every call shares the array: calls whose kernels
+ * overlap on the GPU (different streams, no ordering) race.  stream is a
+ * cudaStream_t (NULL: the legacy default stream).  Errors: cc4s_cc_last_error(NULL). */
+int cc4s_cc_energy_noalloc(const double* T1, const double* T2, const double* Vpphh, int64_t No,
+                           int64_t Nv, int is_complex, double* energy, void* stream);
+
 
 /* Releases the handle and its device memory. */
 int cc4s_cc_destroy(cc4s_cc_handle* h);

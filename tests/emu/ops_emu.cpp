@@ -130,6 +130,36 @@ void gemm_split(const Contraction& g, cudaStream_t, SplitScratch&) {
     }
 }
 
+// Plain-loop stand-in for the allocation-free energy entry (host pointers).
+int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t o, int64_t v,
+                   int cplx, double* out, cudaStream_t, const char** err) {
+  if (!T1 || !T2 || !V || !out) { *err = "null pointer"; return ERR_INVALID_ARGUMENT; }
+  if (o <= 0 || v <= 0) { *err = "No and Nv must be positive"; return ERR_BAD_SHAPE; }
+  if (o * o > 65536) { *err = "No too large"; return ERR_BAD_SHAPE; }
+  double acc[4] = {0, 0, 0, 0};
+  for (int64_t j = 0; j < o; ++j)
+    for (int64_t i = 0; i < o; ++i)
+      for (int64_t b = 0; b < v; ++b)
+        for (int64_t a = 0; a < v; ++a) {
+          const int64_t e = a + v * (b + v * (i + o * j)), ex = b + v * (a + v * (i + o * j));
+          const int64_t ai = a + v * i, bj = b + v * j;
+          if (!cplx) {
+            const double x = T2[e] + T1[ai] * T1[bj];
+            acc[0] += x * V[e];
+            acc[1] += x * V[ex];
+          } else {
+            const double xr = T2[2 * e] + T1[2 * ai] * T1[2 * bj] - T1[2 * ai + 1] * T1[2 * bj + 1];
+            const double xi = T2[2 * e + 1] + T1[2 * ai] * T1[2 * bj + 1] + T1[2 * ai + 1] * T1[2 * bj];
+            acc[0] += xr * V[2 * e] + xi * V[2 * e + 1];
+            acc[1] += xr * V[2 * ex] + xi * V[2 * ex + 1];
+            acc[2] += xi * V[2 * e] - xr * V[2 * e + 1];
+            acc[3] += xi * V[2 * ex] - xr * V[2 * ex + 1];
+          }
+        }
+  out[0] = 2 * acc[0]; out[1] = -acc[1]; out[2] = 2 * acc[2]; out[3] = -acc[3];
+  return OK;
+}
+
 namespace ops {
 
 double* alloc(size_t elems) {
