@@ -30,7 +30,7 @@ MIXERS = {"DiisMixer": 0, "LinearMixer": 1}
 EXPORTS = [
     "cc4s_cc_default_options", "cc4s_cc_create", "cc4s_cc_set_inputs",
     "cc4s_cc_set_initial_amplitudes", "cc4s_cc_run", "cc4s_cc_get_amplitudes",
-    "cc4s_cc_residual", "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
+    "cc4s_cc_residual", "cc4s_cc_backward", "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
     "cc4s_cc_last_error",
 ]
 
@@ -96,6 +96,7 @@ def load(path=None):
     lib.cc4s_cc_get_amplitudes.argtypes = [ctypes.c_void_p, dp, dp]
     lib.cc4s_cc_residual.argtypes = [ctypes.c_void_p, dp, dp, dp, dp]
     lib.cc4s_cc_get_stats.argtypes = [ctypes.c_void_p, P(Stats)]
+    lib.cc4s_cc_backward.argtypes = [ctypes.c_void_p, dp, dp]
     lib.cc4s_cc_energy_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p]

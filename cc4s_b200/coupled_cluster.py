@@ -91,6 +91,7 @@ class Solver:
                                                 _abi.ptr(g), NG, int(cplx), int(bool(half_grid))))
         self.No, self.Nv, self.NG = No, Nv, NG
         self.cplx = cplx and not half_grid
+        self.in_complex_input = cplx
 
     def _dtype(self):
         return np.complex128 if self.cplx else np.float64
@@ -139,6 +140,22 @@ class Solver:
         t1, t2 = self._alloc_amps()
         self._check(self.lib.cc4s_cc_get_amplitudes(self.h, _abi.ptr(t1), _abi.ptr(t2)))
         return self._unpack(t1, t2)
+
+    def backward(self, gradient=False):
+        """Adjoint at the current amplitudes: S(G) = dE/dV(G) and, on the real
+        path, dE/dGamma in the caller's vertex layout (cc4s_cc_backward)."""
+        S = np.zeros(self.NG)
+        g = None
+        if gradient:
+            k = 2 if self.in_complex_input else 1
+            g = np.zeros(self.NG * (self.No + self.Nv) ** 2 * k)
+        self._check(self.lib.cc4s_cc_backward(self.h, _abi.ptr(S), _abi.ptr(g)))
+        if g is not None:
+            Np = self.No + self.Nv
+            if self.in_complex_input:
+                g = g.view(np.complex128)
+            g = g.reshape((self.NG, Np, Np), order="F")
+        return S, g
 
     def stats(self):
         s = _abi.Stats()

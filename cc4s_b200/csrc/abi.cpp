@@ -206,6 +206,49 @@ void Handle::residual(const double* T1, const double* T2, double* R1, double* R2
   (void)n1;
 }
 
+// Adjoint of the energy at the current (frozen) amplitudes.
+void Handle::backward(double* S_of_G, double* dE_dGamma) {
+  require_inputs();
+  if (!have_T) throw Error(ERR_STATE, "no amplitudes: run or set initial amplitudes first");
+  if (!S_of_G && !dE_dGamma) return;
+  if (dE_dGamma && complex_path)
+    throw Error(ERR_UNSUPPORTED, "dE/dGamma is provided on the real (half-grid) path only");
+  const int64_t G = solver->aux_rows(), o = shape.o, v = shape.v, n1 = o * v;
+  double* Sd = ops::alloc(G);
+  double* dG = nullptr;
+  try {
+    if (dE_dGamma) dG = ops::alloc(G * n1);
+    solver->structure_factor(Tcur, Sd, dG);
+    std::vector<double> S(G), g;
+    ops::d2h(S.data(), Sd, G, stream);
+    if (dG) {
+      g.resize(G * n1);
+      ops::d2h(g.data(), dG, G * n1, stream);
+    }
+    ops::sync(stream);
+    const int64_t NG = in_NG, Np = in_Np;
+    if (S_of_G)
+      for (int64_t k = 0; k < NG; ++k) S_of_G[k] = S[k] + (in_stacked ? S[k + NG] : 0.0);
+    if (dE_dGamma) {
+      // caller layout Gamma[G, p, q] column-major, ph block p = No + a, q = i
+      const int64_t es = in_complex ? 2 : 1;
+      std::memset(dE_dGamma, 0, sizeof(double) * NG * Np * Np * es);
+      for (int64_t part = 0; part < (in_stacked ? 2 : 1); ++part)
+        for (int64_t k = 0; k < NG; ++k)
+          for (int64_t a = 0; a < v; ++a)
+            for (int64_t i = 0; i < o; ++i)
+              dE_dGamma[(k + NG * ((o + a) + Np * i)) * es + part] =
+                  g[((part * NG + k) * v + a) * o + i];
+    }
+  } catch (...) {
+    ops::release(Sd);
+    ops::release(dG);
+    throw;
+  }
+  ops::release(Sd);
+  ops::release(dG);
+}
+
 }  // namespace cc4s_b200
 
 // ---------------------------------------------------------------------------
@@ -302,6 +345,11 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
                      double* R2) {
   if (!h || !h->impl || !R1 || !R2) return CC4S_ERR_INVALID_ARGUMENT;
   return guarded(h, [&] { h->impl->residual(T1, T2, R1, R2); return 0; });
+}
+
+int cc4s_cc_backward(cc4s_cc_handle* h, double* S_of_G, double* dE_dGamma) {
+  if (!h || !h->impl) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] { h->impl->backward(S_of_G, dE_dGamma); return 0; });
 }
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {

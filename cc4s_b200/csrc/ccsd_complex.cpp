@@ -22,6 +22,7 @@ namespace cc4s_b200 {
 
 CcsdComplex::CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Stream s)
     : Schedule(s), sys_(sys), opt_(opt) {
+  so_ = sys.o; sv_ = sys.v; sG_ = sys.G; scplx_ = true; sGph_ = sys.Gph; sGhp_ = sys.Ghp;
   const int64_t o = sys.o, v = sys.v, G = sys.G, n1 = v * o, D2 = n1 * n1;
   if (o <= 0 || v <= 0 || G <= 0) throw Error(ERR_BAD_SHAPE, "CcsdComplex: empty dimension");
   D2_ = D2;

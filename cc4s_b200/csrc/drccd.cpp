@@ -12,6 +12,7 @@ Drccd::Drccd(int64_t o, int64_t v, int64_t G, bool complex_path, double* Gph, do
              const DrccdOptions& opt, Stream s)
     : Schedule(s), o_(o), v_(v), G_(G), D2_(o * v * o * v), cplx_(complex_path), Gph_(Gph),
       Ghp_(Ghp), opt_(opt) {
+  so_ = o; sv_ = v; sG_ = G; scplx_ = complex_path; sGph_ = Gph; sGhp_ = Ghp;
   const int64_t n1 = o * v, D2 = D2_, pl = cplx_ ? 2 : 1;
   const int64_t gi = cplx_ ? G * n1 : 0;  // imaginary plane of Gph / Ghp
   const int64_t di = cplx_ ? D2 : 0;

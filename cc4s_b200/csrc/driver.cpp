@@ -73,6 +73,10 @@ void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, in
   free_state();
   for (double* p : vertex) ops::release(p);
   vertex.clear();
+  in_NG = NG;
+  in_Np = Np;
+  in_complex = is_complex;
+  in_stacked = half_grid && has_imag;
   auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
   if (!half_grid) {
     // Complex path: planar complex slices (imaginary plane at +size, zero for real input).

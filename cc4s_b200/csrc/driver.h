@@ -23,6 +23,7 @@ struct Handle {
   int run(cc4s_cc_result* out);
   void get_amplitudes(double* T1, double* T2);
   void residual(const double* T1, const double* T2, double* R1, double* R2);
+  void backward(double* S_of_G, double* dE_dGamma);
 
   // helpers
   double* take(size_t elems);
@@ -62,6 +63,9 @@ struct Handle {
   int next_index = 0, count = 0;
   bool linear_has_last = false;
   bool have_T = false;
+  // shape of the caller's vertex (for the adjoint outputs)
+  int64_t in_NG = 0, in_Np = 0;
+  bool in_complex = false, in_stacked = false;
 };
 
 }  // namespace cc4s_b200

@@ -106,6 +106,46 @@ void Schedule::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bo
   if (!wrote) throw Error(ERR_STATE, "zgemm: complex result from real operands");
 }
 
+void Schedule::structure_factor(const double* T, double* S_dev, double* dGph_dev) {
+  const int64_t o = so_, v = sv_, G = sG_, n1 = o * v, D2 = n1 * n1;
+  if (!T || !sGph_) throw Error(ERR_STATE, "structure factor: no amplitudes or vertex");
+  const int64_t planes = scplx_ ? 2 : 1, pl = n1 + D2;
+  if (!adjX_) {
+    adjX_ = take(2 * planes * D2);
+    adjW_ = take(planes * G * n1);
+  }
+  double* X = adjX_;             // X = T2 + T1 T1, then M = 2X - X^x
+  double* M = adjX_ + planes * D2;
+  const double* t = T;
+  const double* Td = T + n1;
+  if (scplx_) ops::zrank1(X, X + D2, Td, Td + pl, t, t + pl, 1.0, n1, s_);
+  else ops::rank1(X, 1.0, Td, 1.0, t, n1, s_);
+  const int64_t d4[4] = {v, o, v, o};
+  const int p_ex[4] = {0, 3, 2, 1};
+  for (int64_t p = 0; p < planes; ++p) {
+    ops::permute4(M + p * D2, X + p * D2, d4, p_ex, -1.0, 0.0, s_);
+    ops::axpby(M + p * D2, 2.0, X + p * D2, 1.0, M + p * D2, 0.0, D2, s_);
+  }
+  const int64_t gi = scplx_ ? G * n1 : 0, mi = scplx_ ? D2 : 0;
+  {  // W[G][(a,i)] = sum_{b,j} Gamma^hp_Gjb M[(b,j),(a,i)]
+    Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
+    c.A = vw(sGhp_, 0, n1, 1, v); c.B = vw(M, o * n1, n1, 0, 1); c.C = rm(adjW_, n1);
+    zgemm(c, gi, mi, gi, false, false, true);
+  }
+  {  // S[G] = Re sum_r conj(Gamma^ph_G,r) W_G,r   (batched dot products)
+    Contraction c; c.M = 1; c.N = 1; c.K = n1; c.batch = G;
+    c.A = vw(sGph_, 0, 0, 0, 1, 0, n1); c.B = vw(adjW_, 0, 1, 0, 0, 0, n1);
+    c.C = vw(S_dev, 0, 0, 0, 0, 0, 1);
+    zgemm(c, gi, gi, 0, scplx_, false);
+  }
+  if (dGph_dev) {
+    if (scplx_) throw Error(ERR_UNSUPPORTED, "dE/dGamma is provided on the real path only");
+    Contraction c; c.M = G; c.N = n1; c.K = n1;  // dE/dGph = 2 Gph M
+    c.A = rm(sGph_, n1); c.B = rm(M, n1); c.C = rm(dGph_dev, n1); c.alpha = 2.0;
+    tc_(c);
+  }
+}
+
 int Schedule::device_error() {
   if (!split_.error) return 0;
   double v = 0.0;

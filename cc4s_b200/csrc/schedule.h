@@ -44,6 +44,15 @@ class Schedule {
   void set_precision(int slices) { precision_ = slices; }
   // Non-zero if a bounded wait inside a tensor-core kernel expired (synchronises).
   int device_error();
+
+  // Adjoint of the energy at frozen amplitudes T (amplitude-vector layout):
+  //   S_dev[G]    = Re sum conj(G^ph_Gai) G^hp_Gjb (2 X_abij - X_abji), the transition
+  //                 structure factor of FiniteSizeCorrection.cxx:113-125 (= dE/dV(G));
+  //   dGph_dev    = dE/dGamma^ph_Gai = 2 sum_bj (2X - X^x)[(a,i),(b,j)] Gamma^ph_Gbj
+  //                 (real path only; may be null).
+  // G runs over the schedule's auxiliary rows (stacked Re/Im rows on the real path).
+  void structure_factor(const double* T, double* S_dev, double* dGph_dev);
+  int64_t aux_rows() const { return sG_; }
   struct Profile {
     double gemm_seconds = 0, gemm_flops = 0;  // all contractions of the last residual
     double top_seconds = 0, top_flops = 0;    // the most expensive single launch
@@ -69,6 +78,13 @@ class Schedule {
   int precision_ = 0;
   SplitScratch split_;
   double* split_mem_ = nullptr;
+  // vertex description for the adjoint (set by each schedule)
+  int64_t so_ = 0, sv_ = 0, sG_ = 0;
+  bool scplx_ = false;
+  double* sGph_ = nullptr;
+  double* sGhp_ = nullptr;
+  double* adjX_ = nullptr;
+  double* adjW_ = nullptr;
   void release_all();
 
   Stream s_;

@@ -144,6 +144,18 @@ int cc4s_cc_get_amplitudes(cc4s_cc_handle* h, double* T1, double* T2);
 int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, double* R1,
                      double* R2);
 
+/* Adjoint form, at the current (frozen) amplitudes — after cc4s_cc_run or
+ * cc4s_cc_set_initial_amplitudes.  Replaces the transition structure factor of
+ * FiniteSizeCorrection::calculateTransitionStructureFactor
+ * (src/main/algorithms/FiniteSizeCorrection.cxx:50-133) with unit singular
+ * vectors and Coulomb potential:
+ *   S_of_G[G] = Re sum conj(Gamma_G,ai) Gamma_G,jb (2 Tt_abij - Tt_abji),
+ *   Tt = T2 + T1 T1, which is dE_c/dV(G) when Gamma_G scales as sqrt(V(G)).
+ * dE_dGamma (optional, real half-grid path only): the gradient of E_c with
+ * respect to the caller's vertex Gamma[G,p,q] (same layout; complex input gives
+ * d/dRe + i d/dIm), nonzero in the particle-hole block.  Either output may be NULL. */
+int cc4s_cc_backward(cc4s_cc_handle* h, double* S_of_G, double* dE_dGamma);
+
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
 
 /* Correlation energy of amplitudes that already live in device memory, computed
@@ -164,7 +176,6 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
  * cudaStream_t (NULL: the legacy default stream).  Errors: cc4s_cc_last_error(NULL). */
 int cc4s_cc_energy_noalloc(const double* T1, const double* T2, const double* Vpphh, int64_t No,
                            int64_t Nv, int is_complex, double* energy, void* stream);
-
 
 /* Releases the handle and its device memory. */
 int cc4s_cc_destroy(cc4s_cc_handle* h);

@@ -173,6 +173,44 @@ def test_split_precision_energy_within_1ueh(Solver, shape):
     assert abs(ra["correlation"] - rb["correlation"]) < 1e-6
 
 
+@pytest.mark.parametrize("cfg", ["c0", "complex"])
+def test_backward_structure_factor(Solver, cfg):
+    """S(G) = dE_c/dV(G) at frozen amplitudes: equals the restated reference
+    structure factor (FiniteSizeCorrection.cxx:113-125) and central finite
+    differences in V(G) (Gamma_G scaled by sqrt(V(G))) to 1e-6 relative."""
+    from oracle.inputs import coulomb_integrals
+    if cfg == "c0":
+        s = inputs.config_system("c0", seed=0)
+    else:
+        s = inputs.synthetic_system(6, 30, 40, complex=True, seed=4)
+    cplx = cfg != "c0"
+    sol = Solver(dict(maxIterations=40, energyConvergence=1e-10))
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+    r = sol.run()
+    T = sol.amplitudes()
+    S, g = sol.backward(gradient=not cplx)
+    S0 = properties.structure_factor(s, T)
+    assert _rel(S, S0) < 1e-11
+    assert abs(S.sum() - r["correlation"]) < TOL_E
+
+    def energy_of(gm):  # E_c at the frozen amplitudes for vertex gm
+        ss = inputs.System(s.eps_h, s.eps_p, gm, s.half_grid)
+        return np.real(coupled_cluster.get_energy(T, coulomb_integrals(ss, ["pphh"])["pphh"])[0])
+
+    h = 1e-5
+    for G in (0, s.NG // 2, s.NG - 1):
+        up, dn = np.ones(s.NG), np.ones(s.NG)
+        up[G] += h
+        dn[G] -= h
+        fd = (energy_of(s.gamma * np.sqrt(up)[:, None, None]) -
+              energy_of(s.gamma * np.sqrt(dn)[:, None, None])) / (2 * h)
+        assert abs(S[G] - fd) < 1e-6 * max(abs(fd), 1e-12)
+    if not cplx:
+        d = np.random.default_rng(0).standard_normal(s.gamma.shape)
+        fd = (energy_of(s.gamma + h * d) - energy_of(s.gamma - h * d)) / (2 * h)
+        assert abs((g * d).sum() - fd) < 1e-6 * abs(fd)
+
+
 def test_complex_run(Solver):
     s = inputs.synthetic_system(6, 30, 60, complex=True, seed=5)
     o = dict(maxIterations=30, energyConvergence=1e-10, amplitudesConvergence=1e-8)
