@@ -167,14 +167,16 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   d |= static_cast<uint64_t>(4) << 61;                       // SWIZZLE_64B
   return d;
 }
-// Instruction descriptor: D = F32, A = B = F16, both K-major, N = 128, M = 128.
-constexpr uint32_t IDESC = (1u << 4) | ((TN >> 3) << 17) | ((TM >> 4) << 24);
+// Instruction descriptors: D = F32, A = B = F16, both K-major, M = 128, N = 128 or 256.
+constexpr uint32_t IDESC128 = (1u << 4) | ((TN >> 3) << 17) | ((TM >> 4) << 24);
+constexpr uint32_t IDESC256 = (1u << 4) | (((2 * TN) >> 3) << 17) | ((TM >> 4) << 24);
 
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                     uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-      ::"r"(tmem_d), "l"(da), "l"(db), "r"(IDESC), "r"(acc));
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
@@ -281,19 +283,20 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         for (int kk = 0; kk < TK / 16; ++kk) {
           // 32 bytes per 16-element K step inside the 64-byte swizzled rows
           const uint32_t koff = kk * 32;
-          // group 0: (1,1); group 1: (1,2),(2,1); group 2: (1,3),(2,2),(3,1)
-#pragma unroll
-          for (int pa = 0; pa < NSLICE; ++pa)
-#pragma unroll
-            for (int pb = 0; pb < NSLICE; ++pb) {
-              if (pa + pb > NSLICE - 1) continue;
-              const int grp = pa + pb;
-              const uint64_t da = sdesc(st + pa * TILE_BYTES + koff);
-              const uint64_t db = sdesc(st + (NSLICE + pb) * TILE_BYTES + koff);
-              // the first product of each group in a chunk overwrites the accumulator
-              const bool init = first && kk == 0 && (pa == 0);
-              umma(tmem + grp * TN, da, db, init ? 0u : 1u);
-            }
+          // Groups of equal weight live at TMEM columns 0 (S1S1), 128 (S1S2 + S2S1)
+          // and 256 (S1S3 + S2S2 + S3S1).  B slices 1 and 2 are adjacent in shared
+          // memory, so A_p x [B1 | B2] is one N = 256 MMA into groups p and p+1.
+          const uint32_t init = (first && kk == 0) ? 0u : 1u;
+          const uint64_t a1 = sdesc(st + 0 * TILE_BYTES + koff);
+          const uint64_t a2 = sdesc(st + 1 * TILE_BYTES + koff);
+          const uint64_t a3 = sdesc(st + 2 * TILE_BYTES + koff);
+          const uint64_t b12 = sdesc(st + (NSLICE + 0) * TILE_BYTES + koff);
+          const uint64_t b1 = b12;
+          const uint64_t b3 = sdesc(st + (NSLICE + 2) * TILE_BYTES + koff);
+          umma(tmem + 0 * TN, a1, b12, IDESC256, init);  // S1 x [S1|S2] -> groups 0, 1
+          umma(tmem + 2 * TN, a1, b3, IDESC128, init);   // S1 x S3      -> group 2
+          umma(tmem + 1 * TN, a2, b12, IDESC256, 1u);    // S2 x [S1|S2] -> groups 1, 2
+          umma(tmem + 2 * TN, a3, b1, IDESC128, 1u);     // S3 x S1      -> group 2
         }
         umma_commit(smem_u32(&bars[NST + s]));  // stage free once these MMAs retire
         first = false;
