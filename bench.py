@@ -112,37 +112,41 @@ def dgemm_peak(device):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_sample(cfg):
+def cpu_sample(cfg, target=2e12):
     """CPU rate of the oracle on the workload's dominant contractions (bounded sample).
 
-    Times one (vo)^3 ring contraction and one particle-particle-ladder slice pair
-    of the workload with the oracle's numpy/BLAS restatement on all host cores,
-    and converts the measured rate into seconds per iteration of the reference
-    formulation.
+    Times, with the oracle's numpy/BLAS restatement on all host cores, a block of
+    the (vo)^3 ring contraction (virtual indices a, b restricted to n values) and
+    one particle-particle-ladder slice pair (sl x sl virtual pairs, occupied pairs
+    restricted to m x m), each sized to about `target` flops, on random operands
+    of the workload's shapes; the measured rate converts the reference
+    formulation's flops into seconds per iteration.
     """
     import numpy as np
-    from oracle import ccsd as occ, inputs as oin
+    from oracle import ccsd as occ
     from cc4s_b200.flops import reference_flops
     o, v, G = CONFIG_SHAPES[cfg]
-    s = oin.config_system(cfg, seed=0)
     rng = np.random.default_rng(0)
-    X = rng.standard_normal((v, v, o, o))
-    Y = rng.standard_normal((v, o, o, v))
+    n = int(min(v, max(1, (target / (2.0 * v * o ** 3)) ** 0.5)))
+    Y = rng.standard_normal((n, o, o, v))
+    X = rng.standard_normal((v, n, o, o))
+    m = min(o, 16)
+    sl = int(min(o, max(1, (target / (2.0 * v * v * (G + m * m))) ** 0.5)))
+    dG = rng.standard_normal((G, 2 * sl, v)) * 0.1 * G ** -0.25
+    Xl = rng.standard_normal((v, v, m, m))
     t0 = time.perf_counter()
     occ.es("akic,cbkj->abij", Y, X)
+    V = occ.es("Gxc,Gyd->xycd", dG[:, :sl, :], dG[:, sl:, :])
+    occ.es("xycd,cdij->xyij", V, Xl)
     t1 = time.perf_counter()
-    dG = np.ascontiguousarray(s.gamma[:, o:, o:])
-    sl = o
-    V = occ.es("Gxc,Gyd->xycd", dG[:, :sl, :], dG[:, sl:2 * sl, :])
-    occ.es("xycd,cdij->xyij", V, X)
-    t2 = time.perf_counter()
-    flops = 2.0 * v ** 3 * o ** 3 + 2.0 * sl * sl * v * v * (G + o * o)
-    rate = flops / (t2 - t0)
+    flops = 2.0 * n * n * v * o ** 3 + 2.0 * sl * sl * v * v * (G + m * m)
+    rate = flops / (t1 - t0)
     s_iter = reference_flops(o, v, G) / rate
-    return dict(s_per_iter=s_iter, rate_tflops=rate / 1e12, sample_seconds=t2 - t0,
+    return dict(s_per_iter=s_iter, rate_tflops=rate / 1e12, sample_seconds=t1 - t0,
                 cores=os.cpu_count(),
-                sample="oracle numpy/BLAS on one (vo)^3 ring contraction and one ladder slice "
-                       "pair (s=No) of %s; s/iter = reference flops / measured rate" % cfg)
+                sample="oracle numpy/BLAS on %s: ring block a,b < %d of akic,cbkj->abij and one "
+                       "ladder slice pair (%d x %d virtuals, %d x %d occupied pairs), %.2g flops; "
+                       "s/iter = reference flops / measured rate" % (cfg, n, sl, sl, m, m, flops))
 
 
 def dist_setup():
@@ -177,7 +181,7 @@ def barrier(world):
         dist.barrier()
 
 
-def timed_run(opts, inputs, W, K, world, local):
+def timed_run(opts, inputs, W, K, world, local, keep_amplitudes=True):
     """W + K iterations; the last K are timed (CUDA events on the library stream)."""
     from cc4s_b200 import Solver
     eh, ep, g, hg = inputs
@@ -193,7 +197,7 @@ def timed_run(opts, inputs, W, K, world, local):
     t = all_max(sum(secs[W:W + K]), world)
     launches = ((st1["gemm_launches"] - st0["gemm_launches"]) +
                 (st1["other_launches"] - st0["other_launches"])) / (W + K)
-    T = sol.amplitudes()
+    T = sol.amplitudes() if keep_amplitudes else None
     sol.close()
     return dict(t=t, r=r, launches=launches, T=T, clocks=clk.summary())
 
@@ -212,14 +216,18 @@ def run_ours(args, world, rank, local):
     base = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
                 mixer=dict(type="DiisMixer", maxResidua=5), device=local)
     forms = ["fp64", "split3"] if args.precision == "both" else [args.precision]
-    runs = {p: timed_run(dict(base, precision=p), inputs, W, K, world, local) for p in forms}
-    head = "split3" if "split3" in runs else "fp64"
+    head = "split3" if "split3" in forms else "fp64"
+    runs = {p: timed_run(dict(base, precision=p), inputs, W, K, world, local,
+                         keep_amplitudes=(p == head)) for p in forms}
     hr = runs[head]
     t = hr["t"]
-    # dominant kernel: per-launch CUDA events around every contraction of one residual
+    # dominant kernel: per-launch CUDA events around every contraction of one
+    # residual, evaluated at the amplitudes the timed run ended with
     prof = Solver(dict(base, precision=head, profile=True, maxIterations=1))
     prof.set_inputs(eh, ep, g, half_grid=hg)
-    prof.residual(hr["T"])
+    prof.set_initial_amplitudes(*hr["T"])
+    hr["T"] = None
+    prof.run()
     ps = prof.stats()
     prof.close()
     pk = peaks()
@@ -290,8 +298,8 @@ def run_reference(args, world, rank):
     o, v, G = CONFIG_SHAPES[cfg]
     from cc4s_b200.flops import reference_flops
     F = reference_flops(o, v, G)
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
+    for _ in range(args.warmup):
+        cpu_sample(cfg)
     samples = [cpu_sample(cfg) for _ in range(max(1, args.steps))]
     s_iter = statistics.median(x["s_per_iter"] for x in samples)
     c = samples[0]

@@ -14,9 +14,8 @@ int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t 
 
 // Reference layout T1[a,i], T2[a,b,i,j] (first index fastest) -> amplitude vector.
 // Complex host buffers are interleaved (re, im); device vectors are planar.
-void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2) {
+void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2, double* st) {
   const int64_t o = shape.o, v = shape.v, n1 = v * o, pl = shape.plane();
-  double* st = Rs[0];
   std::vector<double> h1, h2;
   for (int64_t p = 0; p < shape.planes; ++p) {
     const double* s1 = T1;
@@ -41,9 +40,8 @@ void Handle::upload_amplitudes(double* dst, const double* T1, const double* T2) 
   }
 }
 
-void Handle::download_amplitudes(const double* src, double* T1, double* T2) {
+void Handle::download_amplitudes(const double* src, double* T1, double* T2, double* st) {
   const int64_t o = shape.o, v = shape.v, n1 = v * o, pl = shape.plane();
-  double* st = Rs[0];
   std::vector<double> h1, h2;
   for (int64_t p = 0; p < shape.planes; ++p) {
     const int64_t d1[4] = {1, 1, v, o};
@@ -76,7 +74,7 @@ void Handle::set_initial(const double* T1, const double* T2) {
     if (!std::isfinite(T1[k])) throw Error(ERR_NON_FINITE, "non-finite T1");
   for (int64_t k = 0; k < n1 * n1 * np; ++k)
     if (!std::isfinite(T2[k])) throw Error(ERR_NON_FINITE, "non-finite T2");
-  upload_amplitudes(Tcur, T1, T2);
+  upload_amplitudes(Tcur, T1, T2, Rbuf);
   ops::sync(stream);
   have_T = true;
 }
@@ -104,7 +102,7 @@ void Handle::mix(double* A_new, double* dT_new, double* norm2_dev) {
   int ny = 0;
   for (int i = 0; i < N; ++i)
     if (valid[i]) ys[ny++] = Rs[i];
-  ops::dots(Rs[next], ys, ny, n, scal + 8, ws, stream);
+  ops::dots_packed(Rs[next], ys, ny, shape, scal + 8, ws, stream);
   if (count < N) ++count;
   ops::diis_solve(B, scal + 8, valid.data(), N, next, count, coef, status_dev, stream);
   const double* xs[16];
@@ -114,7 +112,7 @@ void Handle::mix(double* A_new, double* dT_new, double* norm2_dev) {
     xs[j] = A[slot];
     rs[j] = Rs[slot];
   }
-  ops::lincomb(Tcur, xs, rs, coef, count, n, norm2_dev, ws, stream);
+  ops::lincomb_packed(Tcur, xs, rs, coef, count, shape, norm2_dev, ws, stream);
   next_index = (next + 1) % N;
 }
 
@@ -134,8 +132,12 @@ int Handle::run(cc4s_cc_result* out) {
     ops::event_record(ev0, stream);
     solver->residual(have_T ? Tcur : nullptr, Rbuf);
     const int slot = opt.mixer == CC4S_MIXER_DIIS ? next_index : 0;
-    ops::jacobi(A[slot], Rs[slot], Rbuf, have_T ? Tcur : nullptr, sys.eh, sys.ep, shape, shift,
-                stream);
+    if (opt.mixer == CC4S_MIXER_DIIS)
+      ops::jacobi_packed(A[slot], Rs[slot], Rbuf, have_T ? Tcur : nullptr, sys.eh, sys.ep, shape,
+                         shift, stream);
+    else
+      ops::jacobi(A[slot], Rs[slot], Rbuf, have_T ? Tcur : nullptr, sys.eh, sys.ep, shape, shift,
+                  stream);
     const bool second = !have_T;
     mix(A[slot], Rs[slot], scal + 4);
     have_T = true;
@@ -190,19 +192,28 @@ int Handle::run(cc4s_cc_result* out) {
 void Handle::get_amplitudes(double* T1, double* T2) {
   require_inputs();
   if (!have_T) throw Error(ERR_STATE, "no amplitudes: run first");
-  download_amplitudes(Tcur, T1, T2);
+  download_amplitudes(Tcur, T1, T2, Rbuf);
 }
 
 void Handle::residual(const double* T1, const double* T2, double* R1, double* R2) {
   require_inputs();
   const int64_t n1 = shape.n1();
   const bool first = (T1 == nullptr && T2 == nullptr);
-  if (!first) {
-    if (!T1 || !T2) throw Error(ERR_INVALID_ARGUMENT, "give both T1 and T2, or neither");
-    upload_amplitudes(A[0], T1, T2);
+  if (!first && (!T1 || !T2))
+    throw Error(ERR_INVALID_ARGUMENT, "give both T1 and T2, or neither");
+  // The caller's amplitudes go to a temporary device vector (also the staging
+  // buffer of the layout change), so the handle's current amplitudes and mixer
+  // history stay as they were.
+  double* Tin = ops::alloc(shape.total());
+  try {
+    if (!first) upload_amplitudes(Tin, T1, T2, Rbuf);
+    solver->residual(first ? nullptr : Tin, Rbuf);
+    download_amplitudes(Rbuf, R1, R2, Tin);
+  } catch (...) {
+    ops::release(Tin);
+    throw;
   }
-  solver->residual(first ? nullptr : A[0], Rbuf);
-  download_amplitudes(Rbuf, R1, R2);
+  ops::release(Tin);
   (void)n1;
 }
 

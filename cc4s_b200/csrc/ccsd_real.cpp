@@ -5,9 +5,11 @@
 // Layouts (row-major, all FP64):
 //   T1, R1        [a][i]                         (v x o)
 //   T2, R2 "pair" [a][i][b][j]  = X_abij          ((vo) x (vo), symmetric matrix)
-//   "exchange"    Ae[a][i][b][j] = A_abji          (pair layout with i <-> j)
-//   "pp"          Ap[a][b][i][j] = A_abij
 //   vertex        Gpp[G][a][b], Gph[G][a][i], Ghh[G][k][i], Ghp[G][i][a]
+// Only four (vo)^2 buffers are stored besides T and R (Vd, X, Y, EX): the other
+// pairings a contraction needs -- exchange A_abji, pp order A_abij with (a,b) and
+// (i,j) as matrix indices -- are two-level strided views of the pair layout
+// (strides a: o*vo, i: vo, b: o, j: 1), which the contraction kernels read directly.
 //
 // Exact algebraic rearrangements relative to the reference (each term is the
 // same sum, only the contraction order changes):
@@ -40,10 +42,10 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
     scratch_.elems = static_cast<size_t>(std::max<int64_t>(int64_t(1) << 22,
                                                            std::min<int64_t>(64 * v * v, int64_t(1) << 25)));
     scratch_.p = take(scratch_.elems);
-    Vd_ = take(D2); Ve_ = take(D2); Vp_ = take(D2); Vtp_ = take(D2);
+    Vd_ = take(D2);
     Vhhhh_ = take(o * o * o * o); Vhhhp_ = take(o * o * o * v); Vh2_ = take(o * o * o * v);
-    Xd_ = take(D2); Xp_ = take(D2); Te_ = take(D2); Y_ = take(D2); W8_ = take(D2);
-    Tp_ = take(D2); EX_ = take(D2);
+    Xd_ = take(D2); Y_ = take(D2); EX_ = take(D2);
+    W8_ = EX_;
     Kki_ = take(o * o); Kac_ = take(v * v); Lac_ = take(v * v); Lki_ = take(o * o);
     jG_ = take(G);
     U_ = take(G * n1); dGph_ = take(G * n1); W_ = take(G * n1); Z_ = take(G * n1);
@@ -79,17 +81,6 @@ void CcsdReal::build_integrals() {
     c.A = tr(sys_.Gph, n1); c.B = rm(sys_.Gph, n1); c.C = rm(Vd_, n1);
     gemm_(c);
   }
-  const int64_t d4[4] = {v, o, v, o};
-  // Ve[(a,i),(b,j)] = V_baij = V_abji ; Vp[a][b][i][j] = V_abij
-  { const int pm[4] = {0, 3, 2, 1}; ops::permute4(Ve_, Vd_, d4, pm, 1.0, 0.0, s_); }
-  { const int pm[4] = {0, 2, 1, 3}; ops::permute4(Vp_, Vd_, d4, pm, 1.0, 0.0, s_); }
-  // Vtp[c][d][k][l] = 2 V_cdkl - V_dckl = 2 Vp[c][d][k][l] - Vp[c][d][l][k]
-  {
-    const int64_t dp[4] = {v, v, o, o};
-    const int pm[4] = {0, 1, 3, 2};
-    ops::permute4(Vtp_, Vp_, dp, pm, -1.0, 0.0, s_);
-    ops::axpby(Vtp_, 2.0, Vp_, 1.0, Vtp_, 0.0, n1 * n1, s_);
-  }
   // Vhhhh[k][l][i][j] = sum_G Ghh[G][k][i] Ghh[G][l][j]
   {
     Contraction c; c.M = o * o; c.N = o * o; c.K = G; c.Mi = o; c.Ni = o;
@@ -106,11 +97,11 @@ void CcsdReal::build_integrals() {
     c.C = vw(Vhhhp_, o * o * v, v, o * v, 1);
     gemm_(c);
   }
-  // Vh2[i][c][k][l] = 2 V_klic - V_lkic
+  // Vh2[i][k][c][l] = 2 V_klic - V_lkic
   {
     const int64_t dh[4] = {o, o, o, v};
-    const int pa[4] = {2, 3, 0, 1};
-    const int pb[4] = {2, 3, 1, 0};
+    const int pa[4] = {2, 0, 3, 1};
+    const int pb[4] = {2, 1, 3, 0};
     ops::permute4(Vh2_, Vhhhp_, dh, pa, 2.0, 0.0, s_);
     ops::permute4(Vh2_, Vhhhp_, dh, pb, -1.0, 1.0, s_);
   }
@@ -133,25 +124,30 @@ void CcsdReal::residual(const double* T, double* R) {
   double* Gph = sys_.Gph;
   double* Ghh = sys_.Ghh;
   const int64_t d4[4] = {v, o, v, o};
-  const int p_pp[4] = {0, 2, 1, 3};   // pair -> pp
-  const int p_ex[4] = {0, 3, 2, 1};   // pair -> exchange
+  const int p_ex[4] = {0, 3, 2, 1};   // pair -> exchange (i <-> j)
+  // strides of the pair layout [a][i][b][j]
+  const int64_t sA = o * n1, sI = n1, sB = o;
 
   // ---- X = T2 + T1 T1 (Ccsd.cxx:169-170) -----------------------------------
   if (ccd) ops::d2d(Xd_, Td, D2, s_);
   else ops::rank1(Xd_, 1.0, Td, 1.0, t, n1, s_);
-  ops::permute4(Xp_, Xd_, d4, p_pp, 1.0, 0.0, s_);
 
   // ---- Kki, Kac (Ccsd.cxx:172-178) -------------------------------------------
-  {  // Kki[k][i] = sum_{cd,l} Vtp[cd][k][l] Xp[cd][i][l]
-    Contraction c; c.M = o; c.N = o; c.K = v * v * o; c.Ki = o;
-    c.A = vw(Vtp_, 0, o, o * o, 1);
-    c.B = vw(Xp_, o * o, 1, 0, o);
+  // EX <- Vt[(c,k),(d,l)] = 2 V_cdkl - V_cdlk  (= 2 V_cdkl - V_dckl)
+  ops::permute4(EX_, Vd_, d4, p_ex, -1.0, 0.0, s_);
+  ops::axpby(EX_, 2.0, Vd_, 1.0, EX_, 0.0, D2, s_);
+  {  // Kki[k][i] = sum_{c,(d,l)} Vt[(c,k),(d,l)] X[(c,i),(d,l)]
+    Contraction c; c.M = o; c.N = o; c.K = v * n1; c.Ki = n1;
+    c.A = vw(EX_, 0, sI, sA, 1);
+    c.B = vw(Xd_, sA, 1, 0, sI);
     c.C = rm(Kki_, o);
     gemm_(c);
   }
-  {  // Kac[a][c] = -sum_{dkl} Xp[a][dkl] Vtp[c][dkl]
-    Contraction c; c.M = v; c.N = v; c.K = v * o * o;
-    c.A = rm(Xp_, v * o * o); c.B = tr(Vtp_, v * o * o); c.C = rm(Kac_, v);
+  {  // Kac[a][c] = -sum_{k,(d,l)} X[(a,k),(d,l)] Vt[(c,k),(d,l)]
+    Contraction c; c.M = v; c.N = v; c.K = o * n1; c.Ki = n1;
+    c.A = vw(Xd_, 0, sA, sI, 1);
+    c.B = vw(EX_, sI, 1, 0, sA);
+    c.C = rm(Kac_, v);
     c.alpha = -1.0;
     gemm_(c);
   }
@@ -189,7 +185,7 @@ void CcsdReal::residual(const double* T, double* R) {
   ops::d2d(Lki_, Kki_, o * o, s_);
   if (!ccd) {  // Lki[k][i] += sum_{c,l} (2 V_klic - V_lkic) t[c][l]
     Contraction c; c.M = o * o; c.N = 1; c.K = v * o; c.Mi = o; c.Ki = o;
-    c.A = vw(Vh2_, v * o * o, o, o * o, 1);
+    c.A = vw(Vh2_, v * o * o, v * o, o, 1);   // Vh2[i][k][c][l]: m = (i,k), k = (c,l)
     c.B = vw(t, o, 1, 0, 0);
     c.C = vw(Lki_, 1, o, 0, 0);
     c.beta = 1.0;
@@ -247,12 +243,12 @@ void CcsdReal::residual(const double* T, double* R) {
     }
   }
   // ---- ring Xakic (Ccsd.cxx:215-229) -------------------------------------------
-  ops::permute4(Te_, Td, d4, p_ex, 1.0, 0.0, s_);                 // Te = T^x
   if (ccd) ops::d2d(W8_, Td, D2, s_);
   else ops::rank1(W8_, 1.0, Td, 2.0, t, n1, s_);                 // X' = T2 + 2 T1 T1
   ops::permute4(Y_, W8_, d4, p_ex, 1.0, 0.0, s_);                 // X'^x
   ops::axpby(W8_, 1.0, Td, -0.5, Y_, 0.0, D2, s_);               // M1 = T - X'^x / 2
-  ops::axpby(Y_, 2.0, Td, -1.0, Te_, 0.0, D2, s_);               // Y = 2T - T^x
+  ops::permute4(Y_, Td, d4, p_ex, -1.0, 0.0, s_);                 // -T^x
+  ops::axpby(Y_, 2.0, Td, 1.0, Y_, 0.0, D2, s_);                 // Y = 2T - T^x
   {  // Z = Gph M1
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(Z_, n1);
@@ -275,9 +271,12 @@ void CcsdReal::residual(const double* T, double* R) {
     c.A = tr(dGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
     tc_(c);
   }
-  {  // EX = -1/2 T Ve
-    Contraction c; c.M = n1; c.N = n1; c.K = n1;
-    c.A = rm(Td, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
+  {  // EX[(a,i),(c,k)] = -1/2 sum_{(b,j)} T[(a,i),(b,j)] V_bckj,  V_bckj = Vd[(b,k),(c,j)]
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Ki = o; c.Ni = o;
+    c.A = vw(Td, 0, n1, o, 1);
+    c.B = vw(Vd_, sA, 1, sB, sI);
+    c.C = vw(EX_, 0, n1, o, 1);
+    c.alpha = -0.5;
     tc_(c);
   }
   {  // R2 += EX Y
@@ -302,9 +301,12 @@ void CcsdReal::residual(const double* T, double* R) {
       gemm_(c);
     }
   }
-  {  // EX = -1/2 T^x Ve
-    Contraction c; c.M = n1; c.N = n1; c.K = n1;
-    c.A = rm(Te_, n1); c.B = rm(Ve_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
+  {  // EX[(a,i),(c,k)] = -1/2 sum_{(b,j)} T_abji V_bckj = -1/2 T^x Ve (views of T and Vd)
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ki = o; c.Ni = o;
+    c.A = vw(Td, sA, 1, sB, sI);
+    c.B = vw(Vd_, sA, 1, sB, sI);
+    c.C = vw(EX_, sA, sI, o, 1);
+    c.alpha = -0.5;
     tc_(c);
   }
   {  // EX[a][i][c][k] += sum_G dGpp[G][a][c] dGhh[G][k][i]      (m = (a,c), n = (k,i))
@@ -322,10 +324,10 @@ void CcsdReal::residual(const double* T, double* R) {
     tc_(c);
   }
   {  // R2_abij -= sum_ck T_ackj X_bkci : exchange pairing m = (a,j), n = (b,i)
-    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
-    c.A = vw(Te_, o * n1, n1, 0, 1);
-    c.B = vw(EX_, 0, 1, o * n1, n1);
-    c.C = vw(R2, o * n1, 1, o, n1);
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o; c.Ki = o;
+    c.A = vw(Td, sA, 1, sB, sI);           // T_ackj = T[(a,k),(c,j)]
+    c.B = vw(EX_, sB, 1, sA, sI);          // X_bkci = EX[(b,i),(c,k)]
+    c.C = vw(R2, sA, 1, sB, sI);
     c.alpha = -1.0; c.beta = 1.0;
     tc_(c);
   }
@@ -349,25 +351,26 @@ void CcsdReal::residual(const double* T, double* R) {
       gemm_(c);
     }
   }
-  ops::permute4(Tp_, Td, d4, p_pp, 1.0, 0.0, s_);
-  {  // Xkl2[kl][ij] = sum_cd V_cdkl X_cdij
-    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
-    c.A = tr(Vp_, o * o); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
+  {  // Xkl2[kl][ij] = sum_cd V_cdkl X_cdij  (m = (k,l), k = (c,d), n = (i,j))
+    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v; c.Mi = o; c.Ki = v; c.Ni = o;
+    c.A = vw(Vd_, sI, 1, sA, sB);          // V_cdkl = Vd[(c,k),(d,l)]
+    c.B = vw(Xd_, sA, sB, sI, 1);          // X_cdij = X[(c,i),(d,j)]
+    c.C = vw(Xkl2_, o * o * o, o * o, o, 1);
     tc_(c);
   }
-  {  // R2 += Xkl1 X_abkl  (m = (a,b), n = (i,j))
-    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
-    c.A = vw(Xp_, v * o * o, o * o, 0, 1);
-    c.B = vw(Xkl1_, 0, o * o, o, 1);
-    c.C = vw(R2, o * n1, o, n1, 1);
+  {  // R2 += Xkl1 X_abkl  (m = (a,b), k = (k,l), n = (i,j))
+    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ki = o; c.Ni = o;
+    c.A = vw(Xd_, sA, sB, sI, 1);          // X_abkl = X[(a,k),(b,l)]
+    c.B = vw(Xkl1_, o * o * o, o * o, o, 1);
+    c.C = vw(R2, sA, sB, sI, 1);
     c.beta = 1.0;
     tc_(c);
-    c.A.p = opt_.ppl ? Tp_ : Xp_;
+    c.A.p = opt_.ppl ? cp(Td) : Xd_;       // T_abkl (ppl) or X_abkl, same view
     c.B.p = Xkl2_;
     tc_(c);
   }
   // ---- particle-particle ladder (Ccsd.cxx:283-333) ------------------------------
-  if (opt_.ppl) ppl(Xp_, R2, dGpp_);
+  if (opt_.ppl) ppl(Xd_, R2, dGpp_);
   if (ccd) {
     ops::zero(R1, n1, s_);
     profile_finish();
@@ -384,12 +387,16 @@ void CcsdReal::residual(const double* T, double* R) {
     c.A = rm(t, o); c.B = rm(Kki_, o); c.C = rm(R1, o); c.alpha = -1.0; c.beta = 1.0;
     gemm_(c);
   }
-  {  // kck = 2 Vd t - Ve t
+  {  // kck = 2 Vd t - Ve t,  Ve[(a,i),(b,j)] = V_abji = Vd[(a,j),(b,i)]
     Contraction c; c.M = n1; c.N = 1; c.K = n1;
     c.A = rm(Vd_, n1); c.B = vw(t, 0, 1, 0, 0); c.C = vw(kck_, 0, 1, 0, 0); c.alpha = 2.0;
     gemm_(c);
-    c.A = rm(Ve_, n1); c.alpha = -1.0; c.beta = 1.0;
-    gemm_(c);
+    Contraction e; e.M = n1; e.N = 1; e.K = n1; e.Mi = o; e.Ki = o;
+    e.A = vw(Vd_, sA, 1, sB, sI);
+    e.B = vw(t, o, 1, 0, 0);
+    e.C = vw(kck_, o, 1, 0, 0);
+    e.alpha = -1.0; e.beta = 1.0;
+    gemm_(e);
   }
   {  // R1 += (2T - T^x) kck
     Contraction c; c.M = n1; c.N = 1; c.K = n1;
@@ -434,9 +441,11 @@ void CcsdReal::residual(const double* T, double* R) {
     d.beta = 1.0;
     gemm_(d);
   }
-  {  // R1[a][i] -= sum_{ckl} Xp[a][c][k][l] Vh2[i][c][k][l]
-    Contraction c; c.M = v; c.N = o; c.K = v * o * o;
-    c.A = rm(Xp_, v * o * o); c.B = tr(Vh2_, v * o * o); c.C = rm(R1, o);
+  {  // R1[a][i] -= sum_{k,(c,l)} X[(a,k),(c,l)] Vh2[i][k][c][l]
+    Contraction c; c.M = v; c.N = o; c.K = o * n1; c.Ki = n1;
+    c.A = vw(Xd_, 0, sA, sI, 1);
+    c.B = vw(Vh2_, n1, 1, 0, o * n1);
+    c.C = rm(R1, o);
     c.alpha = -1.0; c.beta = 1.0;
     gemm_(c);
   }
@@ -446,7 +455,7 @@ void CcsdReal::residual(const double* T, double* R) {
 // Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of size s,
 //   V[x][y][c][d] = sum_G dGpp[G][x0+x][c] dGpp[G][y0+y][d]          (GEMM, K = G)
 //   R_{x y i j} += sum_cd V[x][y][c][d] X_cdij, mirrored into R_{y x j i} (GEMM, K = v^2)
-void CcsdReal::ppl(const double* Xp, double* R2, const double* dGpp) {
+void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
   const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o;
   const int64_t s = slab_rows_;
   const int64_t nb = (v + s - 1) / s;
@@ -462,9 +471,9 @@ void CcsdReal::ppl(const double* Xp, double* R2, const double* dGpp) {
         tc_(c);
       }
       {
-        Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
-        c.A = vw(slab_, sy * v * v, v * v, 0, 1);
-        c.B = vw(cp(Xp), 0, o * o, o, 1);
+        Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ki = v; c.Ni = o;
+        c.A = vw(slab_, sy * v * v, v * v, v, 1);
+        c.B = vw(cp(Xd), o * n1, o, n1, 1);    // X_cdij = X[(c,i),(d,j)]
         c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
         if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
         c.beta = 1.0;

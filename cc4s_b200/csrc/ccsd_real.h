@@ -30,20 +30,22 @@ class CcsdReal : public Schedule {
 
   void residual(const double* T, double* R) override;
   const double* Vd() const override { return Vd_; }
-  const double* Ve() const override { return Ve_; }
+  // The exchange integrals V_abji are read from Vd through index views (no copy).
+  const double* Ve() const override { return nullptr; }
 
  private:
   void build_integrals();
-  void ppl(const double* Xp, double* R2, const double* dGpp);
+  void ppl(const double* Xd, double* R2, const double* dGpp);
 
   RealSystem sys_;
   RealOptions opt_;
-  // static integrals
-  double *Vd_ = nullptr, *Ve_ = nullptr, *Vp_ = nullptr, *Vtp_ = nullptr;
+  // static integrals: Vd is the only (vo)^2 one; its exchange and pp pairings
+  // are strided views
+  double *Vd_ = nullptr;
   double *Vhhhh_ = nullptr, *Vhhhp_ = nullptr, *Vh2_ = nullptr;
-  // workspace
-  double *Xd_ = nullptr, *Xp_ = nullptr, *Te_ = nullptr, *Y_ = nullptr, *W8_ = nullptr,
-         *Tp_ = nullptr, *EX_ = nullptr;
+  // workspace: four (vo)^2 buffers.  EX also holds 2V - V^x (for Kki, Kac) at
+  // the start of a residual and the ring / singles combinations (W8) between uses.
+  double *Xd_ = nullptr, *Y_ = nullptr, *EX_ = nullptr, *W8_ = nullptr;
   double *Kki_ = nullptr, *Kac_ = nullptr, *Lac_ = nullptr, *Lki_ = nullptr, *jG_ = nullptr;
   double *U_ = nullptr, *dGph_ = nullptr, *W_ = nullptr, *Z_ = nullptr, *W1_ = nullptr,
          *F_ = nullptr, *dGpp_ = nullptr, *dGhh_ = nullptr, *Q_ = nullptr, *Xkl1_ = nullptr,

@@ -176,7 +176,10 @@ void Handle::allocate_state() {
   Tcur = take(n);
   Rbuf = take(n);
   const int N = opt.mixer == CC4S_MIXER_DIIS ? opt.max_residua : 1;
-  for (int k = 0; k < N; ++k) { A.push_back(take(n)); Rs.push_back(take(n)); }
+  // DIIS history in packed form (upper triangle of the symmetric T2 part): half
+  // the memory of full vectors, same overlaps and combinations.
+  const int64_t slot = opt.mixer == CC4S_MIXER_DIIS ? shape.packed_total() : n;
+  for (int k = 0; k < N; ++k) { A.push_back(take(slot)); Rs.push_back(take(slot)); }
   if (opt.mixer == CC4S_MIXER_LINEAR) dTlast = take(n);
   scal = take(64);
   ws = take(4096 * 8);

@@ -31,8 +31,10 @@ struct Handle {
   void allocate_state();
   void reset_mixer();
   void require_inputs() const;
-  void upload_amplitudes(double* dst, const double* T1, const double* T2);
-  void download_amplitudes(const double* src, double* T1, double* T2);
+  // Layout change between the caller's column-major T1/T2 and the device
+  // amplitude vector, through a full-size device staging vector st (not dst/src).
+  void upload_amplitudes(double* dst, const double* T1, const double* T2, double* st);
+  void download_amplitudes(const double* src, double* T1, double* T2, double* st);
   void mix(double* A_new, double* dT_new, double* norm2_dev);
 
   cc4s_cc_options opt;

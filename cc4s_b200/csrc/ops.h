@@ -59,6 +59,10 @@ struct AmpShape {
   int64_t n1() const { return v * o; }
   int64_t plane() const { return v * o + (v * o) * (v * o); }
   int64_t total() const { return plane() * planes; }
+  // Packed form (DIIS history): T2 is a symmetric (vo) x (vo) matrix
+  // (T_abij = T_baji), so each plane keeps [T1 | rows r of T2, columns r..n1-1].
+  int64_t packed_plane() const { return n1() + n1() * (n1() + 1) / 2; }
+  int64_t packed_total() const { return packed_plane() * planes; }
 };
 
 // Jacobi update of CoupledCluster::residuumToAmplitudes:
@@ -67,8 +71,16 @@ struct AmpShape {
 void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const double* eh,
             const double* ep, const AmpShape& sh, double shift, Stream s);
 
+// The same update written into packed slots (AmpShape::packed_*): R and Told are
+// full amplitude vectors with symmetric T2 parts; only their upper triangles are read.
+void jacobi_packed(double* Tnew_p, double* dT_p, const double* R, const double* Told,
+                   const double* eh, const double* ep, const AmpShape& sh, double shift,
+                   Stream s);
+
 // Correlation energy of amplitudes T (AmpShape layout) with the pair-layout integrals
 // Vd[(a,i),(b,j)] = V_abij and Ve[(a,i),(b,j)] = V_abji (real and optional imaginary planes).
+// Ve_re == nullptr (real path only): the exchange integrals are read from Vd itself,
+// V_abji = Vd[(a,j),(b,i)].
 // Writes 4 doubles to out_dev: Re(direct), Re(exchange), Im(direct), Im(exchange).
 void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
             const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s);
@@ -91,6 +103,16 @@ void diis_solve(double* B, const double* dots_dev, const int* valid_host, int N,
 void lincomb(double* out, const double* const* xs, const double* const* ys,
              const double* coef_dev, int nx, int64_t n, double* norm2_dev, double* ws,
              Stream s);
+
+// Packed counterparts of dots and lincomb: the vectors x, ys[k], xs[j] are packed
+// (AmpShape::packed_*) and stand for the full symmetric vectors they represent, so
+// off-diagonal T2 entries count twice in dot products and norms.  lincomb_packed
+// writes the full vector out (both triangles).
+void dots_packed(const double* x, const double* const* ys, int ny, const AmpShape& sh,
+                 double* out_dev, double* ws, Stream s);
+void lincomb_packed(double* out, const double* const* xs, const double* const* ys,
+                    const double* coef_dev, int nx, const AmpShape& sh, double* norm2_dev,
+                    double* ws, Stream s);
 
 // Small host-visible scalars.
 void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, Stream s);

@@ -336,6 +336,210 @@ __global__ void lincomb_kernel(LinArgs a) {
   }
 }
 
+// ---- packed amplitude vectors ----------------------------------------------
+// Per plane a packed vector holds T1 (n1 values) and then, for each row r of
+// the symmetric T2 pair matrix, its columns r..n1-1; row r starts at
+// n1 + tri_off(r, n1).
+__device__ __forceinline__ int64_t tri_off(int64_t r, int64_t n) {
+  return r * n - r * (r - 1) / 2;
+}
+
+struct PackedJacobiArgs {
+  double* Tnew; double* dT; const double* R; const double* Told;
+  const double* eh; const double* ep;
+  int64_t o, v, plane, pplane, items;  // items = planes * (n1 + 1): T1, then T2 rows
+  double shift;
+};
+
+// Same arithmetic as jacobi_kernel, element by element, on the upper triangle.
+__global__ void jacobi_packed_kernel(PackedJacobiArgs a) {
+  const int64_t n1 = a.v * a.o;
+  for (int64_t it = blockIdx.x; it < a.items; it += gridDim.x) {
+    const int64_t pl = it / (n1 + 1), w = it - pl * (n1 + 1);
+    const double* R = a.R + pl * a.plane;
+    const double* To = a.Told ? a.Told + pl * a.plane : nullptr;
+    double* Tn = a.Tnew + pl * a.pplane;
+    double* dT = a.dT + pl * a.pplane;
+    if (w == 0) {
+      for (int64_t ai = threadIdx.x; ai < n1; ai += blockDim.x) {
+        const double D = a.ep[ai / a.o] - a.eh[ai % a.o];
+        double rv = R[ai];
+        const double told = To ? To[ai] : 0.0;
+        if (To && a.shift != 0.0) rv -= a.shift * told;
+        const double tn = rv * (-1.0 / (D + a.shift));
+        Tn[ai] = tn;
+        dT[ai] = To ? tn - told : tn;
+      }
+      continue;
+    }
+    const int64_t r = w - 1;
+    const double Dr = a.ep[r / a.o] - a.eh[r % a.o];
+    const double* Rr = R + n1 + r * n1;
+    const double* Tr = To ? To + n1 + r * n1 : nullptr;
+    const int64_t po = n1 + tri_off(r, n1) - r;  // packed index of column c is po + c
+    for (int64_t c = r + threadIdx.x; c < n1; c += blockDim.x) {
+      const double D = Dr + a.ep[c / a.o] - a.eh[c % a.o];
+      double rv = Rr[c];
+      const double told = Tr ? Tr[c] : 0.0;
+      if (Tr && a.shift != 0.0) rv -= a.shift * told;
+      const double tn = rv * (-1.0 / (D + a.shift));
+      Tn[po + c] = tn;
+      dT[po + c] = Tr ? tn - told : tn;
+    }
+  }
+}
+
+struct PackedDotArgs {
+  const double* x;
+  const double* y[8];
+  int ny;
+  int64_t n1, pplane, items;  // items = planes * (n1 + 1)
+  double* ws;
+};
+
+// Weighted dots: off-diagonal T2 entries stand for two elements of the full vector.
+__global__ void dots_packed_kernel(PackedDotArgs a) {
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t it = blockIdx.x; it < a.items; it += gridDim.x) {
+    const int64_t pl = it / (a.n1 + 1), w = it - pl * (a.n1 + 1);
+    const int64_t b = pl * a.pplane + (w == 0 ? 0 : a.n1 + tri_off(w - 1, a.n1));
+    const int64_t len = w == 0 ? a.n1 : a.n1 - (w - 1);
+    for (int64_t k = threadIdx.x; k < len; k += blockDim.x) {
+      const double wt = (w == 0 || k == 0) ? 1.0 : 2.0;
+      const double xv = wt * a.x[b + k];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (q < a.ny) acc[q] += xv * a.y[q][b + k];
+    }
+  }
+  block_sum<8>(acc);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < a.ny; ++q) a.ws[blockIdx.x * a.ny + q] = acc[q];
+}
+
+struct PackedLinArgs {
+  double* out;
+  const double* x[16];
+  const double* y[16];
+  const double* coef;
+  int nx;
+  int64_t n1, plane, pplane, nT, items;  // nT = ceil(n1 / 32); items = planes * (1 + tiles)
+  double* ws;
+};
+
+// out (full) = sum_j coef[j] x_j on 32 x 32 tiles (I, J), I <= J, of the upper
+// triangle; each tile is written in place and, through shared memory, mirrored.
+__global__ void lincomb_packed_kernel(PackedLinArgs a) {
+  __shared__ double tile[32][33];
+  double c[16];
+  for (int k = 0; k < 16; ++k) c[k] = k < a.nx ? a.coef[k] : 0.0;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t n1 = a.n1, nT = a.nT;
+  const int64_t per = 1 + nT * (nT + 1) / 2;
+  double nrm[1] = {0.0};
+  for (int64_t it = blockIdx.x; it < a.items; it += gridDim.x) {
+    const int64_t pl = it / per, w = it - pl * per;
+    const int64_t pb = pl * a.pplane;
+    double* ob = a.out + pl * a.plane;
+    if (w == 0) {
+      for (int64_t e = threadIdx.x; e < n1; e += blockDim.x) {
+        double v = 0.0, u = 0.0;
+        for (int k = 0; k < a.nx; ++k) {
+          v += c[k] * a.x[k][pb + e];
+          if (a.y[0]) u += c[k] * a.y[k][pb + e];
+        }
+        ob[e] = v;
+        nrm[0] += u * u;
+      }
+      continue;
+    }
+    // tile t -> (I, J): row I of tiles holds nT - I tiles
+    const int64_t t = w - 1;
+    int64_t I = static_cast<int64_t>(
+        (2.0 * nT + 1.0 - sqrt((2.0 * nT + 1.0) * (2.0 * nT + 1.0) - 8.0 * t)) / 2.0);
+    if (I < 0) I = 0;
+    while (I > 0 && tri_off(I, nT) > t) --I;
+    while (I + 1 < nT && tri_off(I + 1, nT) <= t) ++I;
+    const int64_t J = I + (t - tri_off(I, nT));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t r = I * 32 + ty + 8 * q, cc = J * 32 + tx;
+      double v = 0.0;
+      if (r < n1 && cc < n1 && cc >= r) {
+        const int64_t pidx = pb + n1 + tri_off(r, n1) + (cc - r);
+        double u = 0.0;
+        for (int k = 0; k < a.nx; ++k) {
+          v += c[k] * a.x[k][pidx];
+          if (a.y[0]) u += c[k] * a.y[k][pidx];
+        }
+        ob[n1 + r * n1 + cc] = v;
+        nrm[0] += (cc == r ? 1.0 : 2.0) * u * u;
+      }
+      tile[ty + 8 * q][tx] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // element (rr, cc) of the lower triangle = (cc, rr)
+      const int64_t rr = J * 32 + ty + 8 * q, cc = I * 32 + tx;
+      if (rr < n1 && cc < n1 && rr > cc) ob[n1 + rr * n1 + cc] = tile[tx][ty + 8 * q];
+    }
+    __syncthreads();
+  }
+  if (a.ws) {
+    block_sum<1>(nrm);
+    if (threadIdx.x == 0) a.ws[blockIdx.x] = nrm[0];
+  }
+}
+
+struct EnergySwapArgs {
+  const double* T; const double* Vd;
+  int64_t o, v, oT, items;  // oT = ceil(o / 32); items = v * v * oT * oT
+  double* ws;
+};
+
+// Real-path energy with the exchange integrals read from Vd: for each pair (a, b)
+// the o x o blocks X_ab[i][j] and Vd_ab[j][i] = V_abji meet through a shared-memory
+// transpose; the direct term reads Vd_ab[i][j] in place.
+__global__ void energy_swap_kernel(EnergySwapArgs a) {
+  __shared__ double tile[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t o = a.o, v = a.v, n1 = v * o;
+  const double* t1 = a.T;
+  const double* t2 = a.T + n1;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t it = blockIdx.x; it < a.items; it += gridDim.x) {
+    int64_t rest = it;
+    const int64_t jt = rest % a.oT; rest /= a.oT;
+    const int64_t itile = rest % a.oT; rest /= a.oT;
+    const int64_t b = rest % v, aa = rest / v;
+    const int64_t i0 = itile * 32, j0 = jt * 32;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {  // tile[jj][ii] = Vd[(aa, j0+jj), (b, i0+ii)]
+      const int64_t j = j0 + ty + 8 * q, i = i0 + tx;
+      tile[ty + 8 * q][tx] = (j < o && i < o) ? a.Vd[(aa * o + j) * n1 + b * o + i] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t i = i0 + ty + 8 * q, j = j0 + tx;
+      if (i < o && j < o) {
+        const int64_t e = (aa * o + i) * n1 + b * o + j;
+        const double x = t2[e] + t1[aa * o + i] * t1[b * o + j];
+        acc[0] += x * a.Vd[e];
+        acc[1] += x * tile[tx][ty + 8 * q];
+      }
+    }
+    __syncthreads();
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0) {
+    a.ws[blockIdx.x * 4 + 0] = acc[0];
+    a.ws[blockIdx.x * 4 + 1] = acc[1];
+    a.ws[blockIdx.x * 4 + 2] = 0.0;
+    a.ws[blockIdx.x * 4 + 3] = 0.0;
+  }
+}
+
 struct DiisArgs {
   double* B;
   const double* dots;
@@ -540,10 +744,68 @@ void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, S
   count();
 }
 
+void jacobi_packed(double* Tnew_p, double* dT_p, const double* R, const double* Told,
+                   const double* eh, const double* ep, const AmpShape& sh, double shift,
+                   Stream s) {
+  PackedJacobiArgs a{Tnew_p, dT_p, R, Told, eh, ep, sh.o, sh.v, sh.plane(), sh.packed_plane(),
+                     sh.planes * (sh.n1() + 1), shift};
+  jacobi_packed_kernel<<<grid_for(a.items, 1, 148 * 16), 256, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void dots_packed(const double* x, const double* const* ys, int ny, const AmpShape& sh,
+                 double* out_dev, double* ws, Stream s) {
+  if (ny <= 0) return;
+  if (ny > 8) throw Error(ERR_UNSUPPORTED, "dots: at most 8 vectors");
+  PackedDotArgs a{};
+  a.x = x; a.ny = ny; a.n1 = sh.n1(); a.pplane = sh.packed_plane();
+  a.items = sh.planes * (sh.n1() + 1); a.ws = ws;
+  for (int k = 0; k < ny; ++k) a.y[k] = ys[k];
+  dots_packed_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, ny, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+  count();
+}
+
+void lincomb_packed(double* out, const double* const* xs, const double* const* ys,
+                    const double* coef_dev, int nx, const AmpShape& sh, double* norm2_dev,
+                    double* ws, Stream s) {
+  if (nx > 16) throw Error(ERR_UNSUPPORTED, "lincomb: at most 16 vectors");
+  PackedLinArgs a{};
+  a.out = out; a.coef = coef_dev; a.nx = nx;
+  a.n1 = sh.n1(); a.plane = sh.plane(); a.pplane = sh.packed_plane();
+  a.nT = (sh.n1() + 31) / 32;
+  a.items = sh.planes * (1 + a.nT * (a.nT + 1) / 2);
+  a.ws = (ys && norm2_dev) ? ws : nullptr;
+  for (int k = 0; k < nx; ++k) {
+    a.x[k] = xs[k];
+    a.y[k] = ys ? ys[k] : nullptr;
+  }
+  lincomb_packed_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+  if (a.ws) {
+    finish_kernel<<<1, 256, 0, s>>>(norm2_dev, ws, RED_BLOCKS, 1, 1.0, 1.0, 1.0, 1.0);
+    CC_LAUNCH_CHECK();
+    count();
+  }
+}
+
 void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
             const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s) {
-  EnergyArgs a{T, Vd_re, Vd_im, Ve_re, Ve_im, sh.o, sh.v, sh.plane(), (int)sh.planes, ws};
-  energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  if (!Ve_re) {
+    if (sh.planes != 1 || Vd_im || Ve_im)
+      throw Error(ERR_UNSUPPORTED, "energy: exchange from Vd on the real path only");
+    EnergySwapArgs a{T, Vd_re, sh.o, sh.v, (sh.o + 31) / 32, 0, ws};
+    a.items = sh.v * sh.v * a.oT * a.oT;
+    energy_swap_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  } else {
+    EnergyArgs a{T, Vd_re, Vd_im, Ve_re, Ve_im, sh.o, sh.v, sh.plane(), (int)sh.planes, ws};
+    energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  }
   CC_LAUNCH_CHECK();
   // direct = 2 * sum X V_ijab, exchange = -sum X V_ijba  (CoupledCluster.cxx:223-232)
   finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 4, 2.0, -1.0, 2.0, -1.0);

@@ -20,7 +20,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
+#include <vector>
 
 namespace cc4s_b200 {
 
@@ -434,12 +436,65 @@ void pack(const View& v, bool rows_are_m, const Contraction& g, int64_t R, int64
   CC_LAUNCH_CHECK();
 }
 
+// Packed slices of both operands are limited to this many bytes: a longer K is
+// cut into panels (multiples of KCHUNK where possible), each packed and
+// multiplied in turn and accumulated into C in FP64.
+constexpr size_t kPanelBytes = size_t(9) << 28;  // 2.25 GiB
+
+// CC4S_SPLIT_PANEL_BYTES (at least 1 MiB) overrides the limit, e.g. to trade
+// scratch memory for fewer, longer panels.
+size_t panel_bytes() {
+  if (const char* e = std::getenv("CC4S_SPLIT_PANEL_BYTES")) {
+    const long long v = std::atoll(e);
+    if (v >= (1ll << 20)) return static_cast<size_t>(v);
+  }
+  return kPanelBytes;
+}
+
+int64_t panel_len(const Contraction& g) {
+  const int64_t per_k = 2 * NSLICE * (rup(g.M, TM) + rup(g.N, TN));  // bytes per k
+  int64_t P = static_cast<int64_t>(panel_bytes()) / per_k;
+  if (P >= KCHUNK) P = P / KCHUNK * KCHUNK;
+  else P = std::max<int64_t>(TK, P / TK * TK);
+  return P;
+}
+
+struct Panel { int64_t k0, kl, ki, a_off, b_off; };
+
+// K panels of length <= P.  A two-level K index (inner extent Ki) is cut either
+// into groups of whole inner runs (Ki <= P) or inside each run (Ki > P); the
+// operand views are shifted to the panel start.
+std::vector<Panel> panels_of(const Contraction& g, int64_t P) {
+  std::vector<Panel> out;
+  const int64_t K = g.K, Ki = g.Ki > 0 ? g.Ki : K;
+  if (K <= P) {
+    out.push_back({0, K, g.Ki, 0, 0});
+  } else if (Ki >= K) {
+    for (int64_t k0 = 0; k0 < K; k0 += P)
+      out.push_back({k0, std::min(P, K - k0), 0, k0 * g.A.s_ci, k0 * g.B.s_ri});
+  } else if (Ki <= P) {
+    const int64_t runs = P / Ki;
+    for (int64_t q0 = 0; q0 * Ki < K; q0 += runs)
+      out.push_back({q0 * Ki, std::min(runs * Ki, K - q0 * Ki), Ki, q0 * g.A.s_co, q0 * g.B.s_ro});
+  } else {
+    for (int64_t q = 0; q * Ki < K; ++q)
+      for (int64_t r0 = 0; r0 < Ki && q * Ki + r0 < K; r0 += P)
+        out.push_back({q * Ki + r0, std::min(std::min(P, Ki - r0), K - q * Ki - r0), 0,
+                       q * g.A.s_co + r0 * g.A.s_ci, q * g.B.s_ro + r0 * g.B.s_ri});
+  }
+  return out;
+}
+
+void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws);
+
 }  // namespace
 
 uint64_t split_launch_count() { return g_split_launches.load(); }
 
 size_t gemm_split_scratch_bytes(const Contraction& g) {
-  const Layout2 L = layout_of(g);
+  Contraction h = g;
+  h.K = std::min(g.K, panel_len(g));
+  const Layout2 L = layout_of(h);
   return L.a_bytes + L.b_bytes + L.meta_bytes;
 }
 
@@ -447,6 +502,21 @@ void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
   if (g.M <= 0 || g.N <= 0) return;
   if (g.batch != 1) throw Error(ERR_UNSUPPORTED, "gemm_split: batched contraction");
   if (g.K <= 0) throw Error(ERR_UNSUPPORTED, "gemm_split: empty K");
+  const std::vector<Panel> ps = panels_of(g, panel_len(g));
+  for (size_t i = 0; i < ps.size(); ++i) {
+    Contraction h = g;
+    h.K = ps[i].kl;
+    h.Ki = ps[i].ki;
+    h.A.p = g.A.p + ps[i].a_off;
+    h.B.p = g.B.p + ps[i].b_off;
+    if (i > 0) h.beta = 1.0;
+    split_panel(h, s, ws);
+  }
+}
+
+namespace {
+
+void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
   const Layout2 L = layout_of(g);
   if (L.a_bytes + L.b_bytes + L.meta_bytes > ws.bytes) throw Error(ERR_OUT_OF_MEMORY, "gemm_split: scratch too small");
   if (L.Mp * NSLICE >= (int64_t(1) << 31) || L.Np * NSLICE >= (int64_t(1) << 31) || L.Kp >= (int64_t(1) << 31))
@@ -486,4 +556,5 @@ void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
   g_split_launches.fetch_add(1);
 }
 
+}  // namespace
 }  // namespace cc4s_b200

@@ -287,7 +287,12 @@ void energy(const double* T, const double* Vdr, const double* Vdi, const double*
       if (!t1i) {
         const double x = t2r[e] + t1r[r] * t1r[c];
         acc[0] += x * Vdr[e];
-        acc[1] += x * Ver[e];
+        if (Ver) {
+          acc[1] += x * Ver[e];
+        } else {  // V_abji = Vd[(a,j),(b,i)]
+          const int64_t a = r / sh.o, i = r % sh.o, b = c / sh.o, j = c % sh.o;
+          acc[1] += x * Vdr[(a * sh.o + j) * n1 + b * sh.o + i];
+        }
       } else {
         const double xr = t2r[e] + t1r[r] * t1r[c] - t1i[r] * t1i[c];
         const double xi = t2i[e] + t1r[r] * t1i[c] + t1i[r] * t1r[c];
@@ -372,6 +377,90 @@ void lincomb(double* out, const double* const* xs, const double* const* ys, cons
 }
 
 void sum_partials_to(double*, const double*, int, int, Stream) {}
+
+// Packed amplitude vectors: per plane [T1 | T2 rows r, columns r..n1-1].
+static int64_t packed_index(const AmpShape& sh, int64_t pl, int64_t r, int64_t c) {
+  const int64_t n1 = sh.n1();
+  return pl * sh.packed_plane() + n1 + r * n1 - r * (r - 1) / 2 + (c - r);
+}
+
+void jacobi_packed(double* Tnew, double* dT, const double* R, const double* Told,
+                   const double* eh, const double* ep, const AmpShape& sh, double shift,
+                   Stream) {
+  ++g_ops;
+  const int64_t n1 = sh.n1();
+  auto upd = [&](int64_t full, int64_t pk, double D) {
+    double rv = R[full];
+    const double told = Told ? Told[full] : 0.0;
+    if (Told && shift != 0.0) rv -= shift * told;
+    const double tn = rv * (-1.0 / (D + shift));
+    Tnew[pk] = tn;
+    dT[pk] = Told ? tn - told : tn;
+  };
+  for (int64_t pl = 0; pl < sh.planes; ++pl) {
+    for (int64_t ai = 0; ai < n1; ++ai)
+      upd(pl * sh.plane() + ai, pl * sh.packed_plane() + ai, ep[ai / sh.o] - eh[ai % sh.o]);
+    for (int64_t r = 0; r < n1; ++r)
+      for (int64_t c = r; c < n1; ++c)
+        upd(pl * sh.plane() + n1 + r * n1 + c, packed_index(sh, pl, r, c),
+            ep[r / sh.o] - eh[r % sh.o] + ep[c / sh.o] - eh[c % sh.o]);
+  }
+}
+
+void dots_packed(const double* x, const double* const* ys, int ny, const AmpShape& sh,
+                 double* out, double*, Stream) {
+  ++g_ops;
+  const int64_t n1 = sh.n1();
+  for (int k = 0; k < ny; ++k) {
+    double s = 0.0;
+    for (int64_t pl = 0; pl < sh.planes; ++pl) {
+      for (int64_t ai = 0; ai < n1; ++ai) {
+        const int64_t e = pl * sh.packed_plane() + ai;
+        s += x[e] * ys[k][e];
+      }
+      for (int64_t r = 0; r < n1; ++r)
+        for (int64_t c = r; c < n1; ++c) {
+          const int64_t e = packed_index(sh, pl, r, c);
+          s += (c == r ? 1.0 : 2.0) * x[e] * ys[k][e];
+        }
+    }
+    out[k] = s;
+  }
+}
+
+void lincomb_packed(double* out, const double* const* xs, const double* const* ys,
+                    const double* coef, int nx, const AmpShape& sh, double* norm2, double*,
+                    Stream) {
+  ++g_ops;
+  const int64_t n1 = sh.n1();
+  double s2 = 0.0;
+  auto comb = [&](int64_t pk, double& w) {
+    double v = 0.0;
+    w = 0.0;
+    for (int k = 0; k < nx; ++k) {
+      v += coef[k] * xs[k][pk];
+      if (ys) w += coef[k] * ys[k][pk];
+    }
+    return v;
+  };
+  for (int64_t pl = 0; pl < sh.planes; ++pl) {
+    double* ob = out + pl * sh.plane();
+    for (int64_t ai = 0; ai < n1; ++ai) {
+      double w;
+      ob[ai] = comb(pl * sh.packed_plane() + ai, w);
+      s2 += w * w;
+    }
+    for (int64_t r = 0; r < n1; ++r)
+      for (int64_t c = r; c < n1; ++c) {
+        double w;
+        const double v = comb(packed_index(sh, pl, r, c), w);
+        ob[n1 + r * n1 + c] = v;
+        ob[n1 + c * n1 + r] = v;
+        s2 += (c == r ? 1.0 : 2.0) * w * w;
+      }
+  }
+  if (ys && norm2) norm2[0] = s2;
+}
 
 }  // namespace ops
 }  // namespace cc4s_b200

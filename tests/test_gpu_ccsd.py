@@ -156,6 +156,28 @@ def test_split_precision_residual(Solver):
     assert _rel(R2, Q2) > 1e-14  # the tensor-core path really ran
 
 
+def test_split_precision_k_panels(Solver, monkeypatch):
+    """With the packed-slice scratch limited to 1 MiB every split contraction is
+    cut into K panels (one-level, whole inner runs and inside inner runs) that
+    accumulate into C; the residual still agrees with the oracle to 1e-5 and
+    with the single-panel split result to 1e-6."""
+    s = inputs.synthetic_system(16, 128, 256, seed=2)
+    rng = np.random.default_rng(3)
+    T = _rand_T(rng, 128, 16)
+    one = Solver({"precision": "split3"})
+    one.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    P1, P2 = one.residual(T)
+    one.close()
+    monkeypatch.setenv("CC4S_SPLIT_PANEL_BYTES", str(1 << 20))
+    sol = Solver({"precision": "split3"})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    R1, R2 = sol.residual(T)
+    sol.close()
+    Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s))
+    assert _rel(R2, Q2) < 1e-5 and _rel(R1, Q1) < 1e-5
+    assert _rel(R2, P2) < 1e-6 and _rel(R1, P1) < 1e-6
+
+
 @pytest.mark.parametrize("shape", [(8, 40, 200), (10, 64, 150)])
 def test_split_precision_energy_within_1ueh(Solver, shape):
     """Converged CCSD energy of the split-precision form within 1 uEh of FP64."""
