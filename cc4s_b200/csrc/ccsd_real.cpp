@@ -21,14 +21,16 @@
 //   * crossed ring (Ccsd.cxx:233-253): the second term, sum Xbkci T_ackj, is
 //     written straight into the exchange pairing of R2;
 //   * the particle-particle ladder (Ccsd.cxx:283-333) is evaluated on square
-//     slabs of the virtual index pair (a >= b blocks, mirrored into (b,a,j,i)),
-//     V_abcd built per slab from the dressed vertex and never stored whole;
+//     blocks of the virtual index pair (a >= b blocks, mirrored into (b,a,j,i))
+//     and panels of c, V_abcd built per slab from the dressed vertex and never
+//     stored whole;
 //   * singles (Ccsd.cxx:339-375): the Gamma.Gamma.X pair shares one
 //     Gamma (2X - X^x) intermediate.
 #include "ccsd_real.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace cc4s_b200 {
 
@@ -53,16 +55,22 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
     dGpp_ = take(G * v * v); dGhh_ = take(G * o * o);
     Q_ = take(n1 * o * o); Xkl1_ = take(o * o * o * o); Xkl2_ = take(o * o * o * o);
     kck_ = take(n1); P1_ = take(o * o); P_ = take(G * o * v);
-    // PPL slab: s x s virtual pairs times v^2, bounded to 2^28 doubles.
-    int64_t sl = opt.slab;
-    if (sl <= 0) {
-      const double budget = double(int64_t(1) << 28);
-      sl = static_cast<int64_t>(std::floor(std::sqrt(budget / double(v * v))));
-      if (sl >= 16) sl = (sl / 8) * 8;
-      sl = std::max<int64_t>(1, std::min(sl, v));
+    // Ladder slabs: blocks of s virtual orbitals (s^2 rows of the contraction,
+    // 64 by default) times a panel of c_n values of c, sized so that one slab
+    // V[x][y][c][d] (s^2 c_n v doubles) stays within the budget (2^28 doubles;
+    // CC4S_PPL_SLAB_DOUBLES overrides it).
+    int64_t sl = opt.slab > 0 ? opt.slab : 64;
+    slab_rows_ = std::max<int64_t>(1, std::min(sl, v));
+    int64_t budget = int64_t(1) << 28;
+    if (const char* e = std::getenv("CC4S_PPL_SLAB_DOUBLES")) {
+      const long long b = std::atoll(e);
+      if (b > 0) budget = b;
     }
-    slab_rows_ = std::min(sl, v);
-    if (opt.ppl) slab_ = take(slab_rows_ * slab_rows_ * v * v);
+    const int64_t cmax = std::max<int64_t>(
+        1, std::min<int64_t>(v, budget / (slab_rows_ * slab_rows_ * v)));
+    const int64_t npanels = (v + cmax - 1) / cmax;
+    slab_cols_ = (v + npanels - 1) / npanels;
+    if (opt.ppl) slab_ = take(slab_rows_ * slab_rows_ * slab_cols_ * v);
   } catch (...) {
     release_all();
     throw;
@@ -452,32 +460,39 @@ void CcsdReal::residual(const double* T, double* R) {
   profile_finish();
 }
 
-// Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of size s,
-//   V[x][y][c][d] = sum_G dGpp[G][x0+x][c] dGpp[G][y0+y][d]          (GEMM, K = G)
-//   R_{x y i j} += sum_cd V[x][y][c][d] X_cdij, mirrored into R_{y x j i} (GEMM, K = v^2)
+// Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of s virtual
+// orbitals and panels of c_n values of c,
+//   V[x][y][c'][d] = sum_G dGpp[G][x0+x][c0+c'] dGpp[G][y0+y][d]      (GEMM, K = G)
+//   R_{x y i j} += sum_{c',d} V[x][y][c'][d] X_{c0+c',d,i,j}          (GEMM, K = c_n v)
+// with the off-diagonal blocks mirrored into R_{y x j i}.  Panelling c keeps the
+// slab small enough for wide blocks (s^2 = 4096 rows), and each panel reads only
+// its c-range of X.
 void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
   const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o;
-  const int64_t s = slab_rows_;
+  const int64_t s = slab_rows_, cn = slab_cols_;
   const int64_t nb = (v + s - 1) / s;
-  for (int64_t X = 0; X < nb; ++X) {
-    for (int64_t Yb = 0; Yb <= X; ++Yb) {
-      const int64_t x0 = X * s, sx = std::min(s, v - x0);
-      const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
-      {
-        Contraction c; c.M = sx * v; c.N = sy * v; c.K = G; c.Mi = v; c.Ni = v;
-        c.A = vw(cp(dGpp) + x0 * v, v, 1, 0, v * v);
-        c.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
-        c.C = vw(slab_, sy * v * v, v, v * v, 1);
-        tc_(c);
-      }
-      {
-        Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ki = v; c.Ni = o;
-        c.A = vw(slab_, sy * v * v, v * v, v, 1);
-        c.B = vw(cp(Xd), o * n1, o, n1, 1);    // X_cdij = X[(c,i),(d,j)]
-        c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
-        if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
-        c.beta = 1.0;
-        tc_(c);
+  for (int64_t c0 = 0; c0 < v; c0 += cn) {
+    const int64_t nc = std::min(cn, v - c0);
+    for (int64_t X = 0; X < nb; ++X) {
+      for (int64_t Yb = 0; Yb <= X; ++Yb) {
+        const int64_t x0 = X * s, sx = std::min(s, v - x0);
+        const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
+        {  // m = (x, c'), n = (y, d), slab[x][y][c'][d]
+          Contraction c; c.M = sx * nc; c.N = sy * v; c.K = G; c.Mi = nc; c.Ni = v;
+          c.A = vw(cp(dGpp) + x0 * v + c0, v, 1, 0, v * v);
+          c.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
+          c.C = vw(slab_, sy * nc * v, v, nc * v, 1);
+          tc_(c);
+        }
+        {  // m = (x, y), k = (c', d), n = (i, j)
+          Contraction c; c.M = sx * sy; c.N = o * o; c.K = nc * v; c.Mi = sy; c.Ki = v; c.Ni = o;
+          c.A = vw(slab_, sy * nc * v, nc * v, v, 1);
+          c.B = vw(cp(Xd) + c0 * o * n1, o * n1, o, n1, 1);   // X_cdij = X[(c,i),(d,j)]
+          c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
+          if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
+          c.beta = 1.0;
+          tc_(c);
+        }
       }
     }
   }

@@ -8,7 +8,7 @@ namespace cc4s_b200 {
 struct RealOptions {
   bool ccd = false;         // T1 == 0, R1 dropped
   bool ppl = true;          // particle-particle ladder from vertex slabs
-  int64_t slab = 0;         // PPL slab size in virtual orbitals (0: automatic)
+  int64_t slab = 0;         // PPL block size in virtual orbitals (0: automatic)
 };
 
 // Device-resident inputs of the real path.  G counts stacked real rows: the
@@ -50,7 +50,7 @@ class CcsdReal : public Schedule {
   double *U_ = nullptr, *dGph_ = nullptr, *W_ = nullptr, *Z_ = nullptr, *W1_ = nullptr,
          *F_ = nullptr, *dGpp_ = nullptr, *dGhh_ = nullptr, *Q_ = nullptr, *Xkl1_ = nullptr,
          *Xkl2_ = nullptr, *kck_ = nullptr, *P1_ = nullptr, *P_ = nullptr, *slab_ = nullptr;
-  int64_t slab_rows_ = 0;
+  int64_t slab_rows_ = 0, slab_cols_ = 0;  // ladder block size, c-panel size
 };
 
 }  // namespace cc4s_b200

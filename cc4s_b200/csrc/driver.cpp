@@ -154,9 +154,11 @@ void Handle::allocate_state() {
   RealOptions ro;
   ro.ccd = opt.method == CC4S_METHOD_CCD;
   ro.ppl = opt.ppl != 0;
-  // Real path: the ladder is symmetric under (a,c) <-> (b,d), so its slab size is a
-  // free memory/performance choice.  Complex path: slices follow integralsSliceSize.
-  if (complex_path) ro.slab = opt.integrals_slice_size;
+  // integralsSliceSize sets the ladder block size.  Real path: the ladder is
+  // symmetric under (a,c) <-> (b,d), so the block size only trades memory for
+  // speed (0: automatic).  Complex path: blocks follow the reference's slices
+  // exactly (default No).
+  ro.slab = opt.integrals_slice_size;
   if (opt.method == CC4S_METHOD_DRCCD) {
     DrccdOptions dro;
     dro.linearized = opt.linearized != 0;

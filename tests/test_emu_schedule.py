@@ -52,6 +52,22 @@ def test_residual_matches_oracle(emu_lib, shape, method):
             assert np.abs(R1).max() == 0.0
 
 
+@pytest.mark.parametrize("slice_size,budget", [(4, 528), (5, 300), (11, 0)])
+def test_ladder_blocks_and_c_panels(emu_lib, monkeypatch, slice_size, budget):
+    """Real-path ladder on several virtual blocks (integralsSliceSize) and several
+    panels of c (slab budget CC4S_PPL_SLAB_DOUBLES), ragged edges included."""
+    from cc4s_b200 import Solver
+    if budget:
+        monkeypatch.setenv("CC4S_PPL_SLAB_DOUBLES", str(budget))
+    s = inputs.synthetic_system(4, 11, 12, seed=5)
+    T = _rand_T(np.random.default_rng(8), 11, 4)
+    sol = Solver({"integralsSliceSize": slice_size}, lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+    R1, R2 = sol.residual(T)
+    Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s))
+    assert _rel(R2, Q2) < 1e-13 and _rel(R1, Q1) < 1e-13
+
+
 @pytest.mark.parametrize("mixer", [dict(type="DiisMixer", maxResidua=5),
                                    dict(type="DiisMixer", maxResidua=2),
                                    dict(type="LinearMixer", ratio=0.7)])

@@ -156,6 +156,20 @@ def test_split_precision_residual(Solver):
     assert _rel(R2, Q2) > 1e-14  # the tensor-core path really ran
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", TOL_RES), ("split3", 1e-5)])
+def test_ladder_blocks_and_c_panels(Solver, monkeypatch, precision, tol):
+    """Ladder on ragged virtual blocks (48, 48, 32) and four panels of c."""
+    monkeypatch.setenv("CC4S_PPL_SLAB_DOUBLES", str(48 * 48 * 128 * 40))
+    s = inputs.synthetic_system(16, 128, 256, seed=2)
+    T = _rand_T(np.random.default_rng(3), 128, 16)
+    sol = Solver({"precision": precision, "integralsSliceSize": 48})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    R1, R2 = sol.residual(T)
+    sol.close()
+    Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s))
+    assert _rel(R2, Q2) < tol and _rel(R1, Q1) < tol
+
+
 def test_split_precision_k_panels(Solver, monkeypatch):
     """With the packed-slice scratch limited to 1 MiB every split contraction is
     cut into K panels (one-level, whole inner runs and inside inner runs) that
