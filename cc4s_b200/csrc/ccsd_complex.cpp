@@ -232,7 +232,7 @@ void CcsdComplex::residual(const double* T, double* R) {
     {  // R2 += cTdGph^T W
       Contraction c; c.M = n1; c.N = n1; c.K = G;
       c.A = tr(cTdGph_, n1); c.B = rm(W_, n1); c.C = rm(R2, n1); c.beta = 1.0;
-      zgemm(c, gph, gph, pl);
+      zgemm(c, gph, gph, pl, false, false, true);
     }
     {  // dGhh[G][k][i] += sum_d Ghp[G][k][d] t[d][i]
       Contraction c; c.M = o; c.N = o; c.K = v; c.batch = G;
@@ -249,7 +249,7 @@ void CcsdComplex::residual(const double* T, double* R) {
       Contraction c; c.M = n1; c.N = n1; c.K = G; c.Mi = o;
       c.A = vw(Ghp, 1, v, 0, n1); c.B = rm(SQ_, n1); c.C = vw(R2, o * n1, n1, 0, 1);
       c.alpha = -1.0; c.beta = 1.0;
-      zgemm(c, gph, gph, pl, true, false);
+      zgemm(c, gph, gph, pl, true, false, true);
     }
   }
   // ---- ring Xakic (Ccsd.cxx:494-502) -----------------------------------------------
@@ -266,27 +266,27 @@ void CcsdComplex::residual(const double* T, double* R) {
   {  // cTdGph -= 1/2 sum_{dl} conj(Gph[G][d][l]) Y_dail
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(cTdGph_, n1); c.alpha = -0.5; c.beta = 1.0;
-    zgemm(c, gph, D2, gph, true, false);
+    zgemm(c, gph, D2, gph, true, false, true);
   }
   ops::axpby(Y_, 2.0, Td, -1.0, Te_, 0.0, D2, s_);            // Y = 2T - T^x
   ops::axpby(Y_ + D2, 2.0, Td + pl, -1.0, Te_ + D2, 0.0, D2, s_);
   {  // W1[G][(b,j)] = sum_{c,k} Ghp[G][k][c] Y[(c,k),(b,j)]
     Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
     c.A = vw(Ghp, 0, n1, 1, v); c.B = vw(Y_, o * n1, n1, 0, 1); c.C = rm(W1_, n1);
-    zgemm(c, gph, D2, gph);
+    zgemm(c, gph, D2, gph, false, false, true);
   }
   {  // R2 += cTdGph^T W1
     Contraction c; c.M = n1; c.N = n1; c.K = G;
     c.A = tr(cTdGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
-    zgemm(c, gph, gph, pl);
+    zgemm(c, gph, gph, pl, false, false, true);
   }
   {  // EX = T M2^T ;  R2 += EX Y
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(Td, n1); c.B = tr(M2_, n1); c.C = rm(EX_, n1);
-    zgemm(c, pl, D2, D2);
+    zgemm(c, pl, D2, D2, false, false, true);
     Contraction d; d.M = n1; d.N = n1; d.K = n1;
     d.A = rm(EX_, n1); d.B = rm(Y_, n1); d.C = rm(R2, n1); d.beta = 1.0;
-    zgemm(d, D2, D2, pl);
+    zgemm(d, D2, D2, pl, false, false, true);
   }
   // ---- crossed ring Xakci (Ccsd.cxx:509-517) ----------------------------------------
   {
@@ -303,24 +303,24 @@ void CcsdComplex::residual(const double* T, double* R) {
   {  // EX = -1/2 T^x M3^T
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(Te_, n1); c.B = tr(M3_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
-    zgemm(c, D2, D2, D2);
+    zgemm(c, D2, D2, D2, false, false, true);
   }
   {  // EX[a][i][c][k] += sum_G cTdGpp[G][a][c] dGhh[G][k][i]
     Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
     c.A = vw(cTdGpp_, v, 1, 0, v * v); c.B = vw(dGhh_, 0, o * o, o, 1);
     c.C = vw(EX_, o * n1, o, 1, n1); c.beta = 1.0;
-    zgemm(c, gpp, ghh, D2);
+    zgemm(c, gpp, ghh, D2, false, false, true);
   }
   {  // R2 -= EX T
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
     c.A = rm(EX_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1); c.alpha = -1.0; c.beta = 1.0;
-    zgemm(c, D2, pl, pl);
+    zgemm(c, D2, pl, pl, false, false, true);
   }
   {  // R2_abij -= sum_ck T_ackj X_bkci   (exchange pairing)
     Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
     c.A = vw(Te_, o * n1, n1, 0, 1); c.B = vw(EX_, 0, 1, o * n1, n1);
     c.C = vw(R2, o * n1, 1, o, n1); c.alpha = -1.0; c.beta = 1.0;
-    zgemm(c, D2, D2, pl);
+    zgemm(c, D2, D2, pl, false, false, true);
   }
   // ---- symmetrisation, +V (Ccsd.cxx:520,529) -----------------------------------
   ops::symmetrize(R2, n1, s_);
@@ -346,16 +346,16 @@ void CcsdComplex::residual(const double* T, double* R) {
   {  // Xkl2[kl][ij] = sum_cd V_klcd X_cdij
     Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
     c.A = rm(Vh4_, v * v); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
-    zgemm(c, D2, D2, o4);
+    zgemm(c, D2, D2, o4, false, false, true);
   }
   {
     Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
     c.A = vw(Xp_, v * o * o, o * o, 0, 1); c.B = vw(Xkl1_, 0, o * o, o, 1);
     c.C = vw(R2, o * n1, o, n1, 1); c.beta = 1.0;
-    zgemm(c, D2, o4, pl);
+    zgemm(c, D2, o4, pl, false, false, true);
     c.A.p = opt_.ppl ? Tp_ : Xp_;
     c.B.p = Xkl2_;
-    zgemm(c, D2, o4, pl);
+    zgemm(c, D2, o4, pl, false, false, true);
   }
   // ---- particle-particle ladder (Ccsd.cxx:549-601) ---------------------------------
   if (opt_.ppl) {
@@ -376,7 +376,7 @@ void CcsdComplex::residual(const double* T, double* R) {
           c.A = vw(cTdGpp_ + x0 * v, v, 1, 0, v * v);
           c.B = vw(dGpp_ + y0 * v, 0, v * v, v, 1);
           c.C = vw(slab_, sy * v * v, v, v * v, 1);
-          zgemm(c, gpp, gpp, sz);
+          zgemm(c, gpp, gpp, sz, false, false, true);
         }
         {
           Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
@@ -385,7 +385,7 @@ void CcsdComplex::residual(const double* T, double* R) {
           c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
           if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
           c.beta = 1.0;
-          zgemm(c, sz, D2, pl);
+          zgemm(c, sz, D2, pl, false, false, true);
         }
       }
   }
@@ -443,7 +443,7 @@ void CcsdComplex::residual(const double* T, double* R) {
     ops::axpby(W8_ + D2, 2.0, Xd_ + D2, -1.0, W8_ + D2, 0.0, D2, s_);
     Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
     c.A = vw(Ghp, 0, n1, 1, v); c.B = vw(W8_, o * n1, n1, 0, 1); c.C = rm(F_, n1);
-    zgemm(c, gph, D2, gph);
+    zgemm(c, gph, D2, gph, false, false, true);
     Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
     d.A = vw(Gpp, 0, 1, v * v, v); d.B = vw(F_, n1, o, 0, 1); d.C = rm(R1, o); d.beta = 1.0;
     zgemm(d, gpp, gph, pl, true, false);

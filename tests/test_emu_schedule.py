@@ -104,6 +104,23 @@ def test_split_precision_form_accuracy(emu_lib):
     assert ra["correlation"] != rb["correlation"]  # the split path really ran
 
 
+def test_split_precision_complex_path(emu_lib):
+    """Complex path: the large contractions run as split products (exact model of
+    the tensor-core scheme); the converged energy stays far inside 1 uEh."""
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(6, 30, 60, complex=True, seed=1)
+    o = dict(maxIterations=40, energyConvergence=1e-10, amplitudesConvergence=1e-7)
+    a = Solver(o, lib=emu_lib)
+    a.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    ra = a.run()
+    b = Solver(dict(o, precision="split3"), lib=emu_lib)
+    b.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    rb = b.run()
+    assert ra["converged"] and rb["converged"]
+    assert abs(ra["correlation"] - rb["correlation"]) < 1e-8
+    assert ra["correlation"] != rb["correlation"]  # the split path really ran
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 def test_backward_structure_factor_and_gradient(emu_lib, cplx):
     """Adjoint entry: S(G) equals the restated FiniteSizeCorrection structure

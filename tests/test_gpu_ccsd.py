@@ -192,6 +192,32 @@ def test_split_precision_k_panels(Solver, monkeypatch):
     assert _rel(R2, P2) < 1e-6 and _rel(R1, P1) < 1e-6
 
 
+def test_split_precision_complex(Solver):
+    """Complex path in the split form: residual within 1e-5 of the oracle, and the
+    converged energy within 1 uEh of the FP64 form."""
+    s = inputs.synthetic_system(8, 64, 120, complex=True, seed=6)
+    rng = np.random.default_rng(4)
+    T1 = (rng.standard_normal((64, 8)) + 1j * rng.standard_normal((64, 8))) * 0.02
+    T2 = (rng.standard_normal((64, 64, 8, 8)) + 1j * rng.standard_normal((64, 64, 8, 8))) * 0.02
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    sol = Solver({"precision": "split3"})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    R1, R2 = sol.residual((T1, T2))
+    sol.close()
+    Q1, Q2 = ccsd.residuum((T1, T2), ccsd.CcsdInputs(s))
+    assert _rel(R2, Q2) < 1e-5 and _rel(R1, Q1) < 1e-5
+    assert _rel(R2, Q2) > 1e-14
+    o = dict(maxIterations=60, energyConvergence=1e-10, amplitudesConvergence=1e-7)
+    a = Solver(o)
+    a.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    ra = a.run()
+    b = Solver(dict(o, precision="split3"))
+    b.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    rb = b.run()
+    assert ra["converged"] and rb["converged"]
+    assert abs(ra["correlation"] - rb["correlation"]) < 1e-6
+
+
 @pytest.mark.parametrize("shape", [(8, 40, 200), (10, 64, 150)])
 def test_split_precision_energy_within_1ueh(Solver, shape):
     """Converged CCSD energy of the split-precision form within 1 uEh of FP64."""
