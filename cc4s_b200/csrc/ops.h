@@ -79,8 +79,8 @@ void jacobi_packed(double* Tnew_p, double* dT_p, const double* R, const double* 
 
 // Correlation energy of amplitudes T (AmpShape layout) with the pair-layout integrals
 // Vd[(a,i),(b,j)] = V_abij and Ve[(a,i),(b,j)] = V_abji (real and optional imaginary planes).
-// Ve_re == nullptr (real path only): the exchange integrals are read from Vd itself,
-// V_abji = Vd[(a,j),(b,i)].
+// Ve_re == nullptr: the exchange integrals are read from Vd itself,
+// V_baij = Vd[(b,i),(a,j)] (for real integrals this equals V_abji).
 // Writes 4 doubles to out_dev: Re(direct), Re(exchange), Im(direct), Im(exchange).
 void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
             const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s);

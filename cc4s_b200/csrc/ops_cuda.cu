@@ -249,16 +249,24 @@ __global__ void energy_kernel(EnergyArgs a) {
   for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n2;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t r = e / n1, c = e - (e / n1) * n1;
+    // exchange element: Ve[e] or, without Ve, V_baij = Vd[(b,i),(a,j)] (coalesced in j)
+    int64_t ex = e;
+    if (!a.Ver) {
+      const int64_t aa = r / a.o, i = r - aa * a.o, b = c / a.o, j = c - b * a.o;
+      ex = (b * a.o + i) * n1 + aa * a.o + j;
+    }
+    const double* Ver = a.Ver ? a.Ver : a.Vdr;
+    const double* Vei = a.Ver ? a.Vei : a.Vdi;
     if (!t1i) {
       const double x = t2r[e] + t1r[r] * t1r[c];
       acc[0] += x * a.Vdr[e];
-      acc[1] += x * a.Ver[e];
+      acc[1] += x * Ver[ex];
     } else {
       // X = T2 + T1 T1 (complex);  X * conj(V)
       const double xr = t2r[e] + t1r[r] * t1r[c] - t1i[r] * t1i[c];
       const double xi = t2i[e] + t1r[r] * t1i[c] + t1i[r] * t1r[c];
       const double vdr = a.Vdr[e], vdi = a.Vdi ? a.Vdi[e] : 0.0;
-      const double ver = a.Ver[e], vei = a.Vei ? a.Vei[e] : 0.0;
+      const double ver = Ver[ex], vei = Vei ? Vei[ex] : 0.0;
       acc[0] += xr * vdr + xi * vdi;
       acc[1] += xr * ver + xi * vei;
       acc[2] += xi * vdr - xr * vdi;
@@ -488,55 +496,6 @@ __global__ void lincomb_packed_kernel(PackedLinArgs a) {
   if (a.ws) {
     block_sum<1>(nrm);
     if (threadIdx.x == 0) a.ws[blockIdx.x] = nrm[0];
-  }
-}
-
-struct EnergySwapArgs {
-  const double* T; const double* Vd;
-  int64_t o, v, oT, items;  // oT = ceil(o / 32); items = v * v * oT * oT
-  double* ws;
-};
-
-// Real-path energy with the exchange integrals read from Vd: for each pair (a, b)
-// the o x o blocks X_ab[i][j] and Vd_ab[j][i] = V_abji meet through a shared-memory
-// transpose; the direct term reads Vd_ab[i][j] in place.
-__global__ void energy_swap_kernel(EnergySwapArgs a) {
-  __shared__ double tile[32][33];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int64_t o = a.o, v = a.v, n1 = v * o;
-  const double* t1 = a.T;
-  const double* t2 = a.T + n1;
-  double acc[2] = {0.0, 0.0};
-  for (int64_t it = blockIdx.x; it < a.items; it += gridDim.x) {
-    int64_t rest = it;
-    const int64_t jt = rest % a.oT; rest /= a.oT;
-    const int64_t itile = rest % a.oT; rest /= a.oT;
-    const int64_t b = rest % v, aa = rest / v;
-    const int64_t i0 = itile * 32, j0 = jt * 32;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {  // tile[jj][ii] = Vd[(aa, j0+jj), (b, i0+ii)]
-      const int64_t j = j0 + ty + 8 * q, i = i0 + tx;
-      tile[ty + 8 * q][tx] = (j < o && i < o) ? a.Vd[(aa * o + j) * n1 + b * o + i] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int64_t i = i0 + ty + 8 * q, j = j0 + tx;
-      if (i < o && j < o) {
-        const int64_t e = (aa * o + i) * n1 + b * o + j;
-        const double x = t2[e] + t1[aa * o + i] * t1[b * o + j];
-        acc[0] += x * a.Vd[e];
-        acc[1] += x * tile[tx][ty + 8 * q];
-      }
-    }
-    __syncthreads();
-  }
-  block_sum<2>(acc);
-  if (threadIdx.x == 0) {
-    a.ws[blockIdx.x * 4 + 0] = acc[0];
-    a.ws[blockIdx.x * 4 + 1] = acc[1];
-    a.ws[blockIdx.x * 4 + 2] = 0.0;
-    a.ws[blockIdx.x * 4 + 3] = 0.0;
   }
 }
 
@@ -796,16 +755,8 @@ void lincomb_packed(double* out, const double* const* xs, const double* const* y
 
 void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
             const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s) {
-  if (!Ve_re) {
-    if (sh.planes != 1 || Vd_im || Ve_im)
-      throw Error(ERR_UNSUPPORTED, "energy: exchange from Vd on the real path only");
-    EnergySwapArgs a{T, Vd_re, sh.o, sh.v, (sh.o + 31) / 32, 0, ws};
-    a.items = sh.v * sh.v * a.oT * a.oT;
-    energy_swap_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
-  } else {
-    EnergyArgs a{T, Vd_re, Vd_im, Ve_re, Ve_im, sh.o, sh.v, sh.plane(), (int)sh.planes, ws};
-    energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
-  }
+  EnergyArgs a{T, Vd_re, Vd_im, Ve_re, Ve_im, sh.o, sh.v, sh.plane(), (int)sh.planes, ws};
+  energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
   CC_LAUNCH_CHECK();
   // direct = 2 * sum X V_ijab, exchange = -sum X V_ijba  (CoupledCluster.cxx:223-232)
   finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 4, 2.0, -1.0, 2.0, -1.0);

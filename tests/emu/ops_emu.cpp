@@ -284,23 +284,22 @@ void energy(const double* T, const double* Vdr, const double* Vdi, const double*
   for (int64_t r = 0; r < n1; ++r)
     for (int64_t c = 0; c < n1; ++c) {
       const int64_t e = r * n1 + c;
+      // V_baij = Vd[(b,i),(a,j)] when no exchange tensor is given
+      const int64_t ex = ((c / sh.o) * sh.o + r % sh.o) * n1 + (r / sh.o) * sh.o + c % sh.o;
       if (!t1i) {
         const double x = t2r[e] + t1r[r] * t1r[c];
         acc[0] += x * Vdr[e];
-        if (Ver) {
-          acc[1] += x * Ver[e];
-        } else {  // V_abji = Vd[(a,j),(b,i)]
-          const int64_t a = r / sh.o, i = r % sh.o, b = c / sh.o, j = c % sh.o;
-          acc[1] += x * Vdr[(a * sh.o + j) * n1 + b * sh.o + i];
-        }
+        acc[1] += x * (Ver ? Ver[e] : Vdr[ex]);
       } else {
         const double xr = t2r[e] + t1r[r] * t1r[c] - t1i[r] * t1i[c];
         const double xi = t2i[e] + t1r[r] * t1i[c] + t1i[r] * t1r[c];
-        const double vdi = Vdi ? Vdi[e] : 0.0, vei = Vei ? Vei[e] : 0.0;
+        const double vdi = Vdi ? Vdi[e] : 0.0;
+        const double ver = Ver ? Ver[e] : Vdr[ex];
+        const double vei = Ver ? (Vei ? Vei[e] : 0.0) : (Vdi ? Vdi[ex] : 0.0);
         acc[0] += xr * Vdr[e] + xi * vdi;
-        acc[1] += xr * Ver[e] + xi * vei;
+        acc[1] += xr * ver + xi * vei;
         acc[2] += xi * Vdr[e] - xr * vdi;
-        acc[3] += xi * Ver[e] - xr * vei;
+        acc[3] += xi * ver - xr * vei;
       }
     }
   out[0] = 2.0 * acc[0]; out[1] = -acc[1]; out[2] = 2.0 * acc[2]; out[3] = -acc[3];
