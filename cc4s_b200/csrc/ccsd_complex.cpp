@@ -4,7 +4,8 @@
 //
 // Integrals follow VertexCoulombIntegrals.cxx:143-190:
 //   V_pqsr = sum_G conj(Gamma_G,s,p) Gamma_G,q,r.
-// Layouts as on the real path (pair [a][i][b][j], exchange, pp).  Exact
+// Layouts as on the real path: pair [a][i][b][j] storage, other pairings as
+// two-level strided views (strides a: o*vo, i: vo, b: o, j: 1).  Exact
 // rearrangements relative to the reference:
 //   * Vphhh T1 and Vphhp T1 T1 (Ccsd.cxx:490-491) are contracted through the
 //     vertex: sum_G conj(Gamma_G,i,a) sum_k T_bk (Gamma_G,k,j + sum_c Gamma_G,k,c T_cj);
@@ -17,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace cc4s_b200 {
 
@@ -31,9 +33,10 @@ CcsdComplex::CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Strea
                                                            std::min<int64_t>(64 * v * v, int64_t(1) << 25)));
     scratch_.p = take(scratch_.elems);
     auto z = [&](int64_t n) { return take(2 * n); };
-    Vd_ = z(D2); Ven_ = z(D2); Vh4_ = z(D2); Vtc_ = z(D2); M2_ = z(D2); M3_ = z(D2);
+    Vd_ = z(D2); Vh4_ = z(D2); M2_ = z(D2);
     Vhhhh_ = z(o * o * o * o); Vhhhp_ = z(o * o * o * v); Vh2_ = z(o * o * o * v);
-    Xd_ = z(D2); Xp_ = z(D2); Te_ = z(D2); Y_ = z(D2); W8_ = z(D2); Tp_ = z(D2); EX_ = z(D2);
+    Xd_ = z(D2); Y_ = z(D2); EX_ = z(D2);
+    W8_ = EX_;
     Kki_ = z(o * o); Kac_ = z(v * v); Lac_ = z(v * v); Lki_ = z(o * o); jG_ = z(G);
     U_ = z(G * n1); cTdGph_ = z(G * n1); W_ = z(G * n1); SQ_ = z(G * n1); W1_ = z(G * n1);
     F_ = z(G * n1); cTdGpp_ = z(G * v * v); dGpp_ = z(G * v * v); dGhh_ = z(G * o * o);
@@ -43,9 +46,20 @@ CcsdComplex::CcsdComplex(const ComplexSystem& sys, const RealOptions& opt, Strea
     // reference mirrors each a > b slice pair into (b,a,j,i), which equals the
     // directly computed block only for a Hermitian vertex, so for a general
     // complex vertex the result depends on the slicing (Ccsd.cxx:553-598).
+    // Panels of c (slab V[x][y][c-panel][d] within 2^28 complex values, or
+    // CC4S_PPL_SLAB_DOUBLES) split the sum over c exactly and change nothing.
     const int64_t sl = opt.slab > 0 ? opt.slab : o;
     slab_rows_ = std::min(sl, v);
-    if (opt.ppl) slab_ = z(slab_rows_ * slab_rows_ * v * v);
+    int64_t budget = int64_t(1) << 28;
+    if (const char* e = std::getenv("CC4S_PPL_SLAB_DOUBLES")) {
+      const long long b = std::atoll(e);
+      if (b > 0) budget = b;
+    }
+    const int64_t cmax = std::max<int64_t>(
+        1, std::min<int64_t>(v, budget / (slab_rows_ * slab_rows_ * v)));
+    const int64_t npanels = (v + cmax - 1) / cmax;
+    slab_cols_ = (v + npanels - 1) / npanels;
+    if (opt.ppl) slab_ = z(slab_rows_ * slab_rows_ * slab_cols_ * v);
   } catch (...) {
     release_all();
     throw;
@@ -82,8 +96,6 @@ void CcsdComplex::build_integrals() {
     c.C = vw(Vd_, o * n1, n1, 0, 1);
     zgemm(c, gph, gph, D2, true, false);
   }
-  const int64_t d4[4] = {v, o, v, o};
-  { const int pm[4] = {2, 1, 0, 3}; zperm(Ven_, D2, Vd_, D2, d4, pm, 1.0, 0.0); }  // V_baij
   {  // Vh4[k][l][c][d] = V_klcd = sum_G conj(Gph[G][c][k]) Ghp[G][l][d]
     Contraction c; c.M = o * v; c.N = o * v; c.K = G; c.Mi = v; c.Ni = v;
     c.A = vw(Gph, 1, o, 0, n1);
@@ -92,16 +104,10 @@ void CcsdComplex::build_integrals() {
     zgemm(c, gph, gph, D2, true, false);
   }
   const int64_t dh[4] = {o, o, v, v};  // Vh4 [k][l][c][d]
-  {  // Vtc[c][d][k][l] = 2 V_klcd - V_kldc
-    const int pa[4] = {2, 3, 0, 1}, pb[4] = {3, 2, 0, 1};
-    zperm(Vtc_, D2, Vh4_, D2, dh, pa, 2.0, 0.0);
-    zperm(Vtc_, D2, Vh4_, D2, dh, pb, -1.0, 1.0);
-  }
-  {  // M2[(c,k),(d,l)] = V_lkdc - V_lkcd / 2 ;  M3[(c,k),(d,l)] = V_lkcd
+  {  // M2[(c,k),(d,l)] = V_lkdc - V_lkcd / 2  (V_lkcd itself is read as a view of Vh4)
     const int pa[4] = {3, 1, 2, 0}, pb[4] = {2, 1, 3, 0};
     zperm(M2_, D2, Vh4_, D2, dh, pa, 1.0, 0.0);
     zperm(M2_, D2, Vh4_, D2, dh, pb, -0.5, 1.0);
-    zperm(M3_, D2, Vh4_, D2, dh, pb, 1.0, 0.0);
   }
   const int64_t o4 = o * o * o * o, o3v = o * o * o * v;
   {  // Vhhhh[k][l][i][j] = sum_G conj(Ghh[G][i][k]) Ghh[G][l][j]
@@ -118,9 +124,9 @@ void CcsdComplex::build_integrals() {
     c.C = vw(Vhhhp_, o * o * v, v, o * v, 1);
     zgemm(c, G * o * o, gph, o3v, true, false);
   }
-  {  // Vh2[i][c][k][l] = 2 V_klic - V_lkic
+  {  // Vh2[i][k][c][l] = 2 V_klic - V_lkic
     const int64_t dv[4] = {o, o, o, v};
-    const int pa[4] = {2, 3, 0, 1}, pb[4] = {2, 3, 1, 0};
+    const int pa[4] = {2, 0, 3, 1}, pb[4] = {2, 1, 3, 0};
     zperm(Vh2_, o3v, Vhhhp_, o3v, dv, pa, 2.0, 0.0);
     zperm(Vh2_, o3v, Vhhhp_, o3v, dv, pb, -1.0, 1.0);
   }
@@ -146,23 +152,33 @@ void CcsdComplex::residual(const double* T, double* R) {
   const int64_t gpp = G * v * v, gph = G * n1, ghh = G * o * o, o4 = o * o * o * o,
                 o3v = o * o * o * v, gov = G * o * v;
   const int64_t d4[4] = {v, o, v, o};
-  const int p_pp[4] = {0, 2, 1, 3};
+  const int64_t dh[4] = {o, o, v, v};  // Vh4 [k][l][c][d]
   const int p_ex[4] = {0, 3, 2, 1};
+  const int64_t sA = o * n1, sI = n1, sB = o;  // pair-layout strides
 
   // ---- X = T2 + T1 T1 (Ccsd.cxx:460-461) ----------------------------------------
   if (ccd) { ops::d2d(Xd_, Td, D2, s_); ops::d2d(Xd_ + D2, Td + pl, D2, s_); }
   else ops::zrank1(Xd_, Xd_ + D2, Td, Td + pl, t, t + pl, 1.0, n1, s_);
-  zperm(Xp_, D2, Xd_, D2, d4, p_pp, 1.0, 0.0);
   // ---- Kac, Kki (Ccsd.cxx:465-473) ---------------------------------------------
-  {
-    Contraction c; c.M = o; c.N = o; c.K = v * v * o; c.Ki = o;
-    c.A = vw(Vtc_, 0, o, o * o, 1); c.B = vw(Xp_, o * o, 1, 0, o); c.C = rm(Kki_, o);
+  {  // EX <- Vt[(c,k),(d,l)] = 2 V_klcd - V_kldc
+    const int pa[4] = {2, 0, 3, 1}, pb[4] = {3, 0, 2, 1};
+    zperm(EX_, D2, Vh4_, D2, dh, pa, 2.0, 0.0);
+    zperm(EX_, D2, Vh4_, D2, dh, pb, -1.0, 1.0);
+  }
+  {  // Kki[k][i] = sum_{c,(d,l)} Vt[(c,k),(d,l)] X[(c,i),(d,l)]
+    Contraction c; c.M = o; c.N = o; c.K = v * n1; c.Ki = n1;
+    c.A = vw(EX_, 0, sI, sA, 1); c.B = vw(Xd_, sA, 1, 0, sI); c.C = rm(Kki_, o);
     zgemm(c, D2, D2, o * o);
   }
-  {
-    Contraction c; c.M = v; c.N = v; c.K = v * o * o;
-    c.A = rm(Xp_, v * o * o); c.B = tr(Vtc_, v * o * o); c.C = rm(Kac_, v); c.alpha = -1.0;
+  {  // Kac[a][c] = -sum_{k,(d,l)} X[(a,k),(d,l)] Vt[(c,k),(d,l)]
+    Contraction c; c.M = v; c.N = v; c.K = o * n1; c.Ki = n1;
+    c.A = vw(Xd_, 0, sA, sI, 1); c.B = vw(EX_, sI, 1, 0, sA); c.C = rm(Kac_, v); c.alpha = -1.0;
     zgemm(c, D2, D2, v * v);
+  }
+  if (!ccd) {  // kck[(c,k)] = sum_{(d,l)} Vt[(c,k),(d,l)] t[d][l]  (for the singles)
+    Contraction c; c.M = n1; c.N = 1; c.K = n1;
+    c.A = rm(EX_, n1); c.B = vw(t, 0, 1, 0, 0); c.C = vw(kck_, 0, 1, 0, 0);
+    zgemm(c, D2, pl, n1);
   }
   // ---- Lac (Ccsd.cxx:468-470) ----------------------------------------------------
   ops::d2d(Lac_, Kac_, 2 * v * v, s_);
@@ -194,7 +210,7 @@ void CcsdComplex::residual(const double* T, double* R) {
   ops::d2d(Lki_, Kki_, 2 * o * o, s_);
   if (!ccd) {
     Contraction c; c.M = o * o; c.N = 1; c.K = v * o; c.Mi = o; c.Ki = o;
-    c.A = vw(Vh2_, v * o * o, o, o * o, 1); c.B = vw(t, o, 1, 0, 0); c.C = vw(Lki_, 1, o, 0, 0);
+    c.A = vw(Vh2_, v * o * o, v * o, o, 1); c.B = vw(t, o, 1, 0, 0); c.C = vw(Lki_, 1, o, 0, 0);
     c.beta = 1.0;
     zgemm(c, o3v, pl, o * o);
   }
@@ -253,7 +269,6 @@ void CcsdComplex::residual(const double* T, double* R) {
     }
   }
   // ---- ring Xakic (Ccsd.cxx:494-502) -----------------------------------------------
-  zperm(Te_, D2, Td, pl, d4, p_ex, 1.0, 0.0);
   if (ccd) { ops::d2d(W8_, Td, D2, s_); ops::d2d(W8_ + D2, Td + pl, D2, s_); }
   else ops::zrank1(W8_, W8_ + D2, Td, Td + pl, t, t + pl, 2.0, n1, s_);
   zperm(Y_, D2, W8_, D2, d4, p_ex, 1.0, 0.0);  // (T2 + 2 T1 T1)^x
@@ -268,8 +283,9 @@ void CcsdComplex::residual(const double* T, double* R) {
     c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(cTdGph_, n1); c.alpha = -0.5; c.beta = 1.0;
     zgemm(c, gph, D2, gph, true, false, true);
   }
-  ops::axpby(Y_, 2.0, Td, -1.0, Te_, 0.0, D2, s_);            // Y = 2T - T^x
-  ops::axpby(Y_ + D2, 2.0, Td + pl, -1.0, Te_ + D2, 0.0, D2, s_);
+  zperm(Y_, D2, Td, pl, d4, p_ex, -1.0, 0.0);                 // -T^x
+  ops::axpby(Y_, 2.0, Td, 1.0, Y_, 0.0, D2, s_);              // Y = 2T - T^x
+  ops::axpby(Y_ + D2, 2.0, Td + pl, 1.0, Y_ + D2, 0.0, D2, s_);
   {  // W1[G][(b,j)] = sum_{c,k} Ghp[G][k][c] Y[(c,k),(b,j)]
     Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
     c.A = vw(Ghp, 0, n1, 1, v); c.B = vw(Y_, o * n1, n1, 0, 1); c.C = rm(W1_, n1);
@@ -300,10 +316,12 @@ void CcsdComplex::residual(const double* T, double* R) {
     c.alpha = -1.0; c.beta = 1.0;
     zgemm(c, pl, gph, gpp, false, true);
   }
-  {  // EX = -1/2 T^x M3^T
-    Contraction c; c.M = n1; c.N = n1; c.K = n1;
-    c.A = rm(Te_, n1); c.B = tr(M3_, n1); c.C = rm(EX_, n1); c.alpha = -0.5;
-    zgemm(c, D2, D2, D2, false, false, true);
+  {  // EX[(a,i),(c,k)] = -1/2 sum_{l,d} T_adli V_lkcd   (k = (l, d); T^x and Vh4 views)
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ki = v; c.Ni = o;
+    c.A = vw(Td, sA, 1, sI, sB);                   // T_adli = T[(a,l),(d,i)]
+    c.B = vw(Vh4_, o * v * v, 1, v, v * v);        // V_lkcd = Vh4[l][k][c][d]
+    c.C = vw(EX_, sA, sI, o, 1); c.alpha = -0.5;
+    zgemm(c, pl, D2, D2, false, false, true);
   }
   {  // EX[a][i][c][k] += sum_G cTdGpp[G][a][c] dGhh[G][k][i]
     Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
@@ -317,10 +335,11 @@ void CcsdComplex::residual(const double* T, double* R) {
     zgemm(c, D2, pl, pl, false, false, true);
   }
   {  // R2_abij -= sum_ck T_ackj X_bkci   (exchange pairing)
-    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o;
-    c.A = vw(Te_, o * n1, n1, 0, 1); c.B = vw(EX_, 0, 1, o * n1, n1);
-    c.C = vw(R2, o * n1, 1, o, n1); c.alpha = -1.0; c.beta = 1.0;
-    zgemm(c, D2, D2, pl, false, false, true);
+    Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o; c.Ki = o;
+    c.A = vw(Td, sA, 1, sB, sI);                   // T_ackj = T[(a,k),(c,j)]
+    c.B = vw(EX_, sB, 1, sA, sI);                  // X_bkci = EX[(b,i),(c,k)]
+    c.C = vw(R2, sA, 1, sB, sI); c.alpha = -1.0; c.beta = 1.0;
+    zgemm(c, pl, D2, pl, false, false, true);
   }
   // ---- symmetrisation, +V (Ccsd.cxx:520,529) -----------------------------------
   ops::symmetrize(R2, n1, s_);
@@ -342,20 +361,25 @@ void CcsdComplex::residual(const double* T, double* R) {
       zgemm(c, o3v, pl, o4);
     }
   }
-  zperm(Tp_, D2, Td, pl, d4, p_pp, 1.0, 0.0);
-  {  // Xkl2[kl][ij] = sum_cd V_klcd X_cdij
-    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v;
-    c.A = rm(Vh4_, v * v); c.B = rm(Xp_, o * o); c.C = rm(Xkl2_, o * o);
+  {  // Xkl2[kl][ij] = sum_cd V_klcd X_cdij   (k = (c,d))
+    Contraction c; c.M = o * o; c.N = o * o; c.K = v * v; c.Ki = v; c.Ni = o;
+    c.A = vw(Vh4_, 0, v * v, v, 1);
+    c.B = vw(Xd_, sA, sB, sI, 1);                  // X_cdij = X[(c,i),(d,j)]
+    c.C = vw(Xkl2_, 0, o * o, o, 1);
     zgemm(c, D2, D2, o4, false, false, true);
   }
-  {
-    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ni = o;
-    c.A = vw(Xp_, v * o * o, o * o, 0, 1); c.B = vw(Xkl1_, 0, o * o, o, 1);
-    c.C = vw(R2, o * n1, o, n1, 1); c.beta = 1.0;
+  {  // R2 += Xkl1 X_abkl, R2 += Xkl2 T_abkl (or X_abkl)   (m = (a,b), k = (k,l))
+    Contraction c; c.M = v * v; c.N = o * o; c.K = o * o; c.Mi = v; c.Ki = o; c.Ni = o;
+    c.A = vw(Xd_, sA, sB, sI, 1); c.B = vw(Xkl1_, o * o * o, o * o, o, 1);
+    c.C = vw(R2, sA, sB, sI, 1); c.beta = 1.0;
     zgemm(c, D2, o4, pl, false, false, true);
-    c.A.p = opt_.ppl ? Tp_ : Xp_;
     c.B.p = Xkl2_;
-    zgemm(c, D2, o4, pl, false, false, true);
+    if (opt_.ppl) {
+      c.A.p = cp(Td);
+      zgemm(c, pl, o4, pl, false, false, true);
+    } else {
+      zgemm(c, D2, o4, pl, false, false, true);
+    }
   }
   // ---- particle-particle ladder (Ccsd.cxx:549-601) ---------------------------------
   if (opt_.ppl) {
@@ -366,28 +390,32 @@ void CcsdComplex::residual(const double* T, double* R) {
       c.alpha = -1.0; c.beta = 1.0;
       zgemm(c, pl, gph, gpp);
     }
-    const int64_t s = slab_rows_, nb = (v + s - 1) / s, sz = s * s * v * v;
-    for (int64_t X = 0; X < nb; ++X)
-      for (int64_t Yb = 0; Yb <= X; ++Yb) {
-        const int64_t x0 = X * s, sx = std::min(s, v - x0);
-        const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
-        {
-          Contraction c; c.M = sx * v; c.N = sy * v; c.K = G; c.Mi = v; c.Ni = v;
-          c.A = vw(cTdGpp_ + x0 * v, v, 1, 0, v * v);
-          c.B = vw(dGpp_ + y0 * v, 0, v * v, v, 1);
-          c.C = vw(slab_, sy * v * v, v, v * v, 1);
-          zgemm(c, gpp, gpp, sz, false, false, true);
+    const int64_t s = slab_rows_, cn = slab_cols_, nb = (v + s - 1) / s;
+    const int64_t sz = s * s * cn * v;  // imaginary plane of the slab
+    for (int64_t c0 = 0; c0 < v; c0 += cn) {
+      const int64_t nc = std::min(cn, v - c0);
+      for (int64_t X = 0; X < nb; ++X)
+        for (int64_t Yb = 0; Yb <= X; ++Yb) {
+          const int64_t x0 = X * s, sx = std::min(s, v - x0);
+          const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
+          {  // slab[x][y][c'][d], m = (x, c'), n = (y, d)
+            Contraction c; c.M = sx * nc; c.N = sy * v; c.K = G; c.Mi = nc; c.Ni = v;
+            c.A = vw(cTdGpp_ + x0 * v + c0, v, 1, 0, v * v);
+            c.B = vw(dGpp_ + y0 * v, 0, v * v, v, 1);
+            c.C = vw(slab_, sy * nc * v, v, nc * v, 1);
+            zgemm(c, gpp, gpp, sz, false, false, true);
+          }
+          {  // m = (x, y), k = (c', d), n = (i, j)
+            Contraction c; c.M = sx * sy; c.N = o * o; c.K = nc * v; c.Mi = sy; c.Ki = v; c.Ni = o;
+            c.A = vw(slab_, sy * nc * v, nc * v, v, 1);
+            c.B = vw(Xd_ + c0 * sA, sA, sB, sI, 1);   // X_cdij = X[(c,i),(d,j)]
+            c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
+            if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
+            c.beta = 1.0;
+            zgemm(c, sz, D2, pl, false, false, true);
+          }
         }
-        {
-          Contraction c; c.M = sx * sy; c.N = o * o; c.K = v * v; c.Mi = sy; c.Ni = o;
-          c.A = vw(slab_, sy * v * v, v * v, 0, 1);
-          c.B = vw(Xp_, 0, o * o, o, 1);
-          c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
-          if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
-          c.beta = 1.0;
-          zgemm(c, sz, D2, pl, false, false, true);
-        }
-      }
+    }
   }
   if (ccd) {
     ops::zero(R1, n1, s_);
@@ -403,11 +431,6 @@ void CcsdComplex::residual(const double* T, double* R) {
     Contraction d; d.M = v; d.N = o; d.K = o;
     d.A = rm(t, o); d.B = rm(Kki_, o); d.C = rm(R1, o); d.alpha = -1.0; d.beta = 1.0;
     zgemm(d, pl, o * o, pl);
-  }
-  {  // kck[(c,k)] = sum_{d,l} Vtc[c][d][k][l] t[d][l]
-    Contraction c; c.M = n1; c.N = 1; c.K = n1; c.Mi = o; c.Ki = o;
-    c.A = vw(Vtc_, v * o * o, o, o * o, 1); c.B = vw(t, o, 1, 0, 0); c.C = vw(kck_, o, 1, 0, 0);
-    zgemm(c, D2, pl, n1);
   }
   {  // R1 += (2T - T^x) kck
     Contraction c; c.M = n1; c.N = 1; c.K = n1;
@@ -448,9 +471,9 @@ void CcsdComplex::residual(const double* T, double* R) {
     d.A = vw(Gpp, 0, 1, v * v, v); d.B = vw(F_, n1, o, 0, 1); d.C = rm(R1, o); d.beta = 1.0;
     zgemm(d, gpp, gph, pl, true, false);
   }
-  {  // R1 -= Xp Vh2^T
-    Contraction c; c.M = v; c.N = o; c.K = v * o * o;
-    c.A = rm(Xp_, v * o * o); c.B = tr(Vh2_, v * o * o); c.C = rm(R1, o);
+  {  // R1[a][i] -= sum_{k,(c,l)} X[(a,k),(c,l)] Vh2[i][k][c][l]
+    Contraction c; c.M = v; c.N = o; c.K = o * n1; c.Ki = n1;
+    c.A = vw(Xd_, 0, sA, sI, 1); c.B = vw(Vh2_, n1, 1, 0, o * n1); c.C = rm(R1, o);
     c.alpha = -1.0; c.beta = 1.0;
     zgemm(c, D2, o3v, pl);
   }

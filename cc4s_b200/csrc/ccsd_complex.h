@@ -27,9 +27,10 @@ class CcsdComplex : public Schedule {
 
   void residual(const double* T, double* R) override;
   const double* Vd() const override { return Vd_; }
-  const double* Ve() const override { return Ven_; }
+  // The exchange integrals V_baij are read from Vd by block swap (no copy).
+  const double* Ve() const override { return nullptr; }
   const double* Vd_im() const override { return Vd_ + D2_; }
-  const double* Ve_im() const override { return Ven_ + D2_; }
+  const double* Ve_im() const override { return nullptr; }
 
  private:
   void zperm(double* dst, int64_t dst_im, const double* src, int64_t src_im, const int64_t d[4],
@@ -40,16 +41,18 @@ class CcsdComplex : public Schedule {
   ComplexSystem sys_;
   RealOptions opt_;
   int64_t D2_ = 0;
-  double *Vd_ = nullptr, *Ven_ = nullptr, *Vh4_ = nullptr, *Vtc_ = nullptr, *M2_ = nullptr,
-         *M3_ = nullptr, *Vhhhh_ = nullptr, *Vhhhp_ = nullptr, *Vh2_ = nullptr;
-  double *Xd_ = nullptr, *Xp_ = nullptr, *Te_ = nullptr, *Y_ = nullptr, *W8_ = nullptr,
-         *Tp_ = nullptr, *EX_ = nullptr;
+  // Stored (vo)^2 complex tensors: Vd, Vh4, M2, X, Y, EX.  Every other pairing
+  // is a strided view; EX also holds 2 V_klcd - V_kldc at the start of a
+  // residual and the ring / singles combinations (W8) between uses.
+  double *Vd_ = nullptr, *Vh4_ = nullptr, *M2_ = nullptr, *Vhhhh_ = nullptr,
+         *Vhhhp_ = nullptr, *Vh2_ = nullptr;
+  double *Xd_ = nullptr, *Y_ = nullptr, *W8_ = nullptr, *EX_ = nullptr;
   double *Kki_ = nullptr, *Kac_ = nullptr, *Lac_ = nullptr, *Lki_ = nullptr, *jG_ = nullptr,
          *U_ = nullptr, *cTdGph_ = nullptr, *W_ = nullptr, *SQ_ = nullptr, *W1_ = nullptr,
          *F_ = nullptr, *cTdGpp_ = nullptr, *dGpp_ = nullptr, *dGhh_ = nullptr,
          *Xkl1_ = nullptr, *Xkl2_ = nullptr, *kck_ = nullptr, *P1_ = nullptr, *P_ = nullptr,
          *slab_ = nullptr;
-  int64_t slab_rows_ = 0;
+  int64_t slab_rows_ = 0, slab_cols_ = 0;  // ladder block size, c-panel size
 };
 
 }  // namespace cc4s_b200

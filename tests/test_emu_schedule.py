@@ -52,17 +52,23 @@ def test_residual_matches_oracle(emu_lib, shape, method):
             assert np.abs(R1).max() == 0.0
 
 
+@pytest.mark.parametrize("cplx", [False, True])
 @pytest.mark.parametrize("slice_size,budget", [(4, 528), (5, 300), (11, 0)])
-def test_ladder_blocks_and_c_panels(emu_lib, monkeypatch, slice_size, budget):
-    """Real-path ladder on several virtual blocks (integralsSliceSize) and several
-    panels of c (slab budget CC4S_PPL_SLAB_DOUBLES), ragged edges included."""
+def test_ladder_blocks_and_c_panels(emu_lib, monkeypatch, slice_size, budget, cplx):
+    """Ladder on several virtual blocks (integralsSliceSize) and several panels of
+    c (slab budget CC4S_PPL_SLAB_DOUBLES), ragged edges included; the complex case
+    uses a Hermitian vertex, for which the reference's slicing is exact."""
     from cc4s_b200 import Solver
     if budget:
         monkeypatch.setenv("CC4S_PPL_SLAB_DOUBLES", str(budget))
-    s = inputs.synthetic_system(4, 11, 12, seed=5)
+    s = inputs.synthetic_system(4, 11, 12, complex=cplx, seed=5)
     T = _rand_T(np.random.default_rng(8), 11, 4)
+    if cplx:
+        rng = np.random.default_rng(9)
+        T = (T[0] + 0.05j * rng.standard_normal(T[0].shape),
+             T[1] + 0.05j * (lambda x: x + x.transpose(1, 0, 3, 2))(rng.standard_normal(T[1].shape)))
     sol = Solver({"integralsSliceSize": slice_size}, lib=emu_lib)
-    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
     R1, R2 = sol.residual(T)
     Q1, Q2 = ccsd.residuum(T, ccsd.CcsdInputs(s))
     assert _rel(R2, Q2) < 1e-13 and _rel(R1, Q1) < 1e-13
