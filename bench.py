@@ -34,8 +34,10 @@ sys.path.insert(0, ROOT)
 warnings.simplefilter("ignore")
 
 CONFIG_SHAPES = {
-    "c0": (8, 40, 200), "c1": (32, 256, 1024), "c2": (64, 640, 2560), "c4": (32, 320, 1600),
+    "c0": (8, 40, 200), "c1": (32, 256, 1024), "c2": (64, 640, 2560), "c3": (48, 480, 3000),
+    "c4": (32, 320, 1600),
 }
+COMPLEX_CONFIGS = {"c3"}  # complex vertex: 8 real flops per complex multiply-add
 METRIC = "CCSD s/iter & TFLOP/s: TC split-precision vs FP64 on 1 B200 at |ΔEc|≤1µEh"
 
 
@@ -141,7 +143,7 @@ def cpu_sample(cfg, target=2e12):
     t1 = time.perf_counter()
     flops = 2.0 * n * n * v * o ** 3 + 2.0 * sl * sl * v * v * (G + m * m)
     rate = flops / (t1 - t0)
-    s_iter = reference_flops(o, v, G) / rate
+    s_iter = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS) / rate
     return dict(s_per_iter=s_iter, rate_tflops=rate / 1e12, sample_seconds=t1 - t0,
                 cores=os.cpu_count(),
                 sample="oracle numpy/BLAS on %s: ring block a,b < %d of akic,cbkj->abij and one "
@@ -211,7 +213,7 @@ def run_ours(args, world, rank, local):
     o, v, G = CONFIG_SHAPES[cfg]
     inputs = config(cfg, seed=0)
     eh, ep, g, hg = inputs
-    F = reference_flops(o, v, G)
+    F = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS)
     K, W = args.steps, args.warmup
     base = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
                 mixer=dict(type="DiisMixer", maxResidua=5), device=local)
@@ -265,7 +267,8 @@ def run_ours(args, world, rank, local):
     e2e.close()
     h2d = (g.nbytes + eh.nbytes + ep.nbytes) / K
     d2h = (A1.nbytes + A2.nbytes) / K + 5 * 8 + 8
-    conf = {"workload": "CCSD %s: No=%d Nv=%d NG=%d real, DIIS 5, %s" % (cfg, o, v, G, head),
+    kind = "complex" if cfg in COMPLEX_CONFIGS else "real"
+    conf = {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, %s" % (cfg, o, v, G, kind, head),
             "precision": head, "s_per_iter": t / K,
             "flops_per_iter_reference_formulation": F,
             "flops_per_iter_executed": hr["r"]["flops_per_iteration"],
@@ -299,7 +302,7 @@ def run_reference(args, world, rank):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
     from cc4s_b200.flops import reference_flops
-    F = reference_flops(o, v, G)
+    F = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS)
     for _ in range(args.warmup):
         cpu_sample(cfg)
     samples = [cpu_sample(cfg) for _ in range(max(1, args.steps))]
@@ -310,7 +313,8 @@ def run_reference(args, world, rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * s_iter, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d real" % (cfg, o, v, G),
+            "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d %s" % (
+                cfg, o, v, G, "complex" if cfg in COMPLEX_CONFIGS else "real"),
                        "implementation": "CPU restatement of the reference (oracle, numpy/BLAS); "
                                          "the reference build needs MPI + CTF, not installed"},
             "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": c["cores"],
@@ -343,7 +347,8 @@ def main():
             c = cpu_sample(args.config)
             from cc4s_b200.flops import reference_flops
             o, v, G = CONFIG_SHAPES[args.config]
-            line["cpu_baseline"] = {"value": reference_flops(o, v, G) / c["s_per_iter"] / 1e12,
+            cfg = args.config
+            line["cpu_baseline"] = {"value": reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS) / c["s_per_iter"] / 1e12,
                                     "unit": "TFLOP/s", "cores": c["cores"], "kind": "port",
                                     "sample": c["sample"]}
         print(json.dumps(line), flush=True)
