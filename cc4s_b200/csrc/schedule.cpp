@@ -1,6 +1,11 @@
 #include "schedule.h"
 
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 
 namespace cc4s_b200 {
 
@@ -31,6 +36,7 @@ void Schedule::gemm_(const Contraction& c) {
     while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
     ev_flops_.push_back(f);
     ev_split_.push_back(0);
+    ev_shape_.push_back({c.M, c.N, c.K, c.batch});
     ops::event_record(ev_[2 * k], s_);
     gemm(c, s_, scratch_);
     ops::event_record(ev_[2 * k + 1], s_);
@@ -63,6 +69,7 @@ void Schedule::tc_(const Contraction& c) {
     while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
     ev_flops_.push_back(f);
     ev_split_.push_back(1);
+    ev_shape_.push_back({c.M, c.N, c.K, c.batch});
     ops::event_record(ev_[2 * k], s_);
     gemm_split(c, s_, split_);
     ops::event_record(ev_[2 * k + 1], s_);
@@ -171,8 +178,35 @@ void Schedule::profile_finish() {
     }
   }
   p.launches = static_cast<int>(ev_flops_.size());
+  // CC4S_PROFILE_LOG: append a per-shape summary of this residual's contractions
+  if (const char* path = std::getenv("CC4S_PROFILE_LOG")) {
+    std::map<std::array<int64_t, 5>, std::array<double, 3>> agg;  // count, seconds, flops
+    for (size_t k = 0; k < ev_flops_.size(); ++k) {
+      const auto& sh = ev_shape_[k];
+      auto& a = agg[{ev_split_[k] ? 1 : 0, sh[0], sh[1], sh[2], sh[3]}];
+      a[0] += 1;
+      a[1] += 1e-3 * ops::event_ms(ev_[2 * k], ev_[2 * k + 1]);
+      a[2] += ev_flops_[k];
+    }
+    std::vector<std::pair<double, std::array<int64_t, 5>>> order;
+    for (const auto& kv : agg) order.push_back({kv.second[1], kv.first});
+    std::sort(order.rbegin(), order.rend());
+    if (FILE* f = std::fopen(path, "a")) {
+      std::fprintf(f, "# residual: %d launches, %.4f s, %.4g flops\n", p.launches, p.gemm_seconds,
+                   p.gemm_flops);
+      std::fprintf(f, "# kind M N K batch count seconds TFLOP/s(fp64-equivalent)\n");
+      for (const auto& e : order) {
+        const auto& a = agg[e.second];
+        std::fprintf(f, "%s %lld %lld %lld %lld %d %.5f %.2f\n", e.second[0] ? "split" : "dmma",
+                     (long long)e.second[1], (long long)e.second[2], (long long)e.second[3],
+                     (long long)e.second[4], (int)a[0], a[1], a[2] / a[1] / 1e12);
+      }
+      std::fclose(f);
+    }
+  }
   ev_split_.clear();
   ev_flops_.clear();
+  ev_shape_.clear();
   prof_ = p;
 }
 

@@ -2,6 +2,7 @@
 // accounting, split-K scratch and optional per-launch timing of contractions.
 #pragma once
 
+#include <array>
 #include <vector>
 
 #include "ops.h"
@@ -98,6 +99,7 @@ class Schedule {
   std::vector<void*> ev_;
   std::vector<double> ev_flops_;
   std::vector<char> ev_split_;
+  std::vector<std::array<int64_t, 4>> ev_shape_;  // M, N, K, batch of each profiled launch
 };
 
 }  // namespace cc4s_b200
