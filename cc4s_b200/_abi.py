@@ -30,7 +30,8 @@ MIXERS = {"DiisMixer": 0, "LinearMixer": 1}
 EXPORTS = [
     "cc4s_cc_default_options", "cc4s_cc_create", "cc4s_cc_set_inputs",
     "cc4s_cc_set_initial_amplitudes", "cc4s_cc_run", "cc4s_cc_get_amplitudes",
-    "cc4s_cc_residual", "cc4s_cc_backward", "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
+    "cc4s_cc_residual", "cc4s_cc_backward", "cc4s_cc_residual_vjp", "cc4s_cc_relaxed_gradient",
+    "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
     "cc4s_cc_last_error",
 ]
 
@@ -71,6 +72,14 @@ class Stats(ctypes.Structure):
     ]
 
 
+class LambdaResult(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+        ("residuum_norm", ctypes.c_double), ("prepare_seconds", ctypes.c_double),
+        ("vjp_seconds", ctypes.c_double), ("gradient_seconds", ctypes.c_double),
+    ]
+
+
 _LIBS = {}
 
 
@@ -97,6 +106,9 @@ def load(path=None):
     lib.cc4s_cc_residual.argtypes = [ctypes.c_void_p, dp, dp, dp, dp]
     lib.cc4s_cc_get_stats.argtypes = [ctypes.c_void_p, P(Stats)]
     lib.cc4s_cc_backward.argtypes = [ctypes.c_void_p, dp, dp]
+    lib.cc4s_cc_residual_vjp.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp]
+    lib.cc4s_cc_relaxed_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, dp,
+                                             P(LambdaResult)]
     lib.cc4s_cc_energy_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p]

@@ -157,6 +157,46 @@ class Solver:
             g = g.reshape((self.NG, Np, Np), order="F")
         return S, g
 
+    def _vertex_grad_buffer(self):
+        k = 2 if self.in_complex_input else 1
+        return np.zeros(self.NG * (self.No + self.Nv) ** 2 * k)
+
+    def _vertex_grad(self, g):
+        Np = self.No + self.Nv
+        if self.in_complex_input:
+            g = g.view(np.complex128)
+        return g.reshape((self.NG, Np, Np), order="F")
+
+    def residual_vjp(self, T, Rbar, gradient=True):
+        """Transposed-Jacobian product of the residual at amplitudes T = (T1, T2):
+        returns (T1bar, T2bar) = Rbar^T dR/dT and, if asked, Rbar^T dR/dGamma in the
+        vertex layout (cc4s_cc_residual_vjp; real half-grid path)."""
+        t1 = _abi.as_f64(np.asarray(T[0], dtype=np.float64))
+        t2 = _abi.as_f64(np.asarray(T[1], dtype=np.float64))
+        r1 = _abi.as_f64(np.asarray(Rbar[0], dtype=np.float64))
+        r2 = _abi.as_f64(np.asarray(Rbar[1], dtype=np.float64))
+        b1, b2 = self._alloc_amps()
+        g = self._vertex_grad_buffer() if gradient else None
+        self._check(self.lib.cc4s_cc_residual_vjp(self.h, _abi.ptr(t1), _abi.ptr(t2), _abi.ptr(r1),
+                                                  _abi.ptr(r2), _abi.ptr(b1), _abi.ptr(b2),
+                                                  _abi.ptr(g)))
+        T1b, T2b = self._unpack(b1, b2)
+        return (T1b, T2b), (self._vertex_grad(g) if gradient else None)
+
+    def relaxed_gradient(self, max_iterations=100, convergence=1e-10):
+        """dE_c/dGamma of the converged energy (Lambda equations solved on the device;
+        cc4s_cc_relaxed_gradient).  Returns (gradient in the vertex layout, info)."""
+        g = self._vertex_grad_buffer()
+        res = _abi.LambdaResult()
+        st = self._check(self.lib.cc4s_cc_relaxed_gradient(self.h, int(max_iterations),
+                                                           float(convergence), _abi.ptr(g),
+                                                           ctypes.byref(res)),
+                         ok=(0, _abi.WARN_NOT_CONVERGED))
+        info = dict(status=st, iterations=res.iterations, converged=bool(res.converged),
+                    residuum_norm=res.residuum_norm, prepare_seconds=res.prepare_seconds,
+                    vjp_seconds=res.vjp_seconds, gradient_seconds=res.gradient_seconds)
+        return self._vertex_grad(g), info
+
     def stats(self):
         s = _abi.Stats()
         self._check(self.lib.cc4s_cc_get_stats(self.h, ctypes.byref(s)))

@@ -79,16 +79,16 @@ void Handle::set_initial(const double* T1, const double* T2) {
   have_T = true;
 }
 
-void Handle::mix(double* A_new, double* dT_new, double* norm2_dev) {
+void Handle::mix(double* A_new, double* dT_new, double* norm2_dev, double* out) {
   const int64_t n = shape.total();
   if (opt.mixer == CC4S_MIXER_LINEAR) {
     const double r = opt.ratio;
     if (!linear_has_last) {
-      ops::d2d(Tcur, A_new, n, stream);
+      ops::d2d(out, A_new, n, stream);
       ops::d2d(dTlast, dT_new, n, stream);
       linear_has_last = true;
     } else {
-      ops::axpby(Tcur, r, A_new, 1.0 - r, Tcur, 0.0, n, stream);
+      ops::axpby(out, r, A_new, 1.0 - r, out, 0.0, n, stream);
       ops::axpby(dTlast, r, dT_new, 1.0 - r, dTlast, 0.0, n, stream);
     }
     const double* ys[1] = {dTlast};
@@ -112,7 +112,7 @@ void Handle::mix(double* A_new, double* dT_new, double* norm2_dev) {
     xs[j] = A[slot];
     rs[j] = Rs[slot];
   }
-  ops::lincomb_packed(Tcur, xs, rs, coef, count, shape, norm2_dev, ws, stream);
+  ops::lincomb_packed(out, xs, rs, coef, count, shape, norm2_dev, ws, stream);
   next_index = (next + 1) % N;
 }
 
@@ -139,7 +139,7 @@ int Handle::run(cc4s_cc_result* out) {
       ops::jacobi(A[slot], Rs[slot], Rbuf, have_T ? Tcur : nullptr, sys.eh, sys.ep, shape, shift,
                   stream);
     const bool second = !have_T;
-    mix(A[slot], Rs[slot], scal + 4);
+    mix(A[slot], Rs[slot], scal + 4, Tcur);
     have_T = true;
     ops::energy(Tcur, solver->Vd(), solver->Vd_im(), solver->Ve(), solver->Ve_im(), shape, scal, ws, stream);
     ops::event_record(ev1, stream);
@@ -260,6 +260,156 @@ void Handle::backward(double* S_of_G, double* dE_dGamma) {
   ops::release(dG);
 }
 
+// Reverse-mode schedule (real path), built on first use: the fast schedule
+// reuses buffers, this one keeps every recorded value of a residual.
+CcsdReal* Handle::adjoint_schedule() {
+  if (complex_path || opt.method == CC4S_METHOD_DRCCD)
+    throw Error(ERR_UNSUPPORTED, "reverse mode is provided for Ccsd and Ccd on the real path");
+  if (!adj) {
+    RealOptions ro;
+    ro.ccd = opt.method == CC4S_METHOD_CCD;
+    ro.ppl = opt.ppl != 0;
+    ro.slab = opt.integrals_slice_size;
+    ro.adjoint = true;
+    adj.reset(new CcsdReal(sys, ro, stream));
+  }
+  return static_cast<CcsdReal*>(adj.get());
+}
+
+// Device vertex-block adjoints -> caller layout Gamma[G, p, q] (column-major,
+// interleaved complex when the input was complex; stacked Re/Im auxiliary rows
+// go to the two parts).  out is overwritten.
+void Handle::scatter_vertex_bar(const Schedule::VertexBar& vb, double* out) {
+  const int64_t o = shape.o, v = shape.v, G = sys.G, NG = in_NG, Np = in_Np;
+  const int64_t es = in_complex ? 2 : 1, parts = in_stacked ? 2 : 1;
+  std::memset(out, 0, sizeof(double) * NG * Np * Np * es);
+  struct Block { const double* d; int64_t row0, nx, col0, ny; };
+  const Block blocks[4] = {{vb.Gpp, o, v, o, v}, {vb.Gph, o, v, 0, o}, {vb.Ghh, 0, o, 0, o},
+                           {vb.Ghp, 0, o, o, v}};
+  std::vector<double> h;
+  for (const Block& b : blocks) {
+    if (!b.d) continue;
+    h.resize(G * b.nx * b.ny);
+    ops::d2h(h.data(), b.d, h.size(), stream);
+    ops::sync(stream);
+    for (int64_t part = 0; part < parts; ++part)
+      for (int64_t k = 0; k < NG; ++k)
+        for (int64_t x = 0; x < b.nx; ++x)
+          for (int64_t y = 0; y < b.ny; ++y)
+            out[(k + NG * ((b.row0 + x) + Np * (b.col0 + y))) * es + part] +=
+                h[((part * NG + k) * b.nx + x) * b.ny + y];
+  }
+}
+
+void Handle::residual_vjp(const double* T1, const double* T2, const double* R1b,
+                          const double* R2b, double* T1b, double* T2b, double* dGamma) {
+  require_inputs();
+  if (!T1 || !T2 || !R1b || !R2b) throw Error(ERR_INVALID_ARGUMENT, "null amplitudes or adjoint");
+  CcsdReal* adjs = adjoint_schedule();
+  const int64_t n = shape.total(), o = shape.o, v = shape.v, G = sys.G;
+  std::vector<double*> tmp;
+  auto dev = [&](int64_t k) { double* p = ops::alloc(k); tmp.push_back(p); return p; };
+  try {
+    double* Tin = dev(n);
+    double* Rb = dev(n);
+    double* Tb = dev(n);
+    upload_amplitudes(Tin, T1, T2, Rbuf);
+    upload_amplitudes(Rb, R1b, R2b, Rbuf);
+    adjs->prepare_vjp(Tin);
+    Schedule::VertexBar vb;
+    if (dGamma) {
+      vb.Gpp = dev(G * v * v); vb.Gph = dev(G * v * o); vb.Ghh = dev(G * o * o);
+      vb.Ghp = dev(G * o * v);
+      ops::zero(vb.Gpp, G * v * v, stream); ops::zero(vb.Gph, G * v * o, stream);
+      ops::zero(vb.Ghh, G * o * o, stream); ops::zero(vb.Ghp, G * o * v, stream);
+    }
+    adjs->vjp(Rb, Tb, dGamma ? &vb : nullptr, nullptr);
+    download_amplitudes(Tb, T1b, T2b, Rbuf);
+    if (dGamma) scatter_vertex_bar(vb, dGamma);
+  } catch (...) {
+    for (double* p : tmp) ops::release(p);
+    throw;
+  }
+  for (double* p : tmp) ops::release(p);
+}
+
+// Lambda equations (dR/dT + D)^T lambda = -dE/dT by the amplitude iteration's own
+// Jacobi update and mixer, then dE/dGamma = dE/dGamma|_T + lambda^T dR/dGamma.
+void Handle::relaxed_gradient(int max_iterations, double convergence, double* dE_dGamma,
+                              cc4s_cc_lambda_result* out) {
+  require_inputs();
+  if (!have_T) throw Error(ERR_STATE, "no amplitudes: run first");
+  if (max_iterations < 1) throw Error(ERR_INVALID_ARGUMENT, "maxIterations < 1");
+  std::memset(out, 0, sizeof(*out));
+  CcsdReal* adjs = adjoint_schedule();
+  const int64_t n = shape.total(), o = shape.o, v = shape.v, G = sys.G, n1 = shape.n1();
+  std::vector<double*> tmp;
+  auto dev = [&](int64_t k) { double* p = ops::alloc(k); tmp.push_back(p); return p; };
+  try {
+    double* lam = dev(n);
+    double* g = dev(n);
+    double* Jt = dev(n);
+    double* VdB = dev(n1 * n1);
+    ops::event_record(ev0, stream);
+    adjs->prepare_vjp(Tcur);
+    adjs->energy_gradients(Tcur, g, VdB);
+    ops::event_record(ev1, stream);
+    out->prepare_seconds = 1e-3 * ops::event_ms(ev0, ev1);
+    reset_mixer();
+    ops::zero(lam, n, stream);
+    const bool diis = opt.mixer == CC4S_MIXER_DIIS;
+    double host[8];
+    int it = 0;
+    for (; it < max_iterations; ++it) {
+      ops::event_record(ev0, stream);
+      if (it == 0) {
+        ops::d2d(Rbuf, g, n, stream);
+      } else {
+        adjs->vjp(lam, Jt, nullptr, nullptr);
+        ops::axpby(Rbuf, 1.0, g, 1.0, Jt, 0.0, n, stream);
+      }
+      const int slot = diis ? next_index : 0;
+      if (diis)
+        ops::jacobi_packed(A[slot], Rs[slot], Rbuf, it ? lam : nullptr, sys.eh, sys.ep,
+                           shape, opt.level_shift, stream);
+      else
+        ops::jacobi(A[slot], Rs[slot], Rbuf, it ? lam : nullptr, sys.eh, sys.ep, shape,
+                    opt.level_shift, stream);
+      mix(A[slot], Rs[slot], scal + 4, lam);
+      ops::event_record(ev1, stream);
+      ops::d2h(host, scal + 4, 1, stream);
+      double st = 0.0;
+      if (diis) ops::d2h(&st, reinterpret_cast<double*>(status_dev), 1, stream);
+      ops::sync(stream);
+      int status_int;
+      std::memcpy(&status_int, &st, sizeof(int));
+      if (diis && status_int != 0)
+        throw Error(ERR_DIIS_SINGULAR, "Diagonalization failed (singular DIIS system, Lambda)");
+      const double norm = std::sqrt(host[0]);
+      if (!std::isfinite(norm)) throw Error(ERR_NON_FINITE, "non-finite Lambda update");
+      const double sec = 1e-3 * ops::event_ms(ev0, ev1);
+      if (it > 0) out->vjp_seconds = sec;
+      out->residuum_norm = norm;
+      if (norm < convergence) { ++it; out->converged = 1; break; }
+    }
+    out->iterations = it;
+    Schedule::VertexBar vb;
+    vb.Gpp = dev(G * v * v); vb.Gph = dev(G * v * o); vb.Ghh = dev(G * o * o);
+    vb.Ghp = dev(G * o * v);
+    ops::zero(vb.Gpp, G * v * v, stream); ops::zero(vb.Gph, G * v * o, stream);
+    ops::zero(vb.Ghh, G * o * o, stream); ops::zero(vb.Ghp, G * o * v, stream);
+    ops::event_record(ev0, stream);
+    adjs->vjp(lam, Jt, &vb, VdB);
+    ops::event_record(ev1, stream);
+    out->gradient_seconds = 1e-3 * ops::event_ms(ev0, ev1);
+    if (dE_dGamma) scatter_vertex_bar(vb, dE_dGamma);
+  } catch (...) {
+    for (double* p : tmp) ops::release(p);
+    throw;
+  }
+  for (double* p : tmp) ops::release(p);
+}
+
 }  // namespace cc4s_b200
 
 // ---------------------------------------------------------------------------
@@ -361,6 +511,25 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
 int cc4s_cc_backward(cc4s_cc_handle* h, double* S_of_G, double* dE_dGamma) {
   if (!h || !h->impl) return CC4S_ERR_INVALID_ARGUMENT;
   return guarded(h, [&] { h->impl->backward(S_of_G, dE_dGamma); return 0; });
+}
+
+int cc4s_cc_residual_vjp(cc4s_cc_handle* h, const double* T1, const double* T2,
+                         const double* R1bar, const double* R2bar, double* T1bar, double* T2bar,
+                         double* dGamma) {
+  if (!h || !h->impl || !T1bar || !T2bar) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] {
+    h->impl->residual_vjp(T1, T2, R1bar, R2bar, T1bar, T2bar, dGamma);
+    return 0;
+  });
+}
+
+int cc4s_cc_relaxed_gradient(cc4s_cc_handle* h, int max_iterations, double convergence,
+                             double* dE_dGamma, cc4s_cc_lambda_result* out) {
+  if (!h || !h->impl || !out) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] {
+    h->impl->relaxed_gradient(max_iterations, convergence, dE_dGamma, out);
+    return out->converged ? 0 : static_cast<int>(CC4S_WARN_NOT_CONVERGED);
+  });
 }
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {

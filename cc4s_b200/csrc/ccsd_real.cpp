@@ -47,12 +47,20 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
     Vd_ = take(D2);
     Vhhhh_ = take(o * o * o * o); Vhhhp_ = take(o * o * o * v); Vh2_ = take(o * o * o * v);
     Xd_ = take(D2); Y_ = take(D2); EX_ = take(D2);
-    W8_ = EX_;
+    // Roles that share EX, Y and dGph on the fast path get their own buffers in
+    // adjoint mode, where every recorded value must survive the residual.
+    adjoint_ = opt.adjoint;
+    Vt_ = EX2_ = W8r_ = W8s_ = EX_;
+    Yx_ = Y_;
+    if (adjoint_) {
+      Vt_ = take(D2); EX2_ = take(D2); W8r_ = take(D2); W8s_ = take(D2); Yx_ = take(D2);
+    }
     Kki_ = take(o * o); Kac_ = take(v * v); Lac_ = take(v * v); Lki_ = take(o * o);
     jG_ = take(G);
     U_ = take(G * n1); dGph_ = take(G * n1); W_ = take(G * n1); Z_ = take(G * n1);
     W1_ = take(G * n1); F_ = take(G * n1);
     dGpp_ = take(G * v * v); dGhh_ = take(G * o * o);
+    A2_ = adjoint_ ? take(G * n1) : dGph_;
     Q_ = take(n1 * o * o); Xkl1_ = take(o * o * o * o); Xkl2_ = take(o * o * o * o);
     kck_ = take(n1); P1_ = take(o * o); P_ = take(G * o * v);
     // Ladder slabs: blocks of s virtual orbitals (s^2 rows of the contraction,
@@ -76,7 +84,11 @@ CcsdReal::CcsdReal(const RealSystem& sys, const RealOptions& opt, Stream s)
     throw;
   }
   count_flops_ = false;
+  taping_ = adjoint_;
   build_integrals();
+  taping_ = false;
+  integrals_tape_.swap(tape_);
+  tape_.clear();
   count_flops_ = true;
 }
 
@@ -110,8 +122,8 @@ void CcsdReal::build_integrals() {
     const int64_t dh[4] = {o, o, o, v};
     const int pa[4] = {2, 0, 3, 1};
     const int pb[4] = {2, 1, 3, 0};
-    ops::permute4(Vh2_, Vhhhp_, dh, pa, 2.0, 0.0, s_);
-    ops::permute4(Vh2_, Vhhhp_, dh, pb, -1.0, 1.0, s_);
+    perm_(Vh2_, Vhhhp_, dh, pa, 2.0, 0.0);
+    perm_(Vh2_, Vhhhp_, dh, pb, -1.0, 1.0);
   }
 }
 
@@ -137,16 +149,16 @@ void CcsdReal::residual(const double* T, double* R) {
   const int64_t sA = o * n1, sI = n1, sB = o;
 
   // ---- X = T2 + T1 T1 (Ccsd.cxx:169-170) -----------------------------------
-  if (ccd) ops::d2d(Xd_, Td, D2, s_);
-  else ops::rank1(Xd_, 1.0, Td, 1.0, t, n1, s_);
+  if (ccd) copy_(Xd_, Td, D2);
+  else rank1_(Xd_, 1.0, Td, 1.0, t, n1);
 
   // ---- Kki, Kac (Ccsd.cxx:172-178) -------------------------------------------
   // EX <- Vt[(c,k),(d,l)] = 2 V_cdkl - V_cdlk  (= 2 V_cdkl - V_dckl)
-  ops::permute4(EX_, Vd_, d4, p_ex, -1.0, 0.0, s_);
-  ops::axpby(EX_, 2.0, Vd_, 1.0, EX_, 0.0, D2, s_);
+  perm_(Vt_, Vd_, d4, p_ex, -1.0, 0.0);
+  axpby_(Vt_, 2.0, Vd_, 1.0, Vt_, 0.0, D2);
   {  // Kki[k][i] = sum_{c,(d,l)} Vt[(c,k),(d,l)] X[(c,i),(d,l)]
     Contraction c; c.M = o; c.N = o; c.K = v * n1; c.Ki = n1;
-    c.A = vw(EX_, 0, sI, sA, 1);
+    c.A = vw(Vt_, 0, sI, sA, 1);
     c.B = vw(Xd_, sA, 1, 0, sI);
     c.C = rm(Kki_, o);
     gemm_(c);
@@ -154,13 +166,13 @@ void CcsdReal::residual(const double* T, double* R) {
   {  // Kac[a][c] = -sum_{k,(d,l)} X[(a,k),(d,l)] Vt[(c,k),(d,l)]
     Contraction c; c.M = v; c.N = v; c.K = o * n1; c.Ki = n1;
     c.A = vw(Xd_, 0, sA, sI, 1);
-    c.B = vw(EX_, sI, 1, 0, sA);
+    c.B = vw(Vt_, sI, 1, 0, sA);
     c.C = rm(Kac_, v);
     c.alpha = -1.0;
     gemm_(c);
   }
   // ---- Lac (Ccsd.cxx:180-189) --------------------------------------------------
-  ops::d2d(Lac_, Kac_, v * v, s_);
+  copy_(Lac_, Kac_, v * v);
   if (!ccd) {
     {  // jG[G] = sum_{dk} Gph[G][dk] t[dk]
       Contraction c; c.M = G; c.N = 1; c.K = n1;
@@ -190,7 +202,7 @@ void CcsdReal::residual(const double* T, double* R) {
     }
   }
   // ---- Lki (Ccsd.cxx:175,192-193) --------------------------------------------
-  ops::d2d(Lki_, Kki_, o * o, s_);
+  copy_(Lki_, Kki_, o * o);
   if (!ccd) {  // Lki[k][i] += sum_{c,l} (2 V_klic - V_lkic) t[c][l]
     Contraction c; c.M = o * o; c.N = 1; c.K = v * o; c.Mi = o; c.Ki = o;
     c.A = vw(Vh2_, v * o * o, v * o, o, 1);   // Vh2[i][k][c][l]: m = (i,k), k = (c,l)
@@ -212,7 +224,7 @@ void CcsdReal::residual(const double* T, double* R) {
     gemm_(c);
   }
   // ---- T1-dressed vertex terms (Ccsd.cxx:201-210) ----------------------------
-  ops::d2d(dGph_, Gph, G * n1, s_);
+  copy_(dGph_, Gph, G * n1);
   if (!ccd) {
     {  // dGph[G][a][i] -= sum_k t[a][k] Ghh[G][k][i]
       Contraction c; c.M = v; c.N = o; c.K = o; c.batch = G;
@@ -251,24 +263,26 @@ void CcsdReal::residual(const double* T, double* R) {
     }
   }
   // ---- ring Xakic (Ccsd.cxx:215-229) -------------------------------------------
-  if (ccd) ops::d2d(W8_, Td, D2, s_);
-  else ops::rank1(W8_, 1.0, Td, 2.0, t, n1, s_);                 // X' = T2 + 2 T1 T1
-  ops::permute4(Y_, W8_, d4, p_ex, 1.0, 0.0, s_);                 // X'^x
-  ops::axpby(W8_, 1.0, Td, -0.5, Y_, 0.0, D2, s_);               // M1 = T - X'^x / 2
-  ops::permute4(Y_, Td, d4, p_ex, -1.0, 0.0, s_);                 // -T^x
-  ops::axpby(Y_, 2.0, Td, 1.0, Y_, 0.0, D2, s_);                 // Y = 2T - T^x
+  if (ccd) copy_(W8r_, Td, D2);
+  else rank1_(W8r_, 1.0, Td, 2.0, t, n1);                        // X' = T2 + 2 T1 T1
+  perm_(Yx_, W8r_, d4, p_ex, 1.0, 0.0);                          // X'^x
+  axpby_(W8r_, 1.0, Td, -0.5, Yx_, 0.0, D2);                     // M1 = T - X'^x / 2
+  perm_(Y_, Td, d4, p_ex, -1.0, 0.0);                            // -T^x
+  axpby_(Y_, 2.0, Td, 1.0, Y_, 0.0, D2);                         // Y = 2T - T^x
   {  // Z = Gph M1
     Contraction c; c.M = G; c.N = n1; c.K = n1;
-    c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(Z_, n1);
+    c.A = rm(Gph, n1); c.B = rm(W8r_, n1); c.C = rm(Z_, n1);
     tc_(c);
   }
-  if (!ccd) {  // dGph[G][a][i] += sum_d Gpp[G][a][d] t[d][i]
+  // A2 = dGph + Gpp t + Z (in place in dGph on the fast path)
+  if (A2_ != dGph_) copy_(A2_, dGph_, G * n1);
+  if (!ccd) {  // A2[G][a][i] += sum_d Gpp[G][a][d] t[d][i]
     Contraction c; c.M = v; c.N = o; c.K = v; c.batch = G;
-    c.A = with_batch(rm(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(dGph_, o), n1);
+    c.A = with_batch(rm(Gpp, v), v * v); c.B = rm(t, o); c.C = with_batch(rm(A2_, o), n1);
     c.beta = 1.0;
     gemm_(c);
   }
-  ops::axpby(dGph_, 1.0, dGph_, 1.0, Z_, 0.0, G * n1, s_);       // A2 = dGph + Z
+  axpby_(A2_, 1.0, A2_, 1.0, Z_, 0.0, G * n1);
   {  // W1 = Gph Y
     Contraction c; c.M = G; c.N = n1; c.K = n1;
     c.A = rm(Gph, n1); c.B = rm(Y_, n1); c.C = rm(W1_, n1);
@@ -276,7 +290,7 @@ void CcsdReal::residual(const double* T, double* R) {
   }
   {  // R2 += A2^T W1
     Contraction c; c.M = n1; c.N = n1; c.K = G;
-    c.A = tr(dGph_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
+    c.A = tr(A2_, n1); c.B = rm(W1_, n1); c.C = rm(R2, n1); c.beta = 1.0;
     tc_(c);
   }
   {  // EX[(a,i),(c,k)] = -1/2 sum_{(b,j)} T[(a,i),(b,j)] V_bckj,  V_bckj = Vd[(b,k),(c,j)]
@@ -293,8 +307,8 @@ void CcsdReal::residual(const double* T, double* R) {
     tc_(c);
   }
   // ---- crossed ring Xakci (Ccsd.cxx:233-253) ------------------------------------
-  ops::d2d(dGpp_, Gpp, G * v * v, s_);
-  ops::d2d(dGhh_, Ghh, G * o * o, s_);
+  copy_(dGpp_, Gpp, G * v * v);
+  copy_(dGhh_, Ghh, G * o * o);
   if (!ccd) {
     {  // dGpp[G][a][c] -= sum_l t[a][l] Gph[G][c][l]
       Contraction c; c.M = v; c.N = v; c.K = o; c.batch = G;
@@ -313,7 +327,7 @@ void CcsdReal::residual(const double* T, double* R) {
     Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ki = o; c.Ni = o;
     c.A = vw(Td, sA, 1, sB, sI);
     c.B = vw(Vd_, sA, 1, sB, sI);
-    c.C = vw(EX_, sA, sI, o, 1);
+    c.C = vw(EX2_, sA, sI, o, 1);
     c.alpha = -0.5;
     tc_(c);
   }
@@ -321,29 +335,29 @@ void CcsdReal::residual(const double* T, double* R) {
     Contraction c; c.M = v * v; c.N = o * o; c.K = G; c.Mi = v; c.Ni = o;
     c.A = vw(dGpp_, v, 1, 0, v * v);
     c.B = vw(dGhh_, 0, o * o, o, 1);
-    c.C = vw(EX_, o * n1, o, 1, n1);
+    c.C = vw(EX2_, o * n1, o, 1, n1);
     c.beta = 1.0;
     tc_(c);
   }
   {  // R2 -= EX T
     Contraction c; c.M = n1; c.N = n1; c.K = n1;
-    c.A = rm(EX_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1);
+    c.A = rm(EX2_, n1); c.B = rm(Td, n1); c.C = rm(R2, n1);
     c.alpha = -1.0; c.beta = 1.0;
     tc_(c);
   }
   {  // R2_abij -= sum_ck T_ackj X_bkci : exchange pairing m = (a,j), n = (b,i)
     Contraction c; c.M = n1; c.N = n1; c.K = n1; c.Mi = o; c.Ni = o; c.Ki = o;
     c.A = vw(Td, sA, 1, sB, sI);           // T_ackj = T[(a,k),(c,j)]
-    c.B = vw(EX_, sB, 1, sA, sI);          // X_bkci = EX[(b,i),(c,k)]
+    c.B = vw(EX2_, sB, 1, sA, sI);          // X_bkci = EX[(b,i),(c,k)]
     c.C = vw(R2, sA, 1, sB, sI);
     c.alpha = -1.0; c.beta = 1.0;
     tc_(c);
   }
   // ---- P(ab,ij) symmetrisation and +V (Ccsd.cxx:256,263) ----------------------
-  ops::symmetrize(R2, n1, s_);
-  ops::axpby(R2, 1.0, R2, 1.0, Vd_, 0.0, D2, s_);
+  sym_(R2, n1);
+  axpby_(R2, 1.0, R2, 1.0, Vd_, 0.0, D2);
   // ---- hole-hole ladder (Ccsd.cxx:267-281) --------------------------------------
-  ops::d2d(Xkl1_, Vhhhh_, o * o * o * o, s_);
+  copy_(Xkl1_, Vhhhh_, o * o * o * o);
   if (!ccd) {
     {  // Xkl1[k][l][i][j] += sum_c Vhhhp[k][l][i][c] t[c][j]
       Contraction c; c.M = o * o * o; c.N = o; c.K = v;
@@ -380,7 +394,7 @@ void CcsdReal::residual(const double* T, double* R) {
   // ---- particle-particle ladder (Ccsd.cxx:283-333) ------------------------------
   if (opt_.ppl) ppl(Xd_, R2, dGpp_);
   if (ccd) {
-    ops::zero(R1, n1, s_);
+    zero_(R1, n1);
     profile_finish();
     return;
   }
@@ -437,10 +451,10 @@ void CcsdReal::residual(const double* T, double* R) {
     gemm_(d);
   }
   {  // F = Gph (2X - X^x);  R1[a][i] += sum_{G,x} Gpp[G][x][a] F[G][x][i]
-    ops::permute4(W8_, Xd_, d4, p_ex, 1.0, 0.0, s_);
-    ops::axpby(W8_, 2.0, Xd_, -1.0, W8_, 0.0, D2, s_);
+    perm_(W8s_, Xd_, d4, p_ex, 1.0, 0.0);
+    axpby_(W8s_, 2.0, Xd_, -1.0, W8s_, 0.0, D2);
     Contraction c; c.M = G; c.N = n1; c.K = n1;
-    c.A = rm(Gph, n1); c.B = rm(W8_, n1); c.C = rm(F_, n1);
+    c.A = rm(Gph, n1); c.B = rm(W8s_, n1); c.C = rm(F_, n1);
     tc_(c);
     Contraction d; d.M = v; d.N = o; d.K = G * v; d.Ki = v;
     d.A = vw(Gpp, 0, 1, v * v, v);
@@ -477,13 +491,12 @@ void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
       for (int64_t Yb = 0; Yb <= X; ++Yb) {
         const int64_t x0 = X * s, sx = std::min(s, v - x0);
         const int64_t y0 = Yb * s, sy = std::min(s, v - y0);
-        {  // m = (x, c'), n = (y, d), slab[x][y][c'][d]
-          Contraction c; c.M = sx * nc; c.N = sy * v; c.K = G; c.Mi = nc; c.Ni = v;
-          c.A = vw(cp(dGpp) + x0 * v + c0, v, 1, 0, v * v);
-          c.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
-          c.C = vw(slab_, sy * nc * v, v, nc * v, 1);
-          tc_(c);
-        }
+        Contraction build;  // m = (x, c'), n = (y, d), slab[x][y][c'][d]
+        build.M = sx * nc; build.N = sy * v; build.K = G; build.Mi = nc; build.Ni = v;
+        build.A = vw(cp(dGpp) + x0 * v + c0, v, 1, 0, v * v);
+        build.B = vw(cp(dGpp) + y0 * v, 0, v * v, v, 1);
+        build.C = vw(slab_, sy * nc * v, v, nc * v, 1);
+        tc_(build);
         {  // m = (x, y), k = (c', d), n = (i, j)
           Contraction c; c.M = sx * sy; c.N = o * o; c.K = nc * v; c.Mi = sy; c.Ki = v; c.Ni = o;
           c.A = vw(slab_, sy * nc * v, nc * v, v, 1);
@@ -492,10 +505,94 @@ void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
           if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
           c.beta = 1.0;
           tc_(c);
+          if (taping_) {  // the slab is rebuilt before this contraction's adjoint
+            tape_.back().recompute = true;
+            tape_.back().pre = build;
+            tape_.back().zero_p = slab_;
+            tape_.back().zero_n = slab_rows_ * slab_rows_ * slab_cols_ * v;
+          }
         }
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Reverse mode: the residual at T recorded once, replayed backwards per vjp.
+void CcsdReal::energy_gradients(const double* T, double* g, double* Vd_bar) {
+  const int64_t o = sys_.o, v = sys_.v, n1 = v * o, D2 = n1 * n1;
+  const int64_t d4[4] = {v, o, v, o};
+  const int p_ex[4] = {0, 3, 2, 1};
+  double* g2 = g + n1;
+  ops::permute4(g2, Vd_, d4, p_ex, -1.0, 0.0, s_);       // dE/dT2 = 2 Vd - Vd^x
+  ops::axpby(g2, 2.0, Vd_, 1.0, g2, 0.0, D2, s_);
+  Contraction c; c.M = n1; c.N = 1; c.K = n1;           // dE/dT1 = 2 (dE/dT2) T1
+  c.A = rm(g2, n1); c.B = vw(cp(T), 0, 1, 0, 0); c.C = vw(g, 0, 1, 0, 0); c.alpha = 2.0;
+  gemm(c, s_, scratch_);
+  if (Vd_bar) {  // dE/dVd = 2 X - X^x, X staged in the forward output buffer (never
+                 // read by the reverse sweep)
+    if (!Rf_) Rf_ = take(n1 + D2);
+    double* X = Rf_ + n1;
+    ops::rank1(X, 1.0, T + n1, 1.0, T, n1, s_);
+    ops::permute4(Vd_bar, X, d4, p_ex, -1.0, 0.0, s_);
+    ops::axpby(Vd_bar, 2.0, X, 1.0, Vd_bar, 0.0, D2, s_);
+  }
+}
+
+void CcsdReal::prepare_vjp(const double* T) {
+  if (!adjoint_) throw Error(ERR_STATE, "reverse mode needs a schedule built in adjoint mode");
+  if (!T) throw Error(ERR_INVALID_ARGUMENT, "prepare_vjp: no amplitudes");
+  const int64_t n1 = sys_.v * sys_.o;
+  if (!Rf_) Rf_ = take(n1 + n1 * n1);
+  tape_.clear();
+  taping_ = true;
+  try {
+    residual(T, Rf_);
+  } catch (...) {
+    taping_ = false;
+    throw;
+  }
+  taping_ = false;
+  Tprep_ = T;
+}
+
+void CcsdReal::vjp(const double* Rbar, double* Tbar, const VertexBar* gbar,
+                   const double* extra_Vd_bar) {
+  if (!Tprep_) throw Error(ERR_STATE, "vjp before prepare_vjp");
+  const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o, n = n1 + n1 * n1;
+  while (bar_bufs_.size() < owned_.size()) {
+    const size_t k = bar_bufs_.size();
+    bar_bufs_.push_back(owned_[k] == scratch_.p ? nullptr : ops::alloc(owned_n_[k]));
+  }
+  regions_.clear();
+  for (size_t k = 0; k < owned_.size(); ++k) {
+    if (!bar_bufs_[k]) continue;
+    ops::zero(bar_bufs_[k], owned_n_[k], s_);
+    regions_.push_back({owned_[k], static_cast<int64_t>(owned_n_[k]), bar_bufs_[k]});
+  }
+  ops::zero(Tbar, n, s_);
+  regions_.push_back({Tprep_, n, Tbar});
+  if (gbar) {
+    if (gbar->Gpp) regions_.push_back({sys_.Gpp, G * v * v, gbar->Gpp});
+    if (gbar->Gph) regions_.push_back({sys_.Gph, G * n1, gbar->Gph});
+    if (gbar->Ghh) regions_.push_back({sys_.Ghh, G * o * o, gbar->Ghh});
+    if (gbar->Ghp) regions_.push_back({sys_.Ghp, G * n1, gbar->Ghp});
+  }
+  ops::d2d(bar_of(Rf_), Rbar, n, s_);
+  try {
+    reverse(tape_);
+    // the amplitudes are symmetric, T_abij = T_baji: project the T2 adjoint
+    ops::symmetrize(Tbar + n1, n1, s_);
+    ops::axpby(Tbar + n1, 0.5, Tbar + n1, 0.0, nullptr, 0.0, n1 * n1, s_);
+    if (gbar) {
+      if (extra_Vd_bar) ops::axpby(bar_of(Vd_), 1.0, bar_of(Vd_), 1.0, extra_Vd_bar, 0.0, n1 * n1, s_);
+      reverse(integrals_tape_);
+    }
+  } catch (...) {
+    regions_.clear();
+    throw;
+  }
+  regions_.clear();
 }
 
 }  // namespace cc4s_b200

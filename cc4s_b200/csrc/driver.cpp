@@ -46,6 +46,7 @@ double* Handle::take(size_t elems) {
 }
 
 void Handle::free_state() {
+  adj.reset();
   solver.reset();
   for (double* p : state) ops::release(p);
   state.clear();

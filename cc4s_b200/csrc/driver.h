@@ -35,7 +35,14 @@ struct Handle {
   // amplitude vector, through a full-size device staging vector st (not dst/src).
   void upload_amplitudes(double* dst, const double* T1, const double* T2, double* st);
   void download_amplitudes(const double* src, double* T1, double* T2, double* st);
-  void mix(double* A_new, double* dT_new, double* norm2_dev);
+  void mix(double* A_new, double* dT_new, double* norm2_dev, double* out);
+  // reverse mode (real path)
+  CcsdReal* adjoint_schedule();
+  void scatter_vertex_bar(const Schedule::VertexBar& vb, double* out);
+  void residual_vjp(const double* T1, const double* T2, const double* R1b, const double* R2b,
+                    double* T1b, double* T2b, double* dGamma);
+  void relaxed_gradient(int max_iterations, double convergence, double* dE_dGamma,
+                        cc4s_cc_lambda_result* out);
 
   cc4s_cc_options opt;
   Stream stream = nullptr;
@@ -50,6 +57,7 @@ struct Handle {
   std::vector<double*> vertex;  // device inputs (vertex slices, energies)
   std::vector<double*> state;   // amplitudes, DIIS history, scalars
   std::unique_ptr<Schedule> solver;
+  std::unique_ptr<Schedule> adj;  // reverse-mode schedule, built on first use
 
   double* Tcur = nullptr;   // current amplitudes (mixer output)
   double* Rbuf = nullptr;   // residual

@@ -19,16 +19,26 @@ void Schedule::release_all() {
   split_ = SplitScratch();
   for (double* p : owned_) ops::release(p);
   owned_.clear();
+  owned_n_.clear();
+  for (double* p : bar_bufs_) ops::release(p);
+  bar_bufs_.clear();
 }
 
 double* Schedule::take(size_t elems) {
   double* p = ops::alloc(elems);
   owned_.push_back(p);
+  owned_n_.push_back(elems);
   bytes_ += elems * sizeof(double);
   return p;
 }
 
 void Schedule::gemm_(const Contraction& c) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::GEMM;
+    op.c = c;
+    tape_.push_back(op);
+  }
   const double f = 2.0 * double(c.M) * double(c.N) * double(c.K) * double(c.batch);
   if (count_flops_) flops_ += f;
   if (profile_ && count_flops_) {
@@ -46,7 +56,7 @@ void Schedule::gemm_(const Contraction& c) {
 }
 
 void Schedule::tc_(const Contraction& c) {
-  if (precision_ == 0 || c.batch != 1 || c.K < 64 || c.M < 64 || c.N < 64) {
+  if (precision_ == 0 || taping_ || c.batch != 1 || c.K < 64 || c.M < 64 || c.N < 64) {
     gemm_(c);
     return;
   }
@@ -208,6 +218,237 @@ void Schedule::profile_finish() {
   ev_flops_.clear();
   ev_shape_.clear();
   prof_ = p;
+}
+
+
+// ---------------------------------------------------------------------------
+// Reverse mode.
+
+void Schedule::perm_(double* dst, const double* src, const int64_t d[4], const int p[4],
+                     double alpha, double beta) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::PERM;
+    op.dst = dst; op.x = src; op.a = alpha; op.b = beta;
+    for (int k = 0; k < 4; ++k) { op.d[k] = d[k]; op.perm[k] = p[k]; }
+    tape_.push_back(op);
+  }
+  ops::permute4(dst, src, d, p, alpha, beta, s_);
+}
+
+void Schedule::axpby_(double* out, double a, const double* x, double b, const double* y,
+                      double c, int64_t n) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::AXPBY;
+    op.dst = out; op.x = x; op.y = y; op.a = a; op.b = b; op.cc = c; op.n = n;
+    tape_.push_back(op);
+  }
+  ops::axpby(out, a, x, b, y, c, n, s_);
+}
+
+void Schedule::rank1_(double* out, double a, const double* A, double b, const double* t,
+                      int64_t n) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::RANK1;
+    op.dst = out; op.x = A; op.y = t; op.a = a; op.b = b; op.n = n;
+    tape_.push_back(op);
+  }
+  ops::rank1(out, a, A, b, t, n, s_);
+}
+
+void Schedule::sym_(double* R, int64_t n) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::SYMM;
+    op.dst = R; op.n = n;
+    tape_.push_back(op);
+  }
+  ops::symmetrize(R, n, s_);
+}
+
+void Schedule::copy_(double* dst, const double* src, int64_t n) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::COPY;
+    op.dst = dst; op.x = src; op.n = n;
+    tape_.push_back(op);
+  }
+  ops::d2d(dst, src, n, s_);
+}
+
+void Schedule::zero_(double* p, int64_t n) {
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::ZERO;
+    op.dst = p; op.n = n;
+    tape_.push_back(op);
+  }
+  ops::zero(p, n, s_);
+}
+
+double* Schedule::bar_of(const double* p) const {
+  if (!p) return nullptr;
+  for (const Region& r : regions_)
+    if (p >= r.p && p < r.p + r.n) return r.bar ? r.bar + (p - r.p) : nullptr;
+  return nullptr;
+}
+
+View Schedule::barv(const View& v) const {
+  View w = v;
+  w.p = bar_of(v.p);
+  return w;
+}
+
+namespace {
+View transposed(const View& v) {
+  View t = v;
+  std::swap(t.s_ro, t.s_co);
+  std::swap(t.s_ri, t.s_ci);
+  return t;
+}
+}  // namespace
+
+// Adjoint of C (and C2) = alpha A B + beta C:  Abar += alpha Cbar B^T,
+// Bbar += alpha A^T Cbar.  An adjoint output that every batch entry shares
+// (batch strides zero) is summed over the batch by folding the batch index into
+// the contraction index, or launch by launch where that is not expressible.
+void Schedule::reverse_gemm(const Contraction& c) {
+  if (c.M <= 0 || c.N <= 0 || c.K <= 0 || c.batch <= 0) return;
+  if (c.beta != 0.0 && c.beta != 1.0)
+    throw Error(ERR_UNSUPPORTED, "reverse mode: contraction with beta other than 0 or 1");
+  auto run = [&](Contraction d) {
+    const bool shared = d.batch > 1 && d.C.s_bo == 0 && d.C.s_bi == 0;
+    if (!shared) { gemm(d, s_, scratch_); return; }
+    if (d.Ki == 0 && d.Bi == 0 && d.A.s_bo == 0 && d.B.s_bo == 0) {
+      // sum over the batch as part of the contraction: k' = (b, k)
+      Contraction e = d;
+      e.K = d.K * d.batch; e.Ki = d.K; e.batch = 1;
+      e.A.s_co = d.A.s_bi; e.B.s_ro = d.B.s_bi;
+      e.A.s_bi = e.B.s_bi = e.C.s_bi = 0;
+      gemm(e, s_, scratch_);
+      return;
+    }
+    const int64_t Bi = d.Bi > 0 ? d.Bi : d.batch;
+    for (int64_t b = 0; b < d.batch; ++b) {
+      Contraction e = d;
+      e.batch = 1; e.Bi = 0;
+      const int64_t bo = b / Bi, bi = b % Bi;
+      e.A.p += bo * d.A.s_bo + bi * d.A.s_bi;
+      e.B.p += bo * d.B.s_bo + bi * d.B.s_bi;
+      e.A.s_bo = e.A.s_bi = e.B.s_bo = e.B.s_bi = e.C.s_bo = e.C.s_bi = 0;
+      gemm(e, s_, scratch_);
+    }
+  };
+  const bool hasA = bar_of(c.A.p) != nullptr, hasB = bar_of(c.B.p) != nullptr;
+  const View outs[2] = {c.C, c.C2};
+  for (int w = 0; w < 2; ++w) {
+    const View& O = outs[w];
+    if (!O.p || !bar_of(O.p)) continue;
+    if (hasA) {
+      Contraction d;
+      d.M = c.M; d.N = c.K; d.K = c.N; d.batch = c.batch;
+      d.Mi = c.Mi; d.Ni = c.Ki; d.Ki = c.Ni; d.Bi = c.Bi;
+      d.A = barv(O); d.B = transposed(c.B); d.C = barv(c.A);
+      d.alpha = c.alpha; d.beta = 1.0;
+      run(d);
+    }
+    if (hasB) {
+      Contraction d;
+      d.M = c.K; d.N = c.N; d.K = c.M; d.batch = c.batch;
+      d.Mi = c.Ki; d.Ni = c.Ni; d.Ki = c.Mi; d.Bi = c.Bi;
+      d.A = transposed(c.A); d.B = barv(O); d.C = barv(c.B);
+      d.alpha = c.alpha; d.beta = 1.0;
+      run(d);
+    }
+  }
+}
+
+void Schedule::reverse(const std::vector<TapeOp>& tape) {
+  for (size_t k = tape.size(); k-- > 0;) {
+    const TapeOp& op = tape[k];
+    switch (op.kind) {
+      case TapeOp::GEMM: {
+        if (op.recompute) {
+          gemm(op.pre, s_, scratch_);
+          if (double* zb = bar_of(op.zero_p)) ops::zero(zb, op.zero_n, s_);
+        }
+        reverse_gemm(op.c);
+        break;
+      }
+      case TapeOp::PERM: {  // dst = a P(src) + b dst
+        double* db = bar_of(op.dst);
+        if (!db) break;
+        int64_t e[4];
+        int inv[4];
+        for (int q = 0; q < 4; ++q) e[q] = op.d[op.perm[q]];
+        for (int q = 0; q < 4; ++q) inv[op.perm[q]] = q;
+        if (double* sb = bar_of(op.x)) ops::permute4(sb, db, e, inv, op.a, 1.0, s_);
+        const int64_t n = e[0] * e[1] * e[2] * e[3];
+        if (op.b == 0.0) ops::zero(db, n, s_);
+        else if (op.b != 1.0) ops::axpby(db, op.b, db, 0.0, nullptr, 0.0, n, s_);
+        break;
+      }
+      case TapeOp::AXPBY: {  // out = a x + b y + c out
+        double* ob = bar_of(op.dst);
+        if (!ob) break;
+        double keep = op.cc;
+        if (op.x == op.dst) keep += op.a;
+        else if (double* xb = bar_of(op.x)) ops::axpby(xb, 1.0, xb, op.a, ob, 0.0, op.n, s_);
+        if (op.y) {
+          if (op.y == op.dst) keep += op.b;
+          else if (double* yb = bar_of(op.y)) ops::axpby(yb, 1.0, yb, op.b, ob, 0.0, op.n, s_);
+        }
+        if (keep == 0.0) ops::zero(ob, op.n, s_);
+        else if (keep != 1.0) ops::axpby(ob, keep, ob, 0.0, nullptr, 0.0, op.n, s_);
+        break;
+      }
+      case TapeOp::RANK1: {  // out = a A + b t t^T  (n x n)
+        double* ob = bar_of(op.dst);
+        if (!ob) break;
+        const int64_t n = op.n;
+        if (double* tb = bar_of(op.y)) {  // tbar += b (obar + obar^T) t
+          Contraction g; g.M = n; g.N = 1; g.K = n;
+          g.A = rm(ob, n); g.B = vw(cp(op.y), 0, 1, 0, 0); g.C = vw(tb, 0, 1, 0, 0);
+          g.alpha = op.b; g.beta = 1.0;
+          gemm(g, s_, scratch_);
+          g.A = tr(ob, n);
+          gemm(g, s_, scratch_);
+        }
+        if (op.x == op.dst) {
+          if (op.a != 1.0) ops::axpby(ob, op.a, ob, 0.0, nullptr, 0.0, n * n, s_);
+        } else {
+          if (double* ab = bar_of(op.x)) ops::axpby(ab, 1.0, ab, op.a, ob, 0.0, n * n, s_);
+          ops::zero(ob, n * n, s_);
+        }
+        break;
+      }
+      case TapeOp::SYMM: {
+        if (double* rb = bar_of(op.dst)) ops::symmetrize(rb, op.n, s_);
+        break;
+      }
+      case TapeOp::COPY: {
+        double* db = bar_of(op.dst);
+        if (!db) break;
+        if (double* sb = bar_of(op.x)) ops::axpby(sb, 1.0, sb, 1.0, db, 0.0, op.n, s_);
+        ops::zero(db, op.n, s_);
+        break;
+      }
+      case TapeOp::ZERO: {
+        if (double* db = bar_of(op.dst)) ops::zero(db, op.n, s_);
+        break;
+      }
+    }
+  }
+}
+
+void Schedule::prepare_vjp(const double*) {
+  throw Error(ERR_UNSUPPORTED, "reverse mode is provided for the real-path CCSD/CCD schedule");
+}
+
+void Schedule::vjp(const double*, double*, const VertexBar*, const double*) {
+  throw Error(ERR_UNSUPPORTED, "reverse mode is provided for the real-path CCSD/CCD schedule");
 }
 
 }  // namespace cc4s_b200

@@ -54,6 +54,27 @@ class Schedule {
   // G runs over the schedule's auxiliary rows (stacked Re/Im rows on the real path).
   void structure_factor(const double* T, double* S_dev, double* dGph_dev);
   int64_t aux_rows() const { return sG_; }
+
+  // ---- reverse mode ---------------------------------------------------------
+  // Vector-Jacobian products of the residual at fixed amplitudes, for schedules
+  // built in adjoint mode.  prepare_vjp(T) evaluates the residual once in FP64
+  // with every device operation recorded (buffers that the fast path reuses are
+  // separate allocations then, so every recorded value survives);
+  // vjp(Rbar, Tbar, gbar) replays the record backwards:
+  //   Tbar = Rbar^T dR/dT   (amplitude-vector layout, T2 part symmetrised),
+  //   gbar->X += Rbar^T dR/dGamma_X  for the vertex blocks given (may be null),
+  // where extra_Vd_bar (pair layout, may be null) is added to the adjoint of the
+  // integrals V_abij before they are propagated to the vertex.
+  struct VertexBar {
+    double* Gpp = nullptr;  // [G][v][v]
+    double* Gph = nullptr;  // [G][v][o]
+    double* Ghh = nullptr;  // [G][o][o]
+    double* Ghp = nullptr;  // [G][o][v]
+  };
+  bool adjoint_mode() const { return adjoint_; }
+  virtual void prepare_vjp(const double* T);
+  virtual void vjp(const double* Rbar, double* Tbar, const VertexBar* gbar,
+                   const double* extra_Vd_bar);
   struct Profile {
     double gemm_seconds = 0, gemm_flops = 0;  // all contractions of the last residual
     double top_seconds = 0, top_flops = 0;    // the most expensive single launch
@@ -65,6 +86,45 @@ class Schedule {
   const Profile& profile() const { return prof_; }
 
  protected:
+  // One recorded device operation (forward), replayed backwards by reverse().
+  struct TapeOp {
+    enum Kind { GEMM, PERM, AXPBY, RANK1, SYMM, COPY, ZERO } kind = GEMM;
+    Contraction c;                      // GEMM
+    bool recompute = false;             // GEMM: rerun `pre` forward and clear the
+    Contraction pre;                    // adjoint of [zero_p, zero_p + zero_n) first
+    double* zero_p = nullptr;
+    int64_t zero_n = 0;
+    double* dst = nullptr;              // PERM / AXPBY / RANK1 / SYMM / COPY / ZERO output
+    const double* x = nullptr;          // PERM / COPY source, AXPBY x, RANK1 A
+    const double* y = nullptr;          // AXPBY y, RANK1 t
+    int64_t d[4] = {0, 0, 0, 0};
+    int perm[4] = {0, 1, 2, 3};
+    double a = 0.0, b = 0.0, cc = 0.0;  // PERM alpha/beta; AXPBY a, b, c; RANK1 a, b
+    int64_t n = 0;
+  };
+  // A forward buffer and its adjoint (same size and layout).
+  struct Region { const double* p; int64_t n; double* bar; };
+  double* bar_of(const double* p) const;
+  View barv(const View& v) const;
+  void reverse(const std::vector<TapeOp>& tape);
+  void reverse_gemm(const Contraction& c);
+  // Bandwidth operations that are recorded while taping.
+  void perm_(double* dst, const double* src, const int64_t d[4], const int p[4], double alpha,
+             double beta);
+  void axpby_(double* out, double a, const double* x, double b, const double* y, double c,
+              int64_t n);
+  void rank1_(double* out, double a, const double* A, double b, const double* t, int64_t n);
+  void sym_(double* R, int64_t n);
+  void copy_(double* dst, const double* src, int64_t n);
+  void zero_(double* p, int64_t n);
+  bool adjoint_ = false;
+  bool taping_ = false;
+  std::vector<TapeOp> tape_;            // residual at the prepared amplitudes
+  std::vector<TapeOp> integrals_tape_;  // iteration-independent integrals from the vertex
+  std::vector<Region> regions_;
+  std::vector<size_t> owned_n_;         // element counts of owned_
+  std::vector<double*> bar_bufs_;       // adjoints of owned_ (adjoint mode)
+
   double* take(size_t elems);
   void gemm_(const Contraction& c);
   // A large contraction: split precision when enabled (batch 1), else FP64.

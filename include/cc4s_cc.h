@@ -107,6 +107,16 @@ typedef struct {
   int split_launches;
 } cc4s_cc_stats;
 
+/* Outcome of the Lambda solve behind cc4s_cc_relaxed_gradient. */
+typedef struct {
+  int iterations;           /* Jacobi + mixer iterations of the Lambda equations */
+  int converged;            /* 1 if the norm of the last change fell below the threshold */
+  double residuum_norm;     /* norm of the last (extrapolated) change of Lambda */
+  double prepare_seconds;   /* recorded forward residual + energy gradients */
+  double vjp_seconds;       /* one Lambda iteration (one transposed-Jacobian product) */
+  double gradient_seconds;  /* final product with dR/dGamma and the integrals */
+} cc4s_cc_lambda_result;
+
 /* Fills the defaults of the reference. */
 void cc4s_cc_default_options(cc4s_cc_options* opt);
 
@@ -155,6 +165,30 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
  * respect to the caller's vertex Gamma[G,p,q] (same layout; complex input gives
  * d/dRe + i d/dIm), nonzero in the particle-hole block.  Either output may be NULL. */
 int cc4s_cc_backward(cc4s_cc_handle* h, double* S_of_G, double* dE_dGamma);
+
+/* Transposed-Jacobian product of the residual (real half-grid path, Ccsd / Ccd):
+ * at amplitudes T1 [Nv,No], T2 [Nv,Nv,No,No] (reference layout, as for
+ * cc4s_cc_residual) and an adjoint R1bar, R2bar of the residual (same layout),
+ *   T1bar, T2bar = Rbar^T dR/dT   (T2bar projected on T_abij = T_baji),
+ *   dGamma       = Rbar^T dR/dGamma in the caller's vertex layout (may be NULL).
+ * The adjoint of Ccsd::getResiduum (Ccsd.cxx:77-378), built by replaying the
+ * recorded residual backwards. */
+int cc4s_cc_residual_vjp(cc4s_cc_handle* h, const double* T1, const double* T2,
+                         const double* R1bar, const double* R2bar, double* T1bar, double* T2bar,
+                         double* dGamma);
+
+/* Relaxed gradient of the converged correlation energy (after cc4s_cc_run, real
+ * half-grid path, Ccsd / Ccd): solves the Lambda equations
+ *   (dR/dT + D)^T lambda = -dE/dT
+ * with the amplitude iteration's Jacobi update, level shift and mixer, each
+ * iteration one transposed-Jacobian product, and returns
+ *   dE_dGamma = dE_c/dGamma|_T + lambda^T dR/dGamma
+ * in the caller's vertex layout (complex input: d/dRe + i d/dIm).  Converged when
+ * the norm of the change of lambda is below `convergence`; otherwise status 4.
+ * Replaces finite differences of CoupledCluster::run (CoupledCluster.cxx:56-191)
+ * around converged amplitudes. */
+int cc4s_cc_relaxed_gradient(cc4s_cc_handle* h, int max_iterations, double convergence,
+                             double* dE_dGamma, cc4s_cc_lambda_result* out);
 
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
 

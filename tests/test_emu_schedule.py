@@ -206,3 +206,62 @@ def test_ueg_reference_energies_through_product_schedule(emu_lib):
     assert r["converged"]
     for k, ref in g["ccsd"]["energy"].items():
         assert abs(r[k] - ref) < 1e-10, (k, r[k], ref)
+
+
+@pytest.mark.parametrize("method,ppl", [("Ccsd", True), ("Ccsd", False), ("Ccd", True)])
+def test_residual_vjp_matches_finite_differences(emu_lib, method, ppl):
+    """Transposed-Jacobian product of the residual (reverse replay of the
+    recorded schedule) against central differences of <Rbar, R(T)> in T and in
+    the vertex."""
+    from cc4s_b200 import Solver
+    No, Nv, NG = 3, 8, 6
+    s = inputs.synthetic_system(No, Nv, NG, seed=3)
+    rng = np.random.default_rng(1)
+
+    def sym(x):
+        return x + x.transpose(1, 0, 3, 2)
+    T = (rng.standard_normal((Nv, No)) * 0.1, sym(rng.standard_normal((Nv, Nv, No, No))) * 0.05)
+    Rb = (rng.standard_normal((Nv, No)), rng.standard_normal((Nv, Nv, No, No)))
+    opts = {"method": method, "ppl": ppl}
+    sol = Solver(opts, lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    (T1b, T2b), Gb = sol.residual_vjp(T, Rb)
+
+    def f(TT, gm=None):
+        so = sol
+        if gm is not None:
+            so = Solver(opts, lib=emu_lib)
+            so.set_inputs(s.eps_h, s.eps_p, gm, True)
+        return sum((a * b).sum() for a, b in zip(Rb, so.residual(TT)))
+    d = (rng.standard_normal((Nv, No)) * (method == "Ccsd"), sym(rng.standard_normal((Nv, Nv, No, No))))
+    h = 1e-5
+    fd = (f((T[0] + h * d[0], T[1] + h * d[1])) - f((T[0] - h * d[0], T[1] - h * d[1]))) / (2 * h)
+    assert abs(fd - ((T1b * d[0]).sum() + (T2b * d[1]).sum())) < 1e-7 * abs(fd)
+    dg = rng.standard_normal(s.gamma.shape)
+    fdg = (f(T, s.gamma + h * dg) - f(T, s.gamma - h * dg)) / (2 * h)
+    assert abs(fdg - (Gb * dg).sum()) < 1e-8 * abs(fdg)
+
+
+@pytest.mark.parametrize("method", ["Ccsd", "Ccd"])
+def test_relaxed_gradient_matches_finite_differences(emu_lib, method):
+    """Lambda equations solved with transposed-Jacobian products: dE_c/dGamma of
+    the converged energy against central differences of re-converged energies
+    (step 1e-5, three random directions) to 1e-6 relative."""
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(4, 12, 20, seed=2)
+    opts = dict(method=method, maxIterations=80, energyConvergence=1e-14,
+                amplitudesConvergence=1e-12)
+
+    def energy(gm):
+        so = Solver(opts, lib=emu_lib)
+        so.set_inputs(s.eps_h, s.eps_p, gm, True)
+        return so, so.run()["correlation"]
+    sol, _ = energy(s.gamma)
+    g, info = sol.relaxed_gradient(max_iterations=100, convergence=1e-12)
+    assert info["converged"]
+    rng = np.random.default_rng(5)
+    h = 1e-5
+    for _ in range(3):
+        d = rng.standard_normal(s.gamma.shape)
+        fd = (energy(s.gamma + h * d)[1] - energy(s.gamma - h * d)[1]) / (2 * h)
+        assert abs(fd - (g * d).sum()) < 1e-6 * abs(fd)
