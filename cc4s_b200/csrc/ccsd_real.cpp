@@ -353,6 +353,10 @@ void CcsdReal::residual(const double* T, double* R) {
     c.alpha = -1.0; c.beta = 1.0;
     tc_(c);
   }
+  // ---- particle-particle ladder (Ccsd.cxx:283-333), before the symmetrisation:
+  // L_abij = L_baji holds exactly on the real path, so the a >= b half of the
+  // ladder (diagonal blocks at weight 1/2) is completed by P(ab,ij) below ------
+  if (opt_.ppl) ppl(Xd_, R2, dGpp_);
   // ---- P(ab,ij) symmetrisation and +V (Ccsd.cxx:256,263) ----------------------
   sym_(R2, n1);
   axpby_(R2, 1.0, R2, 1.0, Vd_, 0.0, D2);
@@ -391,8 +395,6 @@ void CcsdReal::residual(const double* T, double* R) {
     c.B.p = Xkl2_;
     tc_(c);
   }
-  // ---- particle-particle ladder (Ccsd.cxx:283-333) ------------------------------
-  if (opt_.ppl) ppl(Xd_, R2, dGpp_);
   if (ccd) {
     zero_(R1, n1);
     profile_finish();
@@ -477,8 +479,9 @@ void CcsdReal::residual(const double* T, double* R) {
 // Particle-particle ladder on virtual-pair slabs: for blocks X >= Y of s virtual
 // orbitals and panels of c_n values of c,
 //   V[x][y][c'][d] = sum_G dGpp[G][x0+x][c0+c'] dGpp[G][y0+y][d]      (GEMM, K = G)
-//   R_{x y i j} += sum_{c',d} V[x][y][c'][d] X_{c0+c',d,i,j}          (GEMM, K = c_n v)
-// with the off-diagonal blocks mirrored into R_{y x j i}.  Panelling c keeps the
+//   R_{x y i j} += w sum_{c',d} V[x][y][c'][d] X_{c0+c',d,i,j}        (GEMM, K = c_n v)
+// with w = 1/2 on diagonal blocks; added before R <- R + R^T, which supplies the
+// mirrored blocks R_{y x j i} (the reference copies them, Ccsd.cxx:318-330).  Panelling c keeps the
 // slab small enough for wide blocks (s^2 = 4096 rows), and each panel reads only
 // its c-range of X.
 void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
@@ -502,7 +505,7 @@ void CcsdReal::ppl(const double* Xd, double* R2, const double* dGpp) {
           c.A = vw(slab_, sy * nc * v, nc * v, v, 1);
           c.B = vw(cp(Xd) + c0 * o * n1, o * n1, o, n1, 1);   // X_cdij = X[(c,i),(d,j)]
           c.C = vw(R2 + x0 * o * n1 + y0 * o, o * n1, o, n1, 1);
-          if (X != Yb) c.C2 = vw(R2 + y0 * o * n1 + x0 * o, o, o * n1, 1, n1);
+          c.alpha = X == Yb ? 0.5 : 1.0;  // the symmetrisation that follows adds the mirror
           c.beta = 1.0;
           tc_(c);
           if (taping_) {  // the slab is rebuilt before this contraction's adjoint

@@ -284,3 +284,53 @@ def test_complex_run(Solver):
     assert abs(r["correlation"] - ref["energy"]["correlation"]) < TOL_E
     T1, T2 = sol.amplitudes()
     assert _rel(T2, ref["amplitudes"][1]) < TOL_AMP
+
+
+def test_residual_vjp_on_device(Solver):
+    """Transposed-Jacobian product of the residual on the B200 against central
+    differences of <Rbar, R(T)> in T and in the vertex."""
+    No, Nv, NG = 6, 30, 40
+    s = inputs.synthetic_system(No, Nv, NG, seed=3)
+    rng = np.random.default_rng(1)
+    T = _rand_T(rng, Nv, No, scale=0.05)
+    Rb = (rng.standard_normal((Nv, No)), rng.standard_normal((Nv, Nv, No, No)))
+    sol = Solver({})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    (T1b, T2b), Gb = sol.residual_vjp(T, Rb)
+
+    def f(TT, gm=None):
+        so = sol
+        if gm is not None:
+            so = Solver({})
+            so.set_inputs(s.eps_h, s.eps_p, gm, True)
+        return sum((a * b).sum() for a, b in zip(Rb, so.residual(TT)))
+    d = _rand_T(rng, Nv, No, scale=1.0)
+    h = 1e-5
+    fd = (f((T[0] + h * d[0], T[1] + h * d[1])) - f((T[0] - h * d[0], T[1] - h * d[1]))) / (2 * h)
+    assert abs(fd - ((T1b * d[0]).sum() + (T2b * d[1]).sum())) < 1e-6 * abs(fd)
+    dg = rng.standard_normal(s.gamma.shape)
+    fdg = (f(T, s.gamma + h * dg) - f(T, s.gamma - h * dg)) / (2 * h)
+    assert abs(fdg - (Gb * dg).sum()) < 1e-6 * abs(fdg)
+
+
+def test_relaxed_gradient_on_device(Solver):
+    """Lambda equations on the B200: dE_c/dGamma of the converged CCSD energy
+    against central differences of re-converged energies (step 1e-5, four
+    random directions) to 1e-6 relative."""
+    s = inputs.synthetic_system(8, 40, 100, seed=2)
+    opts = dict(maxIterations=100, energyConvergence=1e-14, amplitudesConvergence=1e-11)
+
+    def energy(gm):
+        so = Solver(opts)
+        so.set_inputs(s.eps_h, s.eps_p, gm, True)
+        e = so.run()["correlation"]
+        return so, e
+    sol, _ = energy(s.gamma)
+    g, info = sol.relaxed_gradient(max_iterations=100, convergence=1e-11)
+    assert info["converged"]
+    rng = np.random.default_rng(5)
+    h = 1e-5
+    for _ in range(4):
+        d = rng.standard_normal(s.gamma.shape)
+        fd = (energy(s.gamma + h * d)[1] - energy(s.gamma - h * d)[1]) / (2 * h)
+        assert abs(fd - (g * d).sum()) < 1e-6 * abs(fd)
