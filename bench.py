@@ -298,6 +298,60 @@ def run_ours(args, world, rank, local):
     return line
 
 
+def run_adjoint(args, local):
+    """Adjoint form at the workload: converged FP64 CCSD, Lambda equations by
+    transposed-Jacobian products, relaxed dE_c/dGamma; times each against one
+    forward iteration and checks the gradient against central differences of
+    re-converged energies (step 1e-5) on a few random vertex directions."""
+    import numpy as np
+    import torch
+    from cc4s_b200 import Solver
+    from cc4s_b200.synthetic import config
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    eh, ep, g, hg = config(cfg, seed=0)
+    opts = dict(maxIterations=100, energyConvergence=1e-12, amplitudesConvergence=1e-10,
+                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
+
+    def solve(gm):
+        so = Solver(opts)
+        so.set_inputs(eh, ep, gm, half_grid=hg)
+        return so, so.run()
+    sol, r = solve(g)
+    fwd = statistics.median(h["seconds"] for h in r["history"][2:]) if r["iterations"] > 3 else \
+        r["history"][-1]["seconds"]
+    t0 = time.perf_counter()
+    grad, info = sol.relaxed_gradient(max_iterations=100, convergence=1e-10)
+    t_back = time.perf_counter() - t0
+    sol.close()
+    rng = np.random.default_rng(7)
+    h = 1e-5
+    checks = []
+    for _ in range(args.fd_directions):
+        d = rng.standard_normal(g.shape)
+        ep_ = solve(g + h * d)[1]["correlation"]
+        em_ = solve(g - h * d)[1]["correlation"]
+        fd = (ep_ - em_) / (2 * h)
+        an = float((grad * d).sum())
+        checks.append({"fd": fd, "adjoint": an, "rel_err": abs(fd - an) / abs(fd)})
+    return {"metric": "CCSD adjoint: relaxed dE_c/dGamma (Lambda equations) vs one forward iteration",
+            "value": (info["vjp_seconds"] / fwd) if fwd else None, "unit": "x forward iteration",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d real, DIIS 5, FP64" % (cfg, o, v, G),
+                       "forward_iterations": r["iterations"], "forward_s_per_iter": fwd,
+                       "energy": r["correlation"],
+                       "lambda_iterations": info["iterations"], "lambda_converged": info["converged"],
+                       "lambda_residuum_norm": info["residuum_norm"],
+                       "prepare_seconds": info["prepare_seconds"],
+                       "lambda_s_per_iter": info["vjp_seconds"],
+                       "gradient_seconds": info["gradient_seconds"],
+                       "backward_total_seconds": t_back,
+                       "backward_total_vs_forward_iteration": t_back / fwd if fwd else None},
+            "fd_check": {"step": h, "directions": checks,
+                         "max_rel_err": max((c["rel_err"] for c in checks), default=None)}}
+
+
 def run_reference(args, world, rank):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
@@ -332,6 +386,9 @@ def main():
     ap.add_argument("--config", default="c1", choices=sorted(CONFIG_SHAPES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "split3"])
+    ap.add_argument("--adjoint", action="store_true",
+                    help="time and check the adjoint form (relaxed gradient) instead")
+    ap.add_argument("--fd-directions", type=int, default=2)
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -341,6 +398,10 @@ def main():
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return
     world, rank, local = dist_setup()
+    if args.adjoint:
+        if rank == 0:
+            print(json.dumps(run_adjoint(args, local)), flush=True)
+        return
     line = run_ours(args, world, rank, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
