@@ -44,7 +44,7 @@ class Options(ctypes.Structure):
         ("amplitudes_convergence", ctypes.c_double), ("level_shift", ctypes.c_double),
         ("integrals_slice_size", ctypes.c_int64), ("ppl", ctypes.c_int), ("device", ctypes.c_int),
         ("profile", ctypes.c_int), ("linearized", ctypes.c_int),
-        ("adjacent_pairs_exchange", ctypes.c_int),
+        ("adjacent_pairs_exchange", ctypes.c_int), ("precision_refinement", ctypes.c_double),
     ]
 
 
@@ -56,7 +56,7 @@ class Result(ctypes.Structure):
         ("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("history_len", ctypes.c_int),
         ("energy", ctypes.c_double * MAX_HISTORY), ("delta_energy", ctypes.c_double * MAX_HISTORY),
         ("residuum_norm", ctypes.c_double * MAX_HISTORY), ("seconds", ctypes.c_double * MAX_HISTORY),
-        ("flops_per_iteration", ctypes.c_double),
+        ("flops_per_iteration", ctypes.c_double), ("refined_from", ctypes.c_int),
     ]
 
 

@@ -45,6 +45,7 @@ def _options(lib, arguments):
     o.profile = 1 if arguments.get("profile", False) else 0
     o.linearized = 1 if arguments.get("linearized", False) else 0
     o.adjacent_pairs_exchange = 1 if arguments.get("adjacentPairsExchange", False) else 0
+    o.precision_refinement = float(arguments.get("precisionRefinement", 0.0))
     return o
 
 
@@ -134,7 +135,7 @@ class Solver:
                     exchange=res.exchange, secondOrder=res.second_order,
                     correlation_imag=res.correlation_imag, iterations=res.iterations,
                     converged=bool(res.converged), history=hist,
-                    flops_per_iteration=res.flops_per_iteration)
+                    flops_per_iteration=res.flops_per_iteration, refined_from=res.refined_from)
 
     def amplitudes(self):
         t1, t2 = self._alloc_amps()

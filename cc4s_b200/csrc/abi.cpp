@@ -121,6 +121,8 @@ int Handle::run(cc4s_cc_result* out) {
   std::memset(out, 0, sizeof(*out));
   out->second_order = std::nan("");
   reset_mixer();
+  const bool split = opt.precision != CC4S_PRECISION_FP64;
+  solver->set_precision(split ? 3 : 0);
   const int maxIt = opt.max_iterations;
   const double shift = opt.level_shift;
   const int N = static_cast<int>(A.size());
@@ -168,6 +170,12 @@ int Handle::run(cc4s_cc_result* out) {
     }
     if (second) out->second_order = e.real();
     if (std::abs(e - prev) < opt.energy_convergence && norm < opt.amplitudes_convergence) break;
+    // defect correction: the split form brings the amplitudes close, FP64 finishes
+    if (split && !out->refined_from && opt.precision_refinement > 0.0 &&
+        norm < opt.precision_refinement) {
+      solver->set_precision(0);
+      out->refined_from = i + 2;
+    }
     prev = e;
   }
   (void)N;
@@ -459,6 +467,7 @@ void cc4s_cc_default_options(cc4s_cc_options* o) {
   o->profile = 0;
   o->linearized = 0;
   o->adjacent_pairs_exchange = 0;
+  o->precision_refinement = 0.0;
 }
 
 int cc4s_cc_create(const cc4s_cc_options* opt, cc4s_cc_handle** h) {

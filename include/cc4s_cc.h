@@ -79,6 +79,9 @@ typedef struct {
   int profile;                  /* 1: time every contraction launch (CUDA events) */
   int linearized;               /* "linearized" (0), Drccd only, Drccd.cxx:53-55 */
   int adjacent_pairs_exchange;  /* "adjacentPairsExchange" (0), Drccd only, Drccd.cxx:56-58 */
+  double precision_refinement;  /* split form only: once the residuum norm falls below this
+                                   value the remaining iterations run in FP64, so the
+                                   converged amplitudes solve the FP64 equations (0: off) */
 } cc4s_cc_options;
 
 typedef struct {
@@ -92,6 +95,8 @@ typedef struct {
   double residuum_norm[CC4S_MAX_HISTORY]; /* dR (DIIS-extrapolated change norm) */
   double seconds[CC4S_MAX_HISTORY];       /* device time of the iteration */
   double flops_per_iteration;  /* FP64-equivalent flops of one residual (this schedule) */
+  int refined_from;            /* split form with precision_refinement: first iteration run
+                                  in FP64 (1-based; 0: none) */
 } cc4s_cc_result;
 
 typedef struct {

@@ -110,6 +110,25 @@ def test_split_precision_form_accuracy(emu_lib):
     assert ra["correlation"] != rb["correlation"]  # the split path really ran
 
 
+def test_split_precision_refinement_reaches_fp64_fixed_point(emu_lib):
+    """precisionRefinement: split iterations until the residuum norm is below the
+    threshold, FP64 after; the converged energy is the FP64 one to the convergence
+    threshold, while the pure split form differs at the split-precision level."""
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(6, 30, 60, seed=0)
+    o = dict(maxIterations=60, energyConvergence=1e-13, amplitudesConvergence=1e-10)
+    runs = {}
+    for name, extra in (("fp64", {}), ("split", dict(precision="split3")),
+                        ("refined", dict(precision="split3", precisionRefinement=1e-5))):
+        sol = Solver(dict(o, **extra), lib=emu_lib)
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+        runs[name] = sol.run()
+        assert runs[name]["converged"]
+    assert runs["refined"]["refined_from"] > 1
+    assert abs(runs["refined"]["correlation"] - runs["fp64"]["correlation"]) < 1e-12
+    assert abs(runs["split"]["correlation"] - runs["fp64"]["correlation"]) > 1e-14
+
+
 def test_split_precision_complex_path(emu_lib):
     """Complex path: the large contractions run as split products (exact model of
     the tensor-core scheme); the converged energy stays far inside 1 uEh."""
