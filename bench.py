@@ -352,6 +352,44 @@ def run_adjoint(args, local):
                          "max_rel_err": max((c["rel_err"] for c in checks), default=None)}}
 
 
+def run_converge(args, local):
+    """Accuracy of the split form at convergence: FP64, pure split and split with
+    FP64 refinement, each to energyConvergence 1e-10 (DIIS 5, at most 40
+    iterations); reports |E_split - E_fp64|, iterations and time to solution."""
+    import torch
+    from cc4s_b200 import Solver
+    from cc4s_b200.synthetic import config
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    eh, ep, g, hg = config(cfg, seed=0)
+    base = dict(maxIterations=40, energyConvergence=1e-10, amplitudesConvergence=1e-8,
+                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
+    forms = {"fp64": {}, "split3": dict(precision="split3"),
+             "split3_refined": dict(precision="split3", precisionRefinement=args.refine)}
+    out = {}
+    for name, extra in forms.items():
+        so = Solver(dict(base, **extra))
+        so.set_inputs(eh, ep, g, half_grid=hg)
+        r = so.run()
+        so.close()
+        out[name] = {"energy": r["correlation"], "iterations": r["iterations"],
+                     "converged": r["converged"], "seconds": sum(h["seconds"] for h in r["history"]),
+                     "refined_from": r["refined_from"],
+                     "s_per_iter": [h["seconds"] for h in r["history"]]}
+    e64 = out["fp64"]["energy"]
+    for name in ("split3", "split3_refined"):
+        out[name]["abs_dE_vs_fp64"] = abs(out[name]["energy"] - e64)
+    kind = "complex" if cfg in COMPLEX_CONFIGS else "real"
+    return {"metric": "CCSD converged |dE_c| split-precision vs FP64 (bound 1e-6 Eh)",
+            "value": out["split3_refined"]["abs_dE_vs_fp64"], "unit": "Eh",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, energyConvergence 1e-10"
+                                   % (cfg, o, v, G, kind),
+                       "precision_refinement": args.refine},
+            "forms": out}
+
+
 def run_reference(args, world, rank):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
@@ -389,6 +427,10 @@ def main():
     ap.add_argument("--adjoint", action="store_true",
                     help="time and check the adjoint form (relaxed gradient) instead")
     ap.add_argument("--fd-directions", type=int, default=2)
+    ap.add_argument("--converge", action="store_true",
+                    help="converge FP64, split and refined split forms and compare energies")
+    ap.add_argument("--refine", type=float, default=1e-5,
+                    help="residuum norm below which the refined split form switches to FP64")
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -398,9 +440,10 @@ def main():
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return
     world, rank, local = dist_setup()
-    if args.adjoint:
+    if args.adjoint or args.converge:
         if rank == 0:
-            print(json.dumps(run_adjoint(args, local)), flush=True)
+            line = run_adjoint(args, local) if args.adjoint else run_converge(args, local)
+            print(json.dumps(line), flush=True)
         return
     line = run_ours(args, world, rank, local)
     if rank == 0:
