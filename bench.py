@@ -1,15 +1,17 @@
 """Benchmark of the CoupledCluster (CCSD) step on B200.
 
 A "step" is one CCSD iteration (residual, Jacobi update, DIIS, energy) on a
-seeded synthetic system.  Default workload: No=32, Nv=256, NG=1024, real,
-FP64 (the FP64 parity case).  T2 (0.54 GB) and the vertex are larger than
-L2, so no flush is needed between iterations.
+seeded synthetic system.  Default workload: No=64, Nv=640, NG=2560, real
+(T2 13.4 GB), both the split-precision tensor-core form (headline) and the
+FP64 form, W warm-up and K timed iterations each.  T2 and the vertex are far
+larger than L2, so no flush is needed between iterations.
 
 value: reference-equivalent TFLOP/s = F_ref / (s per iteration), with F_ref
 the flop count of the reference's formulation (cc4s_b200.flops), timed with
 CUDA events on the library's stream inside the library, max over ranks.
 e2e: the same metric through the C ABI from host buffers: set_inputs (vertex
-upload and integral build) + K iterations + amplitude download, wall clock.
+upload and integral build) + the first (MP2) iteration + K full iterations +
+amplitude download, wall clock; only the K full iterations' flops count.
 
 Multi-GPU: every rank runs its own replica of the workload (weak scaling, no
 collective on the data path); value is the sum over ranks.
@@ -18,6 +20,8 @@ collective on the data path); value is the sum over ranks.
 reference itself needs MPI and the Cyclops Tensor Framework, which are not
 installed) timed on this host's cores on a bounded sample of the same
 workload.
+--adjoint: relaxed-gradient (Lambda equations) timing and finite-difference
+check; --converge: converged energies of the FP64, split and refined forms.
 """
 import argparse
 import json
@@ -418,10 +422,10 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1", choices=sorted(CONFIG_SHAPES))
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIG_SHAPES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "split3"])
     ap.add_argument("--adjoint", action="store_true",
