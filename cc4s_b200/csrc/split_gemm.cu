@@ -1,6 +1,6 @@
 // Split-precision FP64 contraction: FP16 integer slices on tcgen05 tensor cores.
 //
-// Kernel layout (one 128 x 128 output tile per CTA, 192 threads):
+// Kernel layout (one 128 x 128 output tile per CTA, 320 threads):
 //   warp 0      TMA producer: per k-block of 32, three A-slice and three
 //               B-slice tiles (128 x 32 FP16, 64-byte swizzle) into a 4-stage
 //               shared-memory ring, completion tracked by mbarriers;
@@ -8,8 +8,11 @@
 //               (M=128, N=128, K=16) for the six slice products into three
 //               FP32 accumulators (TMEM columns 0, 128, 256) and commits to
 //               mbarriers that release smem stages and publish K chunks;
-//   warps 2..5  epilogue: after each K chunk, tcgen05.ld the three groups,
-//               recombine in FP64 with the row/column scales and add into C.
+//   warps 2..9  epilogue: after each K chunk, tcgen05.ld the three groups and
+//               add them into FP64 register accumulators (two warps per TMEM
+//               lane quadrant, 64 columns each); after the last chunk, scale,
+//               stage the tile in the idle stage buffers and store C once,
+//               coalesced along the output's contiguous index.
 // Every mbarrier wait is bounded; on expiry the kernel records an error flag
 // and every role leaves its loop, so the kernel always terminates.
 #include "split_gemm.cuh"
@@ -210,7 +213,7 @@ struct SplitParams {
   int* error;
 };
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320)
 split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
              SplitParams p) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -234,7 +237,7 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
       mbar_init(smem_u32(&bars[NST + s]), 1);
     }
     mbar_init(smem_u32(&bars[2 * NST]), 1);
-    mbar_init(smem_u32(&bars[2 * NST + 1]), 128);
+    mbar_init(smem_u32(&bars[2 * NST + 1]), 256);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 1) {
@@ -306,48 +309,73 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
       umma_commit(smem_u32(&bars[2 * NST]));    // chunk accumulators ready
     }
   } else if (warp >= 2) {
-    // ---- epilogue: TMEM -> FP64 recombination -> C ----
-    const int quad = warp & 3;                  // TMEM lanes 32*quad .. 32*quad+31
+    // ---- epilogue: TMEM -> FP64 accumulators (all K chunks) -> one store of C ----
+    // Two warps per TMEM lane quadrant (warp % 4): each thread owns one row and
+    // 64 of the 128 columns, summing the three groups of every chunk in FP64.
+    const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int row = quad * 32 + lane;
-    const int64_t m = m0 + row;
-    const bool mok = m < p.M;
-    const double sa = mok ? ldexp(1.0, p.ea[m]) : 0.0;
-    const int64_t ro = mok ? p.Cm.off(static_cast<uint32_t>(m)) : 0;
-    const int64_t ro2 = (mok && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
+    double acc[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
     for (int c = 0; c < nchunks; ++c) {
       if (!mbar_wait(smem_u32(&bars[2 * NST]), c & 1)) { atomicExch(&abort_flag, 1); break; }
       tc_fence_after();
-      const double w0 = 0x1p-12, w1 = 0x1p-23, w2 = 0x1p-34;
-      for (int cb = 0; cb < TN; cb += 32) {
-        uint32_t g0[32], g1[32], g2[32];
-        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(quad * 32) << 16) + cb;
-        tmem_ld32(lane_addr, g0);
-        tmem_ld32(lane_addr + TN, g1);
-        tmem_ld32(lane_addr + 2 * TN, g2);
+#pragma unroll
+      for (int cb = 0; cb < 64; cb += 32) {
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) +
+                               static_cast<uint32_t>(64 * half + cb);
+        uint32_t g[32];
+        tmem_ld32(taddr, g);
         tmem_wait_ld();
-        if (mok) {
-#pragma unroll 4
-          for (int j = 0; j < 32; ++j) {
-            const int64_t n = n0 + cb + j;
-            if (n >= p.N) break;
-            const double v = (static_cast<double>(__uint_as_float(g0[j])) * w0 +
-                              static_cast<double>(__uint_as_float(g1[j])) * w1 +
-                              static_cast<double>(__uint_as_float(g2[j])) * w2) *
-                             sa * ldexp(1.0, p.eb[n]) * p.alpha;
-            const int64_t co = p.Cn.off(static_cast<uint32_t>(n));
-            double* cptr = p.C + ro + co;
-            const double prev = (c == 0) ? (p.beta != 0.0 ? p.beta * *cptr : 0.0) : *cptr;
-            *cptr = prev + v;
-            if (p.C2) {
-              double* c2 = p.C2 + ro2 + p.C2n.off(static_cast<uint32_t>(n));
-              const double prev2 = (c == 0) ? (p.beta != 0.0 ? p.beta * *c2 : 0.0) : *c2;
-              *c2 = prev2 + v;
-            }
-          }
-        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-12;
+        tmem_ld32(taddr + TN, g);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-23;
+        tmem_ld32(taddr + 2 * TN, g);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-34;
       }
       tc_fence_before();
       mbar_arrive(smem_u32(&bars[2 * NST + 1]));
+    }
+    // After the last chunk every MMA has retired and every TMA load has been
+    // consumed, so the stage buffers hold the scaled tile T[128][129] for a
+    // store along whichever index of the output is contiguous.
+    double* T = reinterpret_cast<double*>(base);
+    constexpr int LDT = TN + 1;
+    const int64_t m = m0 + row;
+    const double sa = m < p.M ? ldexp(p.alpha, p.ea[m]) : 0.0;
+#pragma unroll
+    for (int j = 0; j < 64; ++j) {
+      const int64_t n = n0 + 64 * half + j;
+      T[row * LDT + 64 * half + j] = n < p.N ? acc[j] * sa * ldexp(1.0, p.eb[n]) : 0.0;
+    }
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    if (!abort_flag) {
+      const int ew = warp - 2;  // 0..7
+      for (int out = 0; out < 2; ++out) {
+        double* O = out == 0 ? p.C : p.C2;
+        if (!O) continue;
+        const Ax& Om = out == 0 ? p.Cm : p.C2m;
+        const Ax& On = out == 0 ? p.Cn : p.C2n;
+        const bool n_contig = On.s_i == 1 && On.inner > 1;
+        for (int q = 0; q < 16; ++q) {
+          for (int b = 0; b < 4; ++b) {
+            // n-contiguous: warp row r, lanes along columns; otherwise warp column, lanes along rows
+            const int r = n_contig ? ew + 8 * q : 32 * b + lane;
+            const int cc = n_contig ? 32 * b + lane : ew + 8 * q;
+            const int64_t mm = m0 + r, nn = n0 + cc;
+            if (mm >= p.M || nn >= p.N) continue;
+            double* ptr = O + Om.off(static_cast<uint32_t>(mm)) + On.off(static_cast<uint32_t>(nn));
+            const double v = T[r * LDT + cc];
+            *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+          }
+        }
+      }
     }
   }
   tc_fence_before();
@@ -551,7 +579,7 @@ void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
     configured = true;
   }
   dim3 grid(static_cast<unsigned>(L.Np / TN), static_cast<unsigned>(L.Mp / TM));
-  split_kernel<<<grid, 192, SMEM_BYTES, s>>>(ta, tb, sp);
+  split_kernel<<<grid, 320, SMEM_BYTES, s>>>(ta, tb, sp);
   CC_LAUNCH_CHECK();
   g_split_launches.fetch_add(1);
 }
