@@ -1,0 +1,63 @@
+// Kernel-level check and timing of the split-precision contraction (gemm_split)
+// against the FP64 DMMA contraction (gemm) on plain row-major operands.
+// Usage: split_check [shape index]; prints one line per shape and exits non-zero
+// on a CUDA error, a bounded-wait error flag or a relative difference above 1e-5.
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <cmath>
+#include "../../cc4s_b200/csrc/split_gemm.cuh"
+using namespace cc4s_b200;
+
+int main(int argc, char** argv) {
+  struct S { int64_t M, N, K; int tA, tB; };
+  S shapes[] = {{128, 128, 64, 0, 0}, {200, 136, 100, 0, 1}, {1000, 700, 5000, 1, 0},
+                {4096, 4096, 4096, 0, 0}, {8192, 8192, 8192, 0, 0}, {4096, 4096, 40960, 0, 0},
+                {16384, 16384, 2560, 0, 0}, {8192, 8192, 65536, 0, 0}};
+  int* err; cudaMalloc(&err, 4); cudaMemset(err, 0, 4);
+  SplitScratch ws; ws.bytes = size_t(3) << 30; cudaMalloc(&ws.p, ws.bytes); ws.error = err;
+  GemmScratch gs; gs.elems = 1 << 24; cudaMalloc(&gs.p, gs.elems * 8);
+  const int only = argc > 1 ? atoi(argv[1]) : -1;
+  int idx = -1;
+  for (auto& s : shapes) {
+    ++idx;
+    if (only >= 0 && idx != only) continue;
+    double *A, *B, *C1, *C2;
+    cudaMalloc(&A, s.M * s.K * 8); cudaMalloc(&B, s.K * s.N * 8);
+    cudaMalloc(&C1, s.M * s.N * 8); cudaMalloc(&C2, s.M * s.N * 8);
+    std::vector<double> h(std::max(s.M * s.K, s.K * s.N));
+    srand(7);
+    for (auto& x : h) x = ((rand() / (double)RAND_MAX) - 0.5) * std::pow(2.0, (rand() % 9) - 4);
+    cudaMemcpy(A, h.data(), s.M * s.K * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(B, h.data(), s.K * s.N * 8, cudaMemcpyHostToDevice);
+    Contraction c; c.M = s.M; c.N = s.N; c.K = s.K;
+    c.A = s.tA ? tr(A, s.M) : rm(A, s.K);
+    c.B = s.tB ? tr(B, s.K) : rm(B, s.N);
+    c.C = rm(C1, s.N);
+    cudaEvent_t e0, e1, e2; cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    gemm(c, 0, gs);
+    cudaEventRecord(e0);
+    gemm(c, 0, gs);
+    cudaEventRecord(e1);
+    c.C = rm(C2, s.N);
+    gemm_split(c, 0, ws);
+    cudaEventRecord(e2);
+    gemm_split(c, 0, ws);
+    cudaEvent_t e3; cudaEventCreate(&e3); cudaEventRecord(e3);
+    cudaError_t ce = cudaDeviceSynchronize();
+    float ms64 = 0, ms = 0; cudaEventElapsedTime(&ms64, e0, e1); cudaEventElapsedTime(&ms, e2, e3);
+    int herr = 0; cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
+    std::vector<double> r1(s.M * s.N), r2(s.M * s.N);
+    cudaMemcpy(r1.data(), C1, s.M * s.N * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(r2.data(), C2, s.M * s.N * 8, cudaMemcpyDeviceToHost);
+    double md = 0, mx = 0;
+    for (size_t i = 0; i < r1.size(); ++i) { md = std::fmax(md, std::fabs(r1[i] - r2[i])); mx = std::fmax(mx, std::fabs(r1[i])); }
+    const double f = 2.0 * s.M * s.N * s.K;
+    printf("M=%ld N=%ld K=%ld tA=%d tB=%d: cuda=%s errflag=%d max|diff|/max=%.3e fp64 %.3f ms = %.1f TF; split %.3f ms = %.1f TF(fp64-equiv)\n",
+           (long)s.M, (long)s.N, (long)s.K, s.tA, s.tB, cudaGetErrorString(ce), herr, md / mx,
+           ms64, f / (ms64 * 1e-3) / 1e12, ms, f / (ms * 1e-3) / 1e12);
+    if (ce != cudaSuccess || herr || !(md / mx < 1e-5)) return 1;
+    cudaFree(A); cudaFree(B); cudaFree(C1); cudaFree(C2);
+  }
+  return 0;
+}
