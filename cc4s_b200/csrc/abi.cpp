@@ -1,5 +1,6 @@
 // Iteration loop (CoupledCluster::run) and the extern "C" entry points.
 #include <cmath>
+#include <cstdio>
 #include <complex>
 #include <cstring>
 #include <string>
@@ -79,6 +80,30 @@ void Handle::set_initial(const double* T1, const double* T2) {
   have_T = true;
 }
 
+// Error text of a failed DIIS solve: the reason, the iteration and the bordered
+// overlap matrix (DiisMixer.cxx:116-133 raises the same failure).
+std::string Handle::diis_failure(int status, int iteration, double energy, double norm) {
+  const int N = static_cast<int>(A.size()), M = N + 1;
+  std::vector<double> b(M * M);
+  ops::d2h(b.data(), B, b.size(), stream);
+  ops::sync(stream);
+  std::string msg = std::string("Diagonalization failed (") +
+                    (status == 2 ? "non-finite entry" : "singular") +
+                    " DIIS system) at iteration " + std::to_string(iteration + 1) +
+                    "; previous energy " + std::to_string(energy) + ", residuum norm " +
+                    std::to_string(norm) + "; B =";
+  char buf[64];
+  for (int r = 0; r < M; ++r) {
+    msg += " [";
+    for (int c = 0; c < M; ++c) {
+      std::snprintf(buf, sizeof(buf), c ? " %.3e" : "%.3e", b[r * M + c]);
+      msg += buf;
+    }
+    msg += "]";
+  }
+  return msg;
+}
+
 void Handle::mix(double* A_new, double* dT_new, double* norm2_dev, double* out) {
   const int64_t n = shape.total();
   if (opt.mixer == CC4S_MIXER_LINEAR) {
@@ -153,7 +178,7 @@ int Handle::run(cc4s_cc_result* out) {
     int status_int;
     std::memcpy(&status_int, &st, sizeof(int));
     if (opt.mixer == CC4S_MIXER_DIIS && status_int != 0)
-      throw Error(ERR_DIIS_SINGULAR, "Diagonalization failed (singular DIIS system)");
+      throw Error(ERR_DIIS_SINGULAR, diis_failure(status_int, i, prev.real(), i > 0 && i <= CC4S_MAX_HISTORY ? out->residuum_norm[i - 1] : 0.0));
     if (opt.precision != CC4S_PRECISION_FP64 && solver->device_error())
       throw Error(ERR_TIMEOUT, "a tensor-core kernel gave up a bounded wait");
     Dr = host[0]; Xr = host[1];
@@ -392,7 +417,7 @@ void Handle::relaxed_gradient(int max_iterations, double convergence, double* dE
       int status_int;
       std::memcpy(&status_int, &st, sizeof(int));
       if (diis && status_int != 0)
-        throw Error(ERR_DIIS_SINGULAR, "Diagonalization failed (singular DIIS system, Lambda)");
+        throw Error(ERR_DIIS_SINGULAR, "Lambda equations: " + diis_failure(status_int, it, 0.0, out->residuum_norm));
       const double norm = std::sqrt(host[0]);
       if (!std::isfinite(norm)) throw Error(ERR_NON_FINITE, "non-finite Lambda update");
       const double sec = 1e-3 * ops::event_ms(ev0, ev1);

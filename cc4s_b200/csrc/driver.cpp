@@ -66,31 +66,32 @@ void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, in
     if (!std::isfinite(eps_h[k])) throw Error(ERR_NON_FINITE, "non-finite eps_h");
   for (int64_t k = 0; k < Nv; ++k)
     if (!std::isfinite(eps_p[k])) throw Error(ERR_NON_FINITE, "non-finite eps_p");
-  bool has_imag = false;
-  for (int64_t k = 0; k < nin; ++k) {
-    if (!std::isfinite(gamma[k])) throw Error(ERR_NON_FINITE, "non-finite Coulomb vertex");
-    if (is_complex && (k & 1) && gamma[k] != 0.0) has_imag = true;
-  }
   free_state();
   for (double* p : vertex) ops::release(p);
   vertex.clear();
-  in_NG = NG;
-  in_Np = Np;
-  in_complex = is_complex;
-  in_stacked = half_grid && has_imag;
-  auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
-  if (!half_grid) {
-    // Complex path: planar complex slices (imaginary plane at +size, zero for real input).
-    ComplexSystem cs;
-    cs.o = No; cs.v = Nv; cs.G = NG;
-    cs.eh = vtake(No); cs.ep = vtake(Nv);
-    const int64_t spp = NG * Nv * Nv, sph = NG * Nv * No, shh = NG * No * No;
-    cs.Gpp = vtake(2 * spp); cs.Gph = vtake(2 * sph); cs.Ghh = vtake(2 * shh); cs.Ghp = vtake(2 * sph);
-    ops::h2d(cs.eh, eps_h, No, stream);
-    ops::h2d(cs.ep, eps_p, Nv, stream);
-    double* staging = ops::alloc(nin);
-    try {
-      ops::h2d(staging, gamma, nin, stream);
+  // The vertex goes to the device once; its finiteness and whether any
+  // imaginary part is non-zero are decided there (ops::scan_vertex).
+  double* staging = ops::alloc(nin);
+  bool has_imag = false;
+  try {
+    ops::h2d(staging, gamma, nin, stream);
+    const int flags = ops::scan_vertex(staging, nin, is_complex, stream);
+    if (flags & 1) throw Error(ERR_NON_FINITE, "non-finite Coulomb vertex");
+    has_imag = (flags & 2) != 0;
+    in_NG = NG;
+    in_Np = Np;
+    in_complex = is_complex;
+    in_stacked = half_grid && has_imag;
+    auto vtake = [&](size_t n) { double* p = ops::alloc(n); vertex.push_back(p); return p; };
+    if (!half_grid) {
+      // Complex path: planar complex slices (imaginary plane at +size, zero for real input).
+      ComplexSystem cs;
+      cs.o = No; cs.v = Nv; cs.G = NG;
+      cs.eh = vtake(No); cs.ep = vtake(Nv);
+      const int64_t spp = NG * Nv * Nv, sph = NG * Nv * No, shh = NG * No * No;
+      cs.Gpp = vtake(2 * spp); cs.Gph = vtake(2 * sph); cs.Ghh = vtake(2 * shh); cs.Ghp = vtake(2 * sph);
+      ops::h2d(cs.eh, eps_h, No, stream);
+      ops::h2d(cs.ep, eps_p, Nv, stream);
       const int parts = is_complex ? 2 : 1;
       for (int part = 0; part < 2; ++part) {
         if (part >= parts) {
@@ -104,33 +105,22 @@ void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, in
         ops::gather_vertex(cs.Ghp + part * sph, staging, is_complex, part, NG, Np, 0, No, No, Nv, stream);
       }
       ops::sync(stream);
-    } catch (...) {
-      ops::release(staging);
-      throw;
-    }
-    ops::release(staging);
-    csys = cs;
-    sys = RealSystem();
-    sys.o = No; sys.v = Nv; sys.G = NG; sys.eh = cs.eh; sys.ep = cs.ep;
-    shape = ops::AmpShape{No, Nv, 2};
-    complex_path = true;
-    allocate_state();
-    return;
-  }
-  // Real path: stack Re and (if present) Im rows into one real auxiliary index.
-  const int64_t parts = has_imag ? 2 : 1;
-  const int64_t G = NG * parts;
-  RealSystem rs;
-  rs.o = No; rs.v = Nv; rs.G = G;
-  rs.eh = vtake(No); rs.ep = vtake(Nv);
-  rs.Gpp = vtake(G * Nv * Nv); rs.Gph = vtake(G * Nv * No);
-  rs.Ghh = vtake(G * No * No); rs.Ghp = vtake(G * No * Nv);
-  ops::h2d(rs.eh, eps_h, No, stream);
-  ops::h2d(rs.ep, eps_p, Nv, stream);
-  {
-    double* staging = ops::alloc(nin);
-    try {
-      ops::h2d(staging, gamma, nin, stream);
+      csys = cs;
+      sys = RealSystem();
+      sys.o = No; sys.v = Nv; sys.G = NG; sys.eh = cs.eh; sys.ep = cs.ep;
+      shape = ops::AmpShape{No, Nv, 2};
+      complex_path = true;
+    } else {
+      // Real path: stack Re and (if present) Im rows into one real auxiliary index.
+      const int64_t parts = has_imag ? 2 : 1;
+      const int64_t G = NG * parts;
+      RealSystem rs;
+      rs.o = No; rs.v = Nv; rs.G = G;
+      rs.eh = vtake(No); rs.ep = vtake(Nv);
+      rs.Gpp = vtake(G * Nv * Nv); rs.Gph = vtake(G * Nv * No);
+      rs.Ghh = vtake(G * No * No); rs.Ghp = vtake(G * No * Nv);
+      ops::h2d(rs.eh, eps_h, No, stream);
+      ops::h2d(rs.ep, eps_p, Nv, stream);
       for (int64_t part = 0; part < parts; ++part) {
         const int64_t off = part * NG;
         ops::gather_vertex(rs.Gpp + off * Nv * Nv, staging, is_complex, (int)part, NG, Np, No, Nv, No, Nv, stream);
@@ -139,15 +129,17 @@ void Handle::set_inputs(const double* eps_h, int64_t No, const double* eps_p, in
         ops::gather_vertex(rs.Ghp + off * No * Nv, staging, is_complex, (int)part, NG, Np, 0, No, No, Nv, stream);
       }
       ops::sync(stream);
-    } catch (...) {
-      ops::release(staging);
-      throw;
+      sys = rs;
+      shape = ops::AmpShape{No, Nv, 1};
+      complex_path = false;
     }
+  } catch (...) {
     ops::release(staging);
+    for (double* p : vertex) ops::release(p);
+    vertex.clear();
+    throw;
   }
-  sys = rs;
-  shape = ops::AmpShape{No, Nv, 1};
-  complex_path = false;
+  ops::release(staging);
   allocate_state();
 }
 

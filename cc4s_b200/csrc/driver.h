@@ -36,6 +36,7 @@ struct Handle {
   void upload_amplitudes(double* dst, const double* T1, const double* T2, double* st);
   void download_amplitudes(const double* src, double* T1, double* T2, double* st);
   void mix(double* A_new, double* dT_new, double* norm2_dev, double* out);
+  std::string diis_failure(int status, int iteration, double energy, double norm);
   // reverse mode (real path)
   CcsdReal* adjoint_schedule();
   void scatter_vertex_bar(const Schedule::VertexBar& vb, double* out);

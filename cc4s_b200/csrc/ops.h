@@ -52,6 +52,10 @@ void symmetrize(double* R, int64_t n, Stream s);
 void gather_vertex(double* out, const double* in, bool in_complex, int part, int64_t NG,
                    int64_t Np, int64_t row0, int64_t nx, int64_t col0, int64_t ny, Stream s);
 
+// Scans n doubles of a device vector (complex interleaved when complex_values):
+// returns bit 0 if any is not finite, bit 1 if any imaginary part is non-zero.
+int scan_vertex(const double* p, int64_t n, bool complex_values, Stream s);
+
 // Amplitude vectors: [T1 (v x o, row-major [a][i]) | T2 ((v o) x (v o), row-major [a][i][b][j])],
 // repeated once per plane (real plane, then imaginary plane for complex systems).
 struct AmpShape {
@@ -94,7 +98,8 @@ void dots(const double* x, const double* const* ys, int ny, int64_t n, double* o
 //   (i+1, next+1) and (next+1, i+1) for the valid slots listed in valid[];
 //   the (count+1)^2 corner is solved for rhs (-1, 0, ...) and coef_dev[j]
 //   receives the coefficient of slot (next + N - j) % N, j < count.
-//   status_dev[0] = 0 on success, 1 if the system is singular.
+//   status_dev[0] = 0 on success, 1 if the system is singular (zero pivot),
+//   2 if it holds a non-finite entry.
 void diis_solve(double* B, const double* dots_dev, const int* valid_host, int N, int next,
                 int count, double* coef_dev, int* status_dev, Stream s);
 

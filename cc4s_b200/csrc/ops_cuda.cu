@@ -201,6 +201,18 @@ __global__ void gather_vertex_kernel(double* out, const double* in, int cplx, in
   }
 }
 
+__global__ void scan_vertex_kernel(const double* p, int64_t n, int cplx, int* flags) {
+  int f = 0;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double x = p[e];
+    if (!isfinite(x)) f |= 1;
+    if (cplx && (e & 1) && x != 0.0) f |= 2;
+  }
+  f = __reduce_or_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
 struct JacobiArgs {
   double* Tnew; double* dT; const double* R; const double* Told;
   const double* eh; const double* ep;
@@ -532,7 +544,8 @@ __global__ void diis_solve_kernel(DiisArgs a) {
     double best = fabs(m[k][k]);
     for (int r = k + 1; r < dim; ++r)
       if (fabs(m[r][k]) > best) { best = fabs(m[r][k]); piv = r; }
-    if (best == 0.0 || !isfinite(best)) { singular = 1; break; }
+    if (!isfinite(best)) { singular = 2; break; }
+    if (best == 0.0) { singular = 1; break; }
     if (piv != k) {
       for (int c = 0; c < dim; ++c) { double t = m[k][c]; m[k][c] = m[piv][c]; m[piv][c] = t; }
       double t = x[k]; x[k] = x[piv]; x[piv] = t;
@@ -695,6 +708,24 @@ void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const
   jacobi_kernel<<<grid_for(sh.total(), 256), 256, 0, s>>>(a);
   CC_LAUNCH_CHECK();
   count();
+}
+
+int scan_vertex(const double* p, int64_t n, bool complex_values, Stream s) {
+  int* flags = reinterpret_cast<int*>(alloc(1));
+  int h = 0;
+  try {
+    CC_CHECK(cudaMemsetAsync(flags, 0, sizeof(int), s));
+    scan_vertex_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, n, complex_values ? 1 : 0, flags);
+    CC_LAUNCH_CHECK();
+    count();
+    CC_CHECK(cudaMemcpyAsync(&h, flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CC_CHECK(cudaStreamSynchronize(s));
+  } catch (...) {
+    release(flags);
+    throw;
+  }
+  release(flags);
+  return h;
 }
 
 void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, Stream s) {

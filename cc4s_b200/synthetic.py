@@ -3,7 +3,7 @@
 Occupied energies U[-1.5,-0.5] Eh, virtual U[0.2,3.0] Eh (sorted).  The vertex
 Gamma[G,p,q] has i.i.d. N(0, s^2) entries, s = 0.1 NG^(-1/4), drawn for p <= q
 and symmetrised (real, half-grid integral path) or made Hermitian (complex,
-real and imaginary parts each N(0, s^2/2)).
+real and imaginary parts each N(0, s^2/2)); it is returned column-major.
 """
 import math
 
@@ -26,13 +26,15 @@ def synthetic(No, Nv, NG, complex=False, seed=0):
     Np = No + Nv
     s = 0.1 * NG ** (-0.25)
     iu = np.triu_indices(Np)
+    # column-major (G fastest), the layout in which cc4s holds the vertex and the
+    # C ABI takes it, so handing it to the library needs no copy
     if not complex:
-        g = np.zeros((NG, Np, Np))
+        g = np.zeros((NG, Np, Np), order="F")
         vals = rng.standard_normal((NG, iu[0].size)) * s
         g[:, iu[0], iu[1]] = vals
         g[:, iu[1], iu[0]] = vals
         return eps_h, eps_p, g, True
-    g = np.zeros((NG, Np, Np), dtype=np.complex128)
+    g = np.zeros((NG, Np, Np), dtype=np.complex128, order="F")
     re = rng.standard_normal((NG, iu[0].size)) * (s / math.sqrt(2.0))
     im = rng.standard_normal((NG, iu[0].size)) * (s / math.sqrt(2.0))
     vals = re + 1j * im

@@ -337,7 +337,8 @@ void diis_solve(double* B, const double* dots_dev, const int* valid, int N, int 
     double best = std::fabs(m[k * dim + k]);
     for (int r = k + 1; r < dim; ++r)
       if (std::fabs(m[r * dim + k]) > best) { best = std::fabs(m[r * dim + k]); piv = r; }
-    if (best == 0.0 || !std::isfinite(best)) { singular = 1; break; }
+    if (!std::isfinite(best)) { singular = 2; break; }
+    if (best == 0.0) { singular = 1; break; }
     if (piv != k) {
       for (int c = 0; c < dim; ++c) std::swap(m[k * dim + c], m[piv * dim + c]);
       std::swap(x[k], x[piv]);
@@ -376,6 +377,16 @@ void lincomb(double* out, const double* const* xs, const double* const* ys, cons
 }
 
 void sum_partials_to(double*, const double*, int, int, Stream) {}
+
+int scan_vertex(const double* p, int64_t n, bool complex_values, Stream) {
+  ++g_ops;
+  int f = 0;
+  for (int64_t e = 0; e < n; ++e) {
+    if (!std::isfinite(p[e])) f |= 1;
+    if (complex_values && (e & 1) && p[e] != 0.0) f |= 2;
+  }
+  return f;
+}
 
 // Packed amplitude vectors: per plane [T1 | T2 rows r, columns r..n1-1].
 static int64_t packed_index(const AmpShape& sh, int64_t pl, int64_t r, int64_t c) {
