@@ -217,6 +217,8 @@ def run_ours(args, world, rank, local):
     o, v, G = CONFIG_SHAPES[cfg]
     inputs = config(cfg, seed=0)
     eh, ep, g, hg = inputs
+    if args.vertex_scale is not None:
+        g *= args.vertex_scale
     F = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS)
     K, W = args.steps, args.warmup
     base = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
@@ -315,6 +317,8 @@ def run_adjoint(args, local):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
     eh, ep, g, hg = config(cfg, seed=0)
+    scale = args.vertex_scale if args.vertex_scale is not None else 0.3
+    g *= scale
     # tight enough for 1e-6 differences at step 1e-5, loose enough that the DIIS
     # changes do not vanish (a singular DIIS system ends the reference's run too)
     opts = dict(maxIterations=100, energyConvergence=1e-11, amplitudesConvergence=1e-9,
@@ -345,6 +349,7 @@ def run_adjoint(args, local):
             "value": (info["vjp_seconds"] / fwd) if fwd else None, "unit": "x forward iteration",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d real, DIIS 5, FP64" % (cfg, o, v, G),
+                       "vertex_scale": scale,
                        "forward_iterations": r["iterations"], "forward_s_per_iter": fwd,
                        "energy": r["correlation"],
                        "lambda_iterations": info["iterations"], "lambda_converged": info["converged"],
@@ -360,8 +365,10 @@ def run_adjoint(args, local):
 
 def run_converge(args, local):
     """Accuracy of the split form at convergence: FP64, pure split and split with
-    FP64 refinement, each to energyConvergence 1e-10 (DIIS 5, at most 40
-    iterations); reports |E_split - E_fp64|, iterations and time to solution."""
+    FP64 refinement, each to energyConvergence 1e-10 (DIIS 5, at most 80
+    iterations); reports |E_split - E_fp64|, iterations and time to solution.
+    The synthetic vertex is scaled (default 0.3): unscaled, CCSD diverges at
+    these sizes."""
     import torch
     from cc4s_b200 import Solver
     from cc4s_b200.synthetic import config
@@ -369,7 +376,9 @@ def run_converge(args, local):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
     eh, ep, g, hg = config(cfg, seed=0)
-    base = dict(maxIterations=40, energyConvergence=1e-10, amplitudesConvergence=1e-8,
+    scale = args.vertex_scale if args.vertex_scale is not None else 0.3
+    g *= scale
+    base = dict(maxIterations=80, energyConvergence=1e-10, amplitudesConvergence=1e-8,
                 mixer=dict(type="DiisMixer", maxResidua=5), device=local)
     forms = {"fp64": {}, "split3": dict(precision="split3"),
              "split3_refined": dict(precision="split3", precisionRefinement=args.refine)}
@@ -392,7 +401,7 @@ def run_converge(args, local):
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, energyConvergence 1e-10"
                                    % (cfg, o, v, G, kind),
-                       "precision_refinement": args.refine},
+                       "precision_refinement": args.refine, "vertex_scale": scale},
             "forms": out}
 
 
@@ -437,6 +446,10 @@ def main():
                     help="converge FP64, split and refined split forms and compare energies")
     ap.add_argument("--refine", type=float, default=1e-5,
                     help="residuum norm below which the refined split form switches to FP64")
+    ap.add_argument("--vertex-scale", type=float, default=None,
+                    help="scale of the synthetic vertex (default 1; 0.3 for --converge and "
+                         "--adjoint: CCSD on the unscaled synthetic vertex diverges at these "
+                         "sizes, strongly correlated)")
     args = ap.parse_args()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
