@@ -192,6 +192,23 @@ def test_split_precision_k_panels(Solver, monkeypatch):
     assert _rel(R2, P2) < 1e-6 and _rel(R1, P1) < 1e-6
 
 
+def test_split_precision_refinement_reaches_fp64_energy(Solver):
+    """precisionRefinement: split iterations until the residuum norm is below
+    1e-5, FP64 after; the converged energy equals the FP64 form's to 1e-9 Eh."""
+    s = inputs.synthetic_system(10, 64, 150, seed=0)
+    o = dict(maxIterations=80, energyConvergence=1e-11, amplitudesConvergence=1e-9,
+             mixer=dict(type="DiisMixer", maxResidua=5))
+    runs = {}
+    for name, extra in (("fp64", {}), ("refined", dict(precision="split3", precisionRefinement=1e-5))):
+        sol = Solver(dict(o, **extra))
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+        runs[name] = sol.run()
+        sol.close()
+        assert runs[name]["converged"]
+    assert runs["refined"]["refined_from"] > 1
+    assert abs(runs["refined"]["correlation"] - runs["fp64"]["correlation"]) < TOL_E
+
+
 def test_split_precision_complex(Solver):
     """Complex path in the split form: residual within 1e-5 of the oracle, and the
     converged energy within 1 uEh of the FP64 form."""
