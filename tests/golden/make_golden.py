@@ -12,7 +12,7 @@ import warnings
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
 warnings.simplefilter("ignore")
 
-from oracle import coupled_cluster, inputs  # noqa: E402
+from oracle import coupled_cluster, inputs, triples  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -29,6 +29,10 @@ def c0():
                history_energy=[h["energy"] for h in r["history"]],
                history_dR=[h["dR"] for h in r["history"]],
                T1_norm=float((T1 ** 2).sum() ** 0.5), T2_norm=float((T2 ** 2).sum() ** 0.5))
+    # (T) at the converged amplitudes (tuple-loop restatement; the full-array
+    # restatement agrees on the smaller systems of the tests)
+    V = triples.triples_integrals(s)
+    out["triples"] = dict(correlation=triples.triples_atrip(T1, T2, V, s.eps_h, s.eps_p))
     json.dump(out, open(os.path.join(HERE, "c0_seed0.json"), "w"), indent=1)
 
 

@@ -7,7 +7,7 @@ import warnings
 import numpy as np
 import pytest
 
-from oracle import ccsd, ccsd_reference, coupled_cluster, inputs, mixers, properties
+from oracle import ccsd, ccsd_reference, coupled_cluster, inputs, mixers, properties, triples
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 warnings.simplefilter("ignore")
@@ -141,3 +141,43 @@ def test_linear_mixer():
     m.append((3 * np.ones(2), np.ones(1)), (np.zeros(2), np.zeros(1)))
     assert np.allclose(m.get()[0], 2.0)
     assert abs(m.getResiduumNorm() - np.sqrt(0.75)) < 1e-15
+
+
+def test_ueg_triples_pinned_to_reference_expected_output():
+    """Both (T) restatements, at the restated CCSD amplitudes of the UEG test,
+    reproduce the reference's expected PerturbativeTriplesReference energy
+    (complex path)."""
+    g = json.load(open(os.path.join(GOLDEN, "ueg_rs1.0_7occ_26virt.json")))
+    s = inputs.ueg_system(7, 26, 1.0)
+    r = coupled_cluster.run(s, **g["ccsd"]["options"])
+    T1, T2 = r["amplitudes"]
+    V = triples.triples_integrals(s)
+    ref = g["triples"]["energy"]["correlation"]
+    e_ctf = triples.triples_reference(T1, T2, V, s.eps_h, s.eps_p)
+    e_atrip = triples.triples_atrip(T1, T2, V, s.eps_h, s.eps_p)
+    assert abs(e_ctf - ref) < 1e-12, (e_ctf, ref)
+    assert abs(e_atrip - ref) < 1e-12, (e_atrip, ref)
+
+
+@pytest.mark.parametrize("shape", [(3, 8, 12), (4, 11, 20)])
+def test_triples_restatements_agree_real(shape):
+    """The array form (PerturbativeTriplesReference) and the tuple loop (atrip)
+    give the same real-path energy on arbitrary symmetric amplitudes."""
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, seed=Nv)
+    rng = np.random.default_rng(No)
+    T1, T2 = _rand_T(rng, Nv, No, scale=0.03)
+    V = triples.triples_integrals(s)
+    a = triples.triples_reference(T1, T2, V, s.eps_h, s.eps_p)
+    b = triples.triples_atrip(T1, T2, V, s.eps_h, s.eps_p)
+    assert abs(a - b) < 1e-13 * max(1.0, abs(a)), (a, b)
+
+
+def test_c0_triples_golden():
+    """The committed c0 (T) energy (self-made golden) from the converged oracle amplitudes."""
+    g = json.load(open(os.path.join(GOLDEN, "c0_seed0.json")))
+    s = inputs.config_system("c0", seed=0)
+    r = coupled_cluster.run(s, **g["options"])
+    T1, T2 = r["amplitudes"]
+    e = triples.triples_atrip(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    assert abs(e - g["triples"]["correlation"]) < 1e-10
