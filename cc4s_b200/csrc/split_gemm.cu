@@ -37,6 +37,7 @@ constexpr int TILE_BYTES = TM * TK * 2;           // 8 KB per slice tile
 constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;
 constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t WAIT_LIMIT = 1u << 28;         // bounded mbarrier waits
+constexpr int64_t RASTER_M = 8;                  // tile rows per raster group
 
 std::atomic<uint64_t> g_split_launches{0};
 
@@ -187,15 +188,13 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
@@ -226,7 +225,19 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
   __shared__ int abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * TM, n0 = static_cast<int64_t>(blockIdx.x) * TN;
+  // Tile order: groups of RASTER_M tile rows sweep the tile columns together, so
+  // the CTAs resident at one time share a few A row tiles and reuse each B tile
+  // RASTER_M times from L2 instead of streaming B from DRAM once per tile row.
+  int64_t m0, n0;
+  {
+    const int64_t nM = p.Mp / TM, nN = p.Np / TN, b = blockIdx.x;
+    const int64_t per_group = RASTER_M * nN, group = b / per_group;
+    const int64_t first = group * RASTER_M;
+    const int64_t rows = nM - first < RASTER_M ? nM - first : RASTER_M;
+    const int64_t in = b - group * per_group;
+    m0 = (first + in % rows) * TM;
+    n0 = (in / rows) * TN;
+  }
   const int nchunks = (p.nkb * TK + KCHUNK - 1) / KCHUNK;
   constexpr int KB_PER_CHUNK = KCHUNK / TK;
 
@@ -322,22 +333,22 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
       if (!mbar_wait(smem_u32(&bars[2 * NST]), c & 1)) { atomicExch(&abort_flag, 1); break; }
       tc_fence_after();
 #pragma unroll
-      for (int cb = 0; cb < 64; cb += 32) {
+      for (int cb = 0; cb < 64; cb += 16) {
         const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) +
                                static_cast<uint32_t>(64 * half + cb);
-        uint32_t g[32];
-        tmem_ld32(taddr, g);
+        uint32_t g[16];
+        tmem_ld16(taddr, g);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-12;
-        tmem_ld32(taddr + TN, g);
+        for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-12;
+        tmem_ld16(taddr + TN, g);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-23;
-        tmem_ld32(taddr + 2 * TN, g);
+        for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-23;
+        tmem_ld16(taddr + 2 * TN, g);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-34;
+        for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-34;
       }
       tc_fence_before();
       mbar_arrive(smem_u32(&bars[2 * NST + 1]));
@@ -374,6 +385,226 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
             const double v = T[r * LDT + cc];
             *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
           }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (abort_flag && threadIdx.x == 0) atomicExch(p.error, 1);
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent variant: one CTA per SM walks the tiles (same raster order), so
+// barrier set-up and TMEM allocation happen once, and the producer and the MMA
+// issuer run ahead into the next tile while the epilogue warps store the last
+// one.  TMEM is handed back after each chunk's drain as before; the stores use
+// warp-private transposes (32 rows x 16 columns, XOR-swizzled), so no barrier
+// spans warps and every warp leaves on an abort by a warp-uniform decision.
+constexpr int WBUF_DOUBLES = 32 * 16;
+constexpr int SMEM_BYTES_P = NST * STAGE_BYTES + 8 * WBUF_DOUBLES * 8 + 1024 + 256;
+
+__device__ __forceinline__ void tile_origin(const SplitParams& p, int64_t t, int64_t& m0,
+                                            int64_t& n0) {
+  const int64_t nM = p.Mp / TM, nN = p.Np / TN;
+  const int64_t per_group = RASTER_M * nN, group = t / per_group;
+  const int64_t first = group * RASTER_M;
+  const int64_t rows = nM - first < RASTER_M ? nM - first : RASTER_M;
+  const int64_t in = t - group * per_group;
+  m0 = (first + in % rows) * TM;
+  n0 = (in / rows) * TN;
+}
+
+__global__ void __launch_bounds__(320)
+split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
+                        const __grid_constant__ CUtensorMap tmB, SplitParams p) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  double* wbufs = reinterpret_cast<double*>(base + NST * STAGE_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NST * STAGE_BYTES + 8 * WBUF_DOUBLES * 8);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * NST + 2);
+  __shared__ int abort_flag;
+  volatile int* abort_v = &abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t ntiles = (p.Mp / TM) * (p.Np / TN);
+  const int nchunks = (p.nkb * TK + KCHUNK - 1) / KCHUNK;
+  constexpr int KB_PER_CHUNK = KCHUNK / TK;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(smem_u32(&bars[s]), 1);
+      mbar_init(smem_u32(&bars[NST + s]), 1);
+    }
+    mbar_init(smem_u32(&bars[2 * NST]), 1);
+    mbar_init(smem_u32(&bars[2 * NST + 1]), 256);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_u32(tmem_slot)), "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer: every k-block of every tile of this CTA ----
+    uint32_t it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && !*abort_v; t += gridDim.x) {
+      int64_t m0, n0;
+      tile_origin(p, t, m0, n0);
+      for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+        const int s = it % NST;
+        if (it >= NST && !mbar_wait(smem_u32(&bars[NST + s]), ((it / NST) - 1) & 1)) {
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        if (*abort_v) break;
+        const uint32_t full = smem_u32(&bars[s]);
+        mbar_expect_tx(full, STAGE_BYTES);
+        unsigned char* st = base + s * STAGE_BYTES;
+        for (int q = 0; q < NSLICE; ++q) {
+          tma_load_2d(smem_u32(st + q * TILE_BYTES), &tmA, full, kb * TK,
+                      static_cast<int>(q * p.Mp + m0));
+          tma_load_2d(smem_u32(st + (NSLICE + q) * TILE_BYTES), &tmB, full, kb * TK,
+                      static_cast<int>(q * p.Np + n0));
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: chunks of all tiles, global stage and chunk counters ----
+    uint32_t it = 0, q = 0;
+    for (int64_t t = blockIdx.x; t < ntiles && !*abort_v; t += gridDim.x) {
+      int kb = 0;
+      for (int c = 0; c < nchunks && !*abort_v; ++c, ++q) {
+        if (q > 0 && !mbar_wait(smem_u32(&bars[2 * NST + 1]), (q - 1) & 1)) {
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        tc_fence_after();
+        const int kb_end = min(p.nkb, (c + 1) * KB_PER_CHUNK);
+        bool first = true;
+        for (; kb < kb_end; ++kb, ++it) {
+          const int s = it % NST;
+          if (!mbar_wait(smem_u32(&bars[s]), (it / NST) & 1)) { atomicExch(&abort_flag, 1); break; }
+          tc_fence_after();
+          const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+#pragma unroll
+          for (int kk = 0; kk < TK / 16; ++kk) {
+            const uint32_t koff = kk * 32;
+            const uint32_t init = (first && kk == 0) ? 0u : 1u;
+            const uint64_t a1 = sdesc(st + 0 * TILE_BYTES + koff);
+            const uint64_t a2 = sdesc(st + 1 * TILE_BYTES + koff);
+            const uint64_t a3 = sdesc(st + 2 * TILE_BYTES + koff);
+            const uint64_t b12 = sdesc(st + (NSLICE + 0) * TILE_BYTES + koff);
+            const uint64_t b3 = sdesc(st + (NSLICE + 2) * TILE_BYTES + koff);
+            umma(tmem + 0 * TN, a1, b12, IDESC256, init);  // S1 x [S1|S2] -> groups 0, 1
+            umma(tmem + 2 * TN, a1, b3, IDESC128, init);   // S1 x S3      -> group 2
+            umma(tmem + 1 * TN, a2, b12, IDESC256, 1u);    // S2 x [S1|S2] -> groups 1, 2
+            umma(tmem + 2 * TN, a3, b12, IDESC128, 1u);    // S3 x S1      -> group 2
+          }
+          umma_commit(smem_u32(&bars[NST + s]));
+          first = false;
+        }
+        umma_commit(smem_u32(&bars[2 * NST]));
+      }
+    }
+  } else if (warp >= 2) {
+    // ---- epilogue: per tile, FP64 accumulation of every chunk, then the store ----
+    const int quad = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int row = quad * 32 + lane;
+    double* wb = wbufs + (warp - 2) * WBUF_DOUBLES;
+    const bool m_major = p.Cm.s_i == 1 && p.Cm.inner > 1;  // output contiguous along rows
+    uint32_t q = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      if (__any_sync(0xffffffffu, *abort_v != 0)) break;
+      int64_t m0, n0;
+      tile_origin(p, t, m0, n0);
+      double acc[64];
+#pragma unroll
+      for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+      bool ok = true;
+      for (int c = 0; c < nchunks; ++c, ++q) {
+        const bool got = mbar_wait(smem_u32(&bars[2 * NST]), q & 1);
+        if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+        tc_fence_after();
+#pragma unroll
+        for (int cb = 0; cb < 64; cb += 16) {
+          const uint32_t taddr = tmem + (static_cast<uint32_t>(quad * 32) << 16) +
+                                 static_cast<uint32_t>(64 * half + cb);
+          uint32_t g[16];
+          tmem_ld16(taddr, g);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-12;
+          tmem_ld16(taddr + TN, g);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-23;
+          tmem_ld16(taddr + 2 * TN, g);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) acc[cb + j] += static_cast<double>(__uint_as_float(g[j])) * 0x1p-34;
+        }
+        tc_fence_before();
+        mbar_arrive(smem_u32(&bars[2 * NST + 1]));  // TMEM free: the next chunk may start
+      }
+      if (!ok) { atomicExch(&abort_flag, 1); break; }
+      // store this warp's 32 rows x 64 columns (the MMA issuer is already on the next tile)
+      const int64_t m = m0 + row;
+      const double sa = m < p.M ? ldexp(p.alpha, p.ea[m]) : 0.0;
+      const int64_t rowoff = m < p.M ? p.Cm.off(static_cast<uint32_t>(m)) : 0;
+      const int64_t rowoff2 = (m < p.M && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
+      if (m_major) {
+        // lanes are consecutive rows: store column by column straight from registers
+#pragma unroll
+        for (int j = 0; j < 64; ++j) {
+          const int64_t n = n0 + 64 * half + j;
+          if (m >= p.M || n >= p.N) continue;
+          const double v = acc[j] * sa * ldexp(1.0, p.eb[n]);
+          double* ptr = p.C + rowoff + p.Cn.off(static_cast<uint32_t>(n));
+          *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+          if (p.C2) {
+            double* p2 = p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n));
+            *p2 = p.beta != 0.0 ? v + p.beta * *p2 : v;
+          }
+        }
+      } else {
+        // 16-column pieces through the warp's buffer; lanes then run along columns
+#pragma unroll
+        for (int piece = 0; piece < 4; ++piece) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int64_t n = n0 + 64 * half + 16 * piece + j;
+            const double v = (m < p.M && n < p.N) ? acc[16 * piece + j] * sa * ldexp(1.0, p.eb[n]) : 0.0;
+            wb[lane * 16 + (j ^ (lane & 15))] = v;
+          }
+          __syncwarp();
+#pragma unroll 4
+          for (int k = 0; k < 16; ++k) {
+            const int r = 2 * k + (lane >> 4), cc = lane & 15;  // row within the warp, column
+            const int64_t mm = m0 + quad * 32 + r;
+            const int64_t nn = n0 + 64 * half + 16 * piece + cc;
+            if (mm >= p.M || nn >= p.N) continue;
+            const double v = wb[r * 16 + (cc ^ (r & 15))];
+            double* ptr = p.C + p.Cm.off(static_cast<uint32_t>(mm)) + p.Cn.off(static_cast<uint32_t>(nn));
+            *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+            if (p.C2) {
+              double* p2 = p.C2 + p.C2m.off(static_cast<uint32_t>(mm)) + p.C2n.off(static_cast<uint32_t>(nn));
+              *p2 = p.beta != 0.0 ? v + p.beta * *p2 : v;
+            }
+          }
+          __syncwarp();
         }
       }
     }
@@ -573,13 +804,33 @@ void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
   sp.alpha = g.alpha; sp.beta = g.beta;
   sp.ea = aexp; sp.eb = bexp;
   sp.error = ws.error;
-  static bool configured = false;
-  if (!configured) {
-    CC_CHECK(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    configured = true;
+  const int64_t tiles = (L.Np / TN) * (L.Mp / TM);
+  if (tiles >= (int64_t(1) << 31)) throw Error(ERR_BAD_SHAPE, "gemm_split: too many tiles");
+  // Persistent tile loop by default; CC4S_SPLIT_PERSISTENT=0 selects one tile per CTA.
+  static const bool persistent = [] {
+    const char* e = std::getenv("CC4S_SPLIT_PERSISTENT");
+    return !(e && e[0] == '0');
+  }();
+  if (persistent) {
+    static int sms = 0;
+    if (!sms) {
+      int dev = 0;
+      CC_CHECK(cudaGetDevice(&dev));
+      CC_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      CC_CHECK(cudaFuncSetAttribute(split_kernel_persistent,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES_P));
+    }
+    dim3 grid(static_cast<unsigned>(std::min<int64_t>(tiles, sms)));
+    split_kernel_persistent<<<grid, 320, SMEM_BYTES_P, s>>>(ta, tb, sp);
+  } else {
+    static bool configured = false;
+    if (!configured) {
+      CC_CHECK(cudaFuncSetAttribute(split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+      configured = true;
+    }
+    dim3 grid(static_cast<unsigned>(tiles));
+    split_kernel<<<grid, 320, SMEM_BYTES, s>>>(ta, tb, sp);
   }
-  dim3 grid(static_cast<unsigned>(L.Np / TN), static_cast<unsigned>(L.Mp / TM));
-  split_kernel<<<grid, 320, SMEM_BYTES, s>>>(ta, tb, sp);
   CC_LAUNCH_CHECK();
   g_split_launches.fetch_add(1);
 }
