@@ -31,7 +31,8 @@ EXPORTS = [
     "cc4s_cc_default_options", "cc4s_cc_create", "cc4s_cc_set_inputs",
     "cc4s_cc_set_initial_amplitudes", "cc4s_cc_run", "cc4s_cc_get_amplitudes",
     "cc4s_cc_residual", "cc4s_cc_backward", "cc4s_cc_residual_vjp", "cc4s_cc_relaxed_gradient",
-    "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
+    "cc4s_cc_triples_default_options", "cc4s_cc_perturbative_triples",
+    "cc4s_cc_fsc_default_options", "cc4s_cc_finite_size_correction", "cc4s_cc_get_stats", "cc4s_cc_energy_noalloc", "cc4s_cc_destroy",
     "cc4s_cc_last_error",
 ]
 
@@ -80,6 +81,31 @@ class LambdaResult(ctypes.Structure):
     ]
 
 
+class TriplesOptions(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int64), ("formulation", ctypes.c_int)]
+
+
+class TriplesResult(ctypes.Structure):
+    _fields_ = [
+        ("correlation", ctypes.c_double), ("seconds", ctypes.c_double),
+        ("setup_seconds", ctypes.c_double), ("flops", ctypes.c_double),
+        ("executed_flops", ctypes.c_double), ("block_size", ctypes.c_int64),
+        ("block_triples", ctypes.c_int64), ("phase_seconds", ctypes.c_double * 4),
+    ]
+
+
+class FscOptions(ctypes.Structure):
+    _fields_ = [("interpolation_grid_size", ctypes.c_int), ("unit_factor", ctypes.c_double)]
+
+
+class FscResult(ctypes.Structure):
+    _fields_ = [
+        ("correction", ctypes.c_double), ("uncorrected", ctypes.c_double),
+        ("corrected", ctypes.c_double), ("seconds", ctypes.c_double),
+        ("box", ctypes.c_int64 * 3),
+    ]
+
+
 _LIBS = {}
 
 
@@ -109,6 +135,12 @@ def load(path=None):
     lib.cc4s_cc_residual_vjp.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, dp, dp, dp]
     lib.cc4s_cc_relaxed_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, dp,
                                              P(LambdaResult)]
+    lib.cc4s_cc_triples_default_options.argtypes = [P(TriplesOptions)]
+    lib.cc4s_cc_perturbative_triples.argtypes = [ctypes.c_void_p, P(TriplesOptions),
+                                                 P(TriplesResult)]
+    lib.cc4s_cc_fsc_default_options.argtypes = [P(FscOptions)]
+    lib.cc4s_cc_finite_size_correction.argtypes = [ctypes.c_void_p, dp, ctypes.c_int64, dp, dp, dp,
+                                                   P(FscOptions), dp, P(FscResult)]
     lib.cc4s_cc_energy_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p]
@@ -117,6 +149,8 @@ def load(path=None):
     lib.cc4s_cc_last_error.restype = ctypes.c_char_p
     for name in EXPORTS[1:-1]:
         getattr(lib, name).restype = ctypes.c_int
+    lib.cc4s_cc_triples_default_options.restype = None
+    lib.cc4s_cc_fsc_default_options.restype = None
     _LIBS[path] = lib
     return lib
 

@@ -8,7 +8,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcc4s_b200.so")
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["gemm_f64.cu", "split_gemm.cu", "ops_cuda.cu", "schedule.cpp", "ccsd_real.cpp",
-           "ccsd_complex.cpp", "drccd.cpp", "driver.cpp", "abi.cpp", "energy_noalloc.cu"]
+           "ccsd_complex.cpp", "drccd.cpp", "driver.cpp", "abi.cpp", "energy_noalloc.cu",
+           "triples.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]

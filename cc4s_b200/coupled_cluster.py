@@ -198,6 +198,48 @@ class Solver:
                     vjp_seconds=res.vjp_seconds, gradient_seconds=res.gradient_seconds)
         return self._vertex_grad(g), info
 
+    def perturbative_triples(self, block_size=0, reference_form=False):
+        """(T) energy at the current amplitudes (cc4s_cc_perturbative_triples);
+        reference_form: the conjugation of PerturbativeTriplesReference (complex path)."""
+        o = _abi.TriplesOptions()
+        self.lib.cc4s_cc_triples_default_options(ctypes.byref(o))
+        o.block_size = int(block_size)
+        o.formulation = 1 if reference_form else 0
+        r = _abi.TriplesResult()
+        self._check(self.lib.cc4s_cc_perturbative_triples(self.h, ctypes.byref(o),
+                                                          ctypes.byref(r)))
+        return dict(correlation=r.correlation, seconds=r.seconds,
+                    setup_seconds=r.setup_seconds, flops=r.flops,
+                    executed_flops=r.executed_flops, block_size=r.block_size,
+                    block_triples=r.block_triples,
+                    phase_seconds=dict(zip(("singles", "particle", "hole", "energy"),
+                                           list(r.phase_seconds))))
+
+    def finite_size_correction(self, grid, reciprocal_basis, singular_vectors=None,
+                               coulomb_potential=None, grid_size=20, unit_factor=1.0):
+        """FiniteSizeCorrection at the current amplitudes (cc4s_cc_finite_size_correction).
+        grid [NGG, 3] cartesian G vectors; reciprocal_basis [3, 3] rows Gi, Gj, Gk;
+        singular_vectors U [NGG, NG] (None: identity); coulomb_potential V [NGG].
+        Returns (energy dict, S(G))."""
+        grid = np.ascontiguousarray(grid, dtype=np.float64)
+        NGG = grid.shape[0]
+        B = np.ascontiguousarray(reciprocal_basis, dtype=np.float64).reshape(9)
+        U = None
+        if singular_vectors is not None:
+            U = np.asarray(singular_vectors, dtype=np.complex128).reshape(-1, order="F").view(np.float64)
+        V = None if coulomb_potential is None else np.ascontiguousarray(coulomb_potential, dtype=np.float64)
+        o = _abi.FscOptions()
+        self.lib.cc4s_cc_fsc_default_options(ctypes.byref(o))
+        o.interpolation_grid_size = int(grid_size)
+        o.unit_factor = float(unit_factor)
+        S = np.empty(NGG)
+        r = _abi.FscResult()
+        self._check(self.lib.cc4s_cc_finite_size_correction(
+            self.h, _abi.ptr(U), NGG, _abi.ptr(V), _abi.ptr(grid), _abi.ptr(B), ctypes.byref(o),
+            _abi.ptr(S), ctypes.byref(r)))
+        return (dict(correction=r.correction, uncorrected=r.uncorrected, corrected=r.corrected,
+                     seconds=r.seconds, box=list(r.box)), S)
+
     def stats(self):
         s = _abi.Stats()
         self._check(self.lib.cc4s_cc_get_stats(self.h, ctypes.byref(s)))
@@ -258,3 +300,71 @@ class CoupledCluster:
         return {"energy": energy, "convergenceReached": r["converged"],
                 "amplitudes": {"ph": T1, "pphh": T2}, "iterations": r["iterations"],
                 "history": r["history"]}
+
+
+class PerturbativeTriples:
+    """The cc4s ``PerturbativeTriples`` / ``PerturbativeTriplesReference`` step.
+
+    ``arguments`` holds the reference's input keys (PerturbativeTriples.cxx:27-255,
+    PerturbativeTriplesReference.cxx:56-222): amplitudes ({'ph': T1,
+    'pphh': T2}), slicedEigenEnergies, slicedCoulombVertex or coulombVertex
+    (the integral slices are formed on the device, so coulombIntegrals is not
+    needed), halfGrid; plus precision ('fp64' or 'split3'), blockSize and
+    referenceForm (the complex-path conjugation of PerturbativeTriplesReference;
+    the pipeline sets it for that step name).
+    Returns {'energy': {'correlation', 'unit'}} like the reference.
+    """
+
+    def __init__(self, lib=None):
+        self.lib = lib
+
+    def run(self, arguments):
+        eps = arguments["slicedEigenEnergies"]
+        gamma = _full_vertex(arguments)
+        half_grid = bool(arguments.get("halfGrid", not np.iscomplexobj(gamma)))
+        amps = arguments["amplitudes"]
+        s = Solver(arguments, lib=self.lib)
+        try:
+            s.set_inputs(eps["h"], eps["p"], gamma, half_grid=half_grid)
+            s.set_initial_amplitudes(amps["ph"], amps["pphh"])
+            r = s.perturbative_triples(int(arguments.get("blockSize", 0) or 0),
+                                       reference_form=bool(arguments.get("referenceForm", False)))
+        finally:
+            s.close()
+        return {"energy": {"correlation": r["correlation"], "unit": 1.0}, "stats": r}
+
+
+class FiniteSizeCorrection:
+    """The cc4s ``FiniteSizeCorrection`` step (FiniteSizeCorrection.cxx:28-310).
+
+    ``arguments``: amplitudes ({'ph', 'pphh'}), slicedEigenEnergies,
+    slicedCoulombVertex or coulombVertex, halfGrid, coulombVertexSingularVectors
+    (U [G, F]; optional here, identity if absent), coulombPotential (V [G];
+    optional, 1), gridVectors ([G, 3] cartesian), reciprocalBasis ([3, 3], the
+    rows Gi, Gj, Gk of the gridVectors metaData), interpolationGridSize (20),
+    unitFactor (1).  Returns {'energy': {correction, uncorrected, corrected,
+    unit}, 'transitionStructureFactor': S(G)}.
+    """
+
+    def __init__(self, lib=None):
+        self.lib = lib
+
+    def run(self, arguments):
+        eps = arguments["slicedEigenEnergies"]
+        gamma = _full_vertex(arguments)
+        half_grid = bool(arguments.get("halfGrid", not np.iscomplexobj(gamma)))
+        amps = arguments["amplitudes"]
+        s = Solver(arguments, lib=self.lib)
+        try:
+            s.set_inputs(eps["h"], eps["p"], gamma, half_grid=half_grid)
+            s.set_initial_amplitudes(amps["ph"], amps["pphh"])
+            e, S = s.finite_size_correction(
+                arguments["gridVectors"], arguments["reciprocalBasis"],
+                arguments.get("coulombVertexSingularVectors"), arguments.get("coulombPotential"),
+                int(arguments.get("interpolationGridSize", 20)),
+                float(arguments.get("unitFactor", 1.0)))
+        finally:
+            s.close()
+        return {"energy": {"correction": e["correction"], "uncorrected": e["uncorrected"],
+                           "corrected": e["corrected"], "unit": 1.0},
+                "transitionStructureFactor": S, "stats": e}

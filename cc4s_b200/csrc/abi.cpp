@@ -1,4 +1,5 @@
 // Iteration loop (CoupledCluster::run) and the extern "C" entry points.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <complex>
@@ -453,6 +454,124 @@ struct cc4s_cc_handle {
   Handle* impl;
 };
 
+// Perturbative triples at the current amplitudes (triples.h).  The schedule
+// and its integral slices live for this call only.
+void Handle::triples(const cc4s_cc_triples_options& o, cc4s_cc_triples_result* out) {
+  require_inputs();
+  if (!have_T) throw Error(ERR_STATE, "no amplitudes: run the CoupledCluster step or set initial amplitudes first");
+  if (o.block_size < 0) throw Error(ERR_INVALID_ARGUMENT, "block_size < 0");
+  if (o.formulation != 0 && o.formulation != 1)
+    throw Error(ERR_INVALID_ARGUMENT, "formulation must be 0 or 1");
+  TriplesOptions to;
+  to.block = o.block_size;
+  to.reference_form = o.formulation == 1;
+  Triples tr(sys, complex_path ? &csys : nullptr, to, stream);
+  tr.set_precision(opt.precision == CC4S_PRECISION_SPLIT3 ? 3 : 0);
+  tr.set_profile(opt.profile != 0);
+  const TriplesOutcome r = tr.run(Tcur);
+  if (!std::isfinite(r.energy)) throw Error(ERR_NON_FINITE, "non-finite (T) energy");
+  out->correlation = r.energy;
+  out->seconds = r.seconds;
+  out->setup_seconds = r.setup_seconds;
+  out->flops = r.flops;
+  out->executed_flops = r.executed_flops;
+  out->block_size = r.block;
+  out->block_triples = r.block_triples;
+  for (int k = 0; k < 4; ++k) out->phase_seconds[k] = r.phase_seconds[k];
+}
+
+// Finite-size correction at the current amplitudes: the plane-wave structure
+// factor S(G) on the device (Schedule::structure_factor_pw), then the lattice
+// box and the two energy sums of FiniteSizeCorrection::interpolation
+// (FiniteSizeCorrection.cxx:135-310).  The box geometry comes from the grid
+// vectors on the host, as the reference derives it.
+void Handle::finite_size_correction(const double* U, int64_t NGG, const double* V,
+                                    const double* grid, const double* recip,
+                                    const cc4s_cc_fsc_options& o, double* S_out,
+                                    cc4s_cc_fsc_result* out) {
+  require_inputs();
+  if (!have_T) throw Error(ERR_STATE, "no amplitudes: run the CoupledCluster step or set initial amplitudes first");
+  if (!grid || !recip) throw Error(ERR_INVALID_ARGUMENT, "null grid vectors or reciprocal basis");
+  if (NGG <= 0) throw Error(ERR_BAD_SHAPE, "NGG must be positive");
+  if (!U && NGG != in_NG) throw Error(ERR_BAD_SHAPE, "without singular vectors NGG must equal NG");
+  if (o.interpolation_grid_size <= 0) throw Error(ERR_INVALID_ARGUMENT, "interpolationGridSize <= 0");
+  const int64_t NF = in_NG;
+  // geometry (host): inverse basis, cell volume, box of the lattice coordinates
+  ops::FscGeometry g;
+  double B[3][3], A[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) B[r][c] = recip[3 * r + c];
+  auto cross = [](const double* a, const double* b, double* out3) {
+    out3[0] = a[1] * b[2] - a[2] * b[1];
+    out3[1] = a[2] * b[0] - a[0] * b[2];
+    out3[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double c01[3], c12[3], c20[3];
+  cross(B[0], B[1], c01); cross(B[1], B[2], c12); cross(B[2], B[0], c20);
+  const double omega = std::fabs(c01[0] * B[2][0] + c01[1] * B[2][1] + c01[2] * B[2][2]);
+  if (!(omega > 0.0) || !std::isfinite(omega)) throw Error(ERR_INVALID_ARGUMENT, "degenerate reciprocal basis");
+  for (int c = 0; c < 3; ++c) { A[0][c] = c12[c] / omega; A[1][c] = c20[c] / omega; A[2][c] = c01[c] / omega; }
+  double dmin[3] = {0, 0, 0}, dmax[3] = {0, 0, 0};
+  for (int64_t i = 0; i < NGG; ++i)
+    for (int d = 0; d < 3; ++d) {
+      const double x = A[d][0] * grid[3 * i] + A[d][1] * grid[3 * i + 1] + A[d][2] * grid[3 * i + 2];
+      if (!std::isfinite(x)) throw Error(ERR_NON_FINITE, "non-finite grid vector");
+      dmin[d] = std::min(dmin[d], x);
+      dmax[d] = std::max(dmax[d], x);
+    }
+  int64_t cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    g.dims[d] = static_cast<int64_t>(std::floor(dmax[d] - dmin[d] + 1.5));
+    g.origin[d] = std::floor(dmin[d] + 0.5);
+    if (g.dims[d] < 4) throw Error(ERR_BAD_SHAPE, "interpolation box needs at least 4 points per direction");
+    cells *= g.dims[d];
+    if (cells > (int64_t(1) << 31)) throw Error(ERR_BAD_SHAPE, "interpolation box too large");
+  }
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) { g.A[3 * r + c] = A[r][c]; g.B[3 * r + c] = B[r][c]; }
+  g.NG = NGG;
+  g.N = o.interpolation_grid_size;
+  g.f = o.unit_factor * omega / 2.0 / M_PI / M_PI;
+  std::vector<double*> tmp;
+  auto tk = [&](int64_t n) { double* p = ops::alloc(n); tmp.push_back(p); return p; };
+  try {
+    double* Uw = tk(2 * NGG * NF);
+    double* Ud = U ? tk(2 * NGG * NF) : nullptr;
+    double* Vd = V ? tk(NGG) : nullptr;
+    double* Sd = tk(NGG);
+    double* gd = tk(3 * NGG);
+    double* box = tk(cells);
+    double* red = tk(2048);
+    double* sums = tk(2);
+    ops::event_record(ev0, stream);
+    if (Ud) ops::h2d(Ud, U, 2 * NGG * NF, stream);
+    if (Vd) ops::h2d(Vd, V, NGG, stream);
+    ops::h2d(gd, grid, 3 * NGG, stream);
+    ops::fsc_prepare_u(Uw, Uw + NGG * NF, Ud, Vd, NGG, NF, stream);
+    solver->structure_factor_pw(Tcur, Uw, NGG, NF, Sd);
+    ops::fsc_box(box, Sd, gd, g, stream);
+    ops::fsc_sums(box, Sd, gd, g, red, sums, stream);
+    double h[2];
+    ops::d2h(h, sums, 2, stream);
+    if (S_out) ops::d2h(S_out, Sd, NGG, stream);
+    ops::event_record(ev1, stream);
+    out->seconds = ops::event_ms(ev0, ev1) * 1e-3;
+    ops::sync(stream);
+    if (solver->device_error()) throw Error(ERR_TIMEOUT, "tensor-core kernel wait expired");
+    const double N3 = double(g.N) * g.N * g.N;
+    out->uncorrected = h[0];
+    out->corrected = h[1] / N3 / 8.0;
+    out->correction = out->corrected - out->uncorrected;
+    for (int d = 0; d < 3; ++d) out->box[d] = g.dims[d];
+    if (!std::isfinite(out->corrected) || !std::isfinite(out->uncorrected))
+      throw Error(ERR_NON_FINITE, "non-finite finite-size correction");
+  } catch (...) {
+    for (double* p : tmp) ops::release(p);
+    throw;
+  }
+  for (double* p : tmp) ops::release(p);
+}
+
 namespace {
 thread_local std::string g_create_error;
 
@@ -563,6 +682,40 @@ int cc4s_cc_relaxed_gradient(cc4s_cc_handle* h, int max_iterations, double conve
   return guarded(h, [&] {
     h->impl->relaxed_gradient(max_iterations, convergence, dE_dGamma, out);
     return out->converged ? 0 : static_cast<int>(CC4S_WARN_NOT_CONVERGED);
+  });
+}
+
+void cc4s_cc_triples_default_options(cc4s_cc_triples_options* o) {
+  if (!o) return;
+  o->block_size = 0;
+  o->formulation = 0;
+}
+
+int cc4s_cc_perturbative_triples(cc4s_cc_handle* h, const cc4s_cc_triples_options* opt,
+                                 cc4s_cc_triples_result* out) {
+  if (!h || !h->impl || !opt || !out) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] {
+    h->impl->triples(*opt, out);
+    return 0;
+  });
+}
+
+void cc4s_cc_fsc_default_options(cc4s_cc_fsc_options* o) {
+  if (!o) return;
+  o->interpolation_grid_size = 20;
+  o->unit_factor = 1.0;
+}
+
+int cc4s_cc_finite_size_correction(cc4s_cc_handle* h, const double* singular_vectors,
+                                   int64_t NGG, const double* coulomb_potential,
+                                   const double* grid_vectors, const double* reciprocal_basis,
+                                   const cc4s_cc_fsc_options* opt, double* S_of_G,
+                                   cc4s_cc_fsc_result* out) {
+  if (!h || !h->impl || !opt || !out) return CC4S_ERR_INVALID_ARGUMENT;
+  return guarded(h, [&] {
+    h->impl->finite_size_correction(singular_vectors, NGG, coulomb_potential, grid_vectors,
+                                    reciprocal_basis, *opt, S_of_G, out);
+    return 0;
   });
 }
 

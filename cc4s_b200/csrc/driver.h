@@ -10,6 +10,7 @@
 #include "drccd.h"
 #include "ccsd_real.h"
 #include "ops.h"
+#include "triples.h"
 
 namespace cc4s_b200 {
 
@@ -44,6 +45,12 @@ struct Handle {
                     double* T1b, double* T2b, double* dGamma);
   void relaxed_gradient(int max_iterations, double convergence, double* dE_dGamma,
                         cc4s_cc_lambda_result* out);
+  // finite-size correction (structure factor + interpolation) at the current amplitudes
+  void finite_size_correction(const double* U, int64_t NGG, const double* V, const double* grid,
+                              const double* recip, const cc4s_cc_fsc_options& o, double* S_out,
+                              cc4s_cc_fsc_result* out);
+  // perturbative triples at the current amplitudes
+  void triples(const cc4s_cc_triples_options& o, cc4s_cc_triples_result* out);
 
   cc4s_cc_options opt;
   Stream stream = nullptr;

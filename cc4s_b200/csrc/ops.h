@@ -122,6 +122,63 @@ void lincomb_packed(double* out, const double* const* xs, const double* const* y
 // Small host-visible scalars.
 void sum_partials_to(double* dst_dev, const double* ws, int nparts, int nvals, Stream s);
 
+// ---- finite-size correction ---------------------------------------------------
+// Planar singular vectors for the structure factor: out_re/out_im [NGG][NF] =
+// U[G,F] / sqrt(V[G]) from the caller's column-major complex-interleaved U[G,F]
+// (U == null: the identity, NGG == NF; V == null: 1).
+void fsc_prepare_u(double* out_re, double* out_im, const double* U, const double* V,
+                   int64_t NGG, int64_t NF, Stream s);
+// Complex NF x NF matrix from the stacked real one of the real path: rows and
+// columns [0, NF) hold the real parts, [NF, 2 NF) the imaginary parts of the
+// vertex rows (parts == 2; parts == 1: no imaginary rows):
+//   Q = Qs[F][F'] + Qs[F+][F'+] + i (Qs[F][F'+] - Qs[F+][F']).
+void fsc_stacked_to_complex(double* Q_re, double* Q_im, const double* Qs, int64_t NF, int parts,
+                            Stream s);
+// Lattice box of the interpolation: box[x + nx (y + ny z)] = S[g] at the integer
+// coordinates round(A . G_g) - origin of each grid vector (other points 0).
+struct FscGeometry {
+  double A[9];      // rows: inverse of the reciprocal basis (direct coordinates)
+  double B[9];      // rows: the reciprocal basis Gi, Gj, Gk
+  double origin[3];
+  int64_t dims[3];
+  int64_t NG;       // grid vectors
+  int N;            // interpolationGridSize
+  double f;         // Omega / (2 pi^2) times the unit factors
+};
+void fsc_box(double* box, const double* S, const double* grid, const FscGeometry& g, Stream s);
+// out_dev[0] = sum_{|G| >= 1e-8} f S(G) / |G|^2 (uncorrected),
+// out_dev[1] = sum over the (2N)^3 NG refined points g != 0 of f S_int(A.g) / |g|^2,
+// S_int the Catmull-Rom tricubic interpolation of the box.  ws >= 2 * 148 * 4 doubles.
+void fsc_sums(const double* box, const double* S, const double* grid, const FscGeometry& g,
+              double* ws, double* out_dev, Stream s);
+
+// ---- perturbative triples ---------------------------------------------------
+// One block of the (T) loop: virtual indices a, b, c from three blocks, all
+// holes.  The block array is S[q1][q2][q3] with q = local pair index x*o + y
+// (x the virtual index within its block, y the hole index); pair q of position
+// m is the global pair P[m] + q (= (a, i) -> a*o + i, the layout of T1 rows
+// and of the pair-layout integrals V[(a,i),(b,j)], n1 = v*o).
+struct TriplesBlock {
+  int64_t o = 0, n1 = 0;
+  int64_t P[3] = {0, 0, 0};  // global pair offset of each position (block start * o)
+  int64_t L[3] = {0, 0, 0};  // pairs per position (block length * o)
+};
+// S[q] = t[p1] V[p2][p3] + t[p2] V[p1][p3] + t[p3] V[p1][p2]  (p = P + q): the
+// disconnected (singles) part, written before the connected terms accumulate.
+// Complex: planar operands, imaginary planes S_im, t1_im, V_im (all null on the
+// real path); the products are plain complex products.
+void triples_singles(double* S, double* S_im, const double* t1, const double* t1_im,
+                     const double* V, const double* V_im, const TriplesBlock& b, Stream s);
+// With W = S - singles, D = eps_i + eps_j + eps_k - eps_a - eps_b - eps_c and
+// Y(q) = sum_pi coef[pi] S(q o pi), where S(q o pi) takes the hole indices of the
+// three pairs in the order pi (pi over the six permutations 012, 021, 102, 120,
+// 201, 210):  out_dev[0] = sum_q Re W Re Y / D,  out_dev[1] = sum_q Im W Im Y / D.
+// ws holds the partial sums (>= 2 * 148 * 4 doubles).
+void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                    const double* V, const double* V_im, const double* eps_h,
+                    const double* eps_p, const TriplesBlock& b, const double coef[6],
+                    double* ws, double* out_dev, Stream s);
+
 // Number of bandwidth-kernel launches issued so far.
 uint64_t launch_count();
 

@@ -844,5 +844,304 @@ void lincomb(double* out, const double* const* xs, const double* const* ys,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Finite-size correction: planar singular vectors, the stacked-to-complex fold
+// of the real path, the lattice box of S(G) and the two energy sums.
+__global__ void fsc_prepare_u_kernel(double* ore, double* oim, const double* U, const double* V,
+                                     int64_t NGG, int64_t NF) {
+  const int64_t total = NGG * NF;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t F = e / NGG, G = e - F * NGG;  // reads along the caller's G-fastest layout
+    double re, im;
+    if (U) {
+      re = U[2 * e];
+      im = U[2 * e + 1];
+    } else {
+      re = G == F ? 1.0 : 0.0;
+      im = 0.0;
+    }
+    const double sc = V ? 1.0 / sqrt(V[G]) : 1.0;
+    ore[G * NF + F] = re * sc;
+    oim[G * NF + F] = im * sc;
+  }
+}
+
+__global__ void fsc_stacked_kernel(double* Qr, double* Qi, const double* Qs, int64_t NF,
+                                   int parts) {
+  const int64_t total = NF * NF, S2 = parts * NF;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t F = e / NF, Fp = e - F * NF;
+    if (parts == 2) {
+      Qr[e] = Qs[F * S2 + Fp] + Qs[(F + NF) * S2 + Fp + NF];
+      Qi[e] = Qs[F * S2 + Fp + NF] - Qs[(F + NF) * S2 + Fp];
+    } else {
+      Qr[e] = Qs[e];
+      Qi[e] = 0.0;
+    }
+  }
+}
+
+__device__ __forceinline__ void fsc_direct(const FscGeometry& g, const double v[3], double x[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] = g.A[3 * d] * v[0] + g.A[3 * d + 1] * v[1] + g.A[3 * d + 2] * v[2];
+}
+
+__global__ void fsc_box_kernel(double* box, const double* S, const double* grid, FscGeometry g) {
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < g.NG;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v[3] = {grid[3 * e], grid[3 * e + 1], grid[3 * e + 2]};
+    double x[3];
+    fsc_direct(g, v, x);
+    int64_t i[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) i[d] = static_cast<int64_t>(floor(x[d] + 0.5) - g.origin[d]);
+    box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
+  }
+}
+
+// Catmull-Rom tricubic value of the box at direct coordinates x (unit spacing):
+// index truncated toward zero and clamped, 4 x 4 x 4 neighbourhood from one
+// below it with clamped indices, weights BLEND (1, t, t^2, t^3).
+__device__ double fsc_tricubic(const double* box, const FscGeometry& g, const double x[3]) {
+  const double BLEND[4][4] = {{0.0, -0.5, 1.0, -0.5},
+                              {1.0, 0.0, -2.5, 1.5},
+                              {0.0, 0.5, 2.0, -1.5},
+                              {0.0, 0.0, -0.5, 0.5}};
+  double w[3][4];
+  int64_t base[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double t = x[d] - g.origin[d];
+    int64_t i = static_cast<int64_t>(t);
+    i = i < 0 ? 0 : (i >= g.dims[d] ? g.dims[d] - 1 : i);
+    const double u = t - static_cast<double>(i);
+    const double pw[4] = {1.0, u, u * u, u * u * u};
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      w[d][r] = BLEND[r][0] * pw[0] + BLEND[r][1] * pw[1] + BLEND[r][2] * pw[2] + BLEND[r][3] * pw[3];
+    base[d] = i - 1;
+  }
+  double total = 0.0;
+  for (int sl = 0; sl < 4; ++sl) {
+    int64_t z = base[2] + sl;
+    z = z < 0 ? 0 : (z > g.dims[2] - 1 ? g.dims[2] - 1 : z);
+    for (int r = 0; r < 4; ++r) {
+      int64_t y = base[1] + r;
+      y = y < 0 ? 0 : (y > g.dims[1] - 1 ? g.dims[1] - 1 : y);
+      const double* row = box + g.dims[0] * (y + g.dims[1] * z);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        int64_t xx = base[0] + c;
+        xx = xx < 0 ? 0 : (xx > g.dims[0] - 1 ? g.dims[0] - 1 : xx);
+        total += w[0][c] * w[1][r] * w[2][sl] * row[xx];
+      }
+    }
+  }
+  return total;
+}
+
+__global__ void fsc_sums_kernel(const double* box, const double* S, const double* grid,
+                                FscGeometry g, double* ws) {
+  double acc[2] = {0.0, 0.0};
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t first = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  for (int64_t e = first; e < g.NG; e += stride) {
+    const double v0 = grid[3 * e], v1 = grid[3 * e + 1], v2 = grid[3 * e + 2];
+    const double n2 = v0 * v0 + v1 * v1 + v2 * v2;
+    if (sqrt(n2) >= 1e-8) acc[0] += g.f / n2 * S[e];
+  }
+  const int64_t n2N = 2 * static_cast<int64_t>(g.N);
+  const int64_t total = n2N * n2N * n2N * g.NG;
+  const double inv2N = 1.0 / static_cast<double>(n2N);
+  for (int64_t e = first; e < total; e += stride) {
+    const int64_t i = e % g.NG, abc = e / g.NG;
+    const int64_t c = abc % n2N - g.N, b = (abc / n2N) % n2N - g.N, a = abc / (n2N * n2N) - g.N;
+    double v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double ga = g.B[d] * inv2N * static_cast<double>(a);
+      const double gb = g.B[3 + d] * inv2N * static_cast<double>(b);
+      const double gc = g.B[6 + d] * inv2N * static_cast<double>(c);
+      v[d] = ga + gb + gc + grid[3 * i + d];
+    }
+    const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (sqrt(n2) < 1e-8) continue;
+    double x[3];
+    fsc_direct(g, v, x);
+    acc[1] += g.f * fsc_tricubic(box, g, x) / n2;
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0) {
+    ws[2 * blockIdx.x] = acc[0];
+    ws[2 * blockIdx.x + 1] = acc[1];
+  }
+}
+
+void fsc_prepare_u(double* out_re, double* out_im, const double* U, const double* V,
+                   int64_t NGG, int64_t NF, Stream s) {
+  fsc_prepare_u_kernel<<<grid_for(NGG * NF, 256, 148 * 16), 256, 0, s>>>(out_re, out_im, U, V, NGG,
+                                                                          NF);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void fsc_stacked_to_complex(double* Q_re, double* Q_im, const double* Qs, int64_t NF, int parts,
+                            Stream s) {
+  fsc_stacked_kernel<<<grid_for(NF * NF, 256, 148 * 16), 256, 0, s>>>(Q_re, Q_im, Qs, NF, parts);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void fsc_box(double* box, const double* S, const double* grid, const FscGeometry& g, Stream s) {
+  zero(box, static_cast<size_t>(g.dims[0] * g.dims[1] * g.dims[2]), s);
+  fsc_box_kernel<<<grid_for(g.NG, 256, 148 * 4), 256, 0, s>>>(box, S, grid, g);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void fsc_sums(const double* box, const double* S, const double* grid, const FscGeometry& g,
+              double* ws, double* out_dev, Stream s) {
+  fsc_sums_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(box, S, grid, g, ws);
+  CC_LAUNCH_CHECK();
+  count();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+// ---------------------------------------------------------------------------
+// Perturbative triples: the disconnected part of one block and the block's
+// energy.  Elements run with q3 fastest, so the block array and the rows of
+// the pair-layout integrals are read along their contiguous index; the hole
+// permutations of the energy gather from the same (a, b, c) cube of the block.
+struct TriplesArgs {
+  const double* S;
+  const double* Si;
+  double* Sw;
+  double* Swi;
+  const double* t1;
+  const double* t1i;
+  const double* V;
+  const double* Vi;
+  const double* eh;
+  const double* ep;
+  int64_t o, n1, P1, P2, P3, L2, L3, total;
+  double coef[6];
+  double* ws;
+};
+
+struct Cplx { double re, im; };
+
+template <bool CPLX>
+__device__ __forceinline__ Cplx triples_singles_at(const TriplesArgs& a, int64_t p1, int64_t p2,
+                                                   int64_t p3) {
+  const int64_t v23 = p2 * a.n1 + p3, v13 = p1 * a.n1 + p3, v12 = p1 * a.n1 + p2;
+  if (!CPLX) {
+    return {a.t1[p1] * a.V[v23] + a.t1[p2] * a.V[v13] + a.t1[p3] * a.V[v12], 0.0};
+  }
+  const double t1r = a.t1[p1], t1m = a.t1i[p1], t2r = a.t1[p2], t2m = a.t1i[p2];
+  const double t3r = a.t1[p3], t3m = a.t1i[p3];
+  const double v23r = a.V[v23], v23m = a.Vi[v23], v13r = a.V[v13], v13m = a.Vi[v13];
+  const double v12r = a.V[v12], v12m = a.Vi[v12];
+  return {t1r * v23r - t1m * v23m + t2r * v13r - t2m * v13m + t3r * v12r - t3m * v12m,
+          t1r * v23m + t1m * v23r + t2r * v13m + t2m * v13r + t3r * v12m + t3m * v12r};
+}
+
+template <bool CPLX>
+__global__ void triples_singles_kernel(TriplesArgs a) {
+  const int64_t L23 = a.L2 * a.L3;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q1 = e / L23, r = e - q1 * L23, q2 = r / a.L3, q3 = r - q2 * a.L3;
+    const Cplx x = triples_singles_at<CPLX>(a, a.P1 + q1, a.P2 + q2, a.P3 + q3);
+    a.Sw[e] = x.re;
+    if (CPLX) a.Swi[e] = x.im;
+  }
+}
+
+template <bool CPLX>
+__global__ void triples_energy_kernel(TriplesArgs a) {
+  const int64_t L23 = a.L2 * a.L3, o = a.o;
+  const int64_t X1 = a.P1 / o, X2 = a.P2 / o, X3 = a.P3 / o;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q1 = e / L23, r = e - q1 * L23, q2 = r / a.L3, q3 = r - q2 * a.L3;
+    const int64_t x1 = q1 / o, x2 = q2 / o, x3 = q3 / o;
+    const int64_t y0 = q1 - x1 * o, y1 = q2 - x2 * o, y2 = q3 - x3 * o;
+    const Cplx sg = triples_singles_at<CPLX>(a, a.P1 + q1, a.P2 + q2, a.P3 + q3);
+    const double d = a.eh[y0] + a.eh[y1] + a.eh[y2] - a.ep[X1 + x1] - a.ep[X2 + x2] -
+                     a.ep[X3 + x3];
+    const int64_t b1 = x1 * o * L23, b2 = x2 * o * a.L3, b3 = x3 * o;
+    // the hole permutations 012, 021, 102, 120, 201, 210 of the pair (a, b, c)
+    const int64_t idx[6] = {e,
+                            b1 + y0 * L23 + b2 + y2 * a.L3 + b3 + y1,
+                            b1 + y1 * L23 + b2 + y0 * a.L3 + b3 + y2,
+                            b1 + y1 * L23 + b2 + y2 * a.L3 + b3 + y0,
+                            b1 + y2 * L23 + b2 + y0 * a.L3 + b3 + y1,
+                            b1 + y2 * L23 + b2 + y1 * a.L3 + b3 + y0};
+    double yr = 0.0, yi = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (a.coef[k] == 0.0) continue;
+      yr += a.coef[k] * a.S[idx[k]];
+      if (CPLX) yi += a.coef[k] * a.Si[idx[k]];
+    }
+    const double inv = 1.0 / d;
+    acc[0] += (a.S[e] - sg.re) * yr * inv;
+    if (CPLX) acc[1] += (a.Si[e] - sg.im) * yi * inv;
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0) {
+    a.ws[2 * blockIdx.x] = acc[0];
+    a.ws[2 * blockIdx.x + 1] = acc[1];
+  }
+}
+
+TriplesArgs triples_args(const double* t1, const double* t1i, const double* V, const double* Vi,
+                         const TriplesBlock& b) {
+  TriplesArgs a{};
+  a.t1 = t1; a.t1i = t1i; a.V = V; a.Vi = Vi; a.o = b.o; a.n1 = b.n1;
+  a.P1 = b.P[0]; a.P2 = b.P[1]; a.P3 = b.P[2];
+  a.L2 = b.L[1]; a.L3 = b.L[2];
+  a.total = b.L[0] * b.L[1] * b.L[2];
+  return a;
+}
+
+void triples_singles(double* S, double* S_im, const double* t1, const double* t1_im,
+                     const double* V, const double* V_im, const TriplesBlock& b, Stream s) {
+  TriplesArgs a = triples_args(t1, t1_im, V, V_im, b);
+  a.Sw = S; a.Swi = S_im;
+  if (a.total <= 0) return;
+  const unsigned grid = grid_for(a.total, 256, 148 * 16);
+  if (S_im)
+    triples_singles_kernel<true><<<grid, 256, 0, s>>>(a);
+  else
+    triples_singles_kernel<false><<<grid, 256, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                    const double* V, const double* V_im, const double* eps_h,
+                    const double* eps_p, const TriplesBlock& b, const double coef[6],
+                    double* ws, double* out_dev, Stream s) {
+  TriplesArgs a = triples_args(t1, t1_im, V, V_im, b);
+  a.S = S; a.Si = S_im; a.eh = eps_h; a.ep = eps_p; a.ws = ws;
+  for (int k = 0; k < 6; ++k) a.coef[k] = coef[k];
+  if (S_im)
+    triples_energy_kernel<true><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  else
+    triples_energy_kernel<false><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
 }  // namespace ops
 }  // namespace cc4s_b200

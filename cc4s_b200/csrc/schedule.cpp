@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <vector>
 
 namespace cc4s_b200 {
 
@@ -123,7 +124,9 @@ void Schedule::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bo
   if (!wrote) throw Error(ERR_STATE, "zgemm: complex result from real operands");
 }
 
-void Schedule::structure_factor(const double* T, double* S_dev, double* dGph_dev) {
+// W[G][(a,i)] = sum_{b,j} Gamma^hp_Gjb M[(b,j),(a,i)] with M = 2X - X^x, X = T2 + T1 T1
+// (adjW_; M stays in adjX_ + planes * D2 for the gradient).
+void Schedule::structure_factor_w(const double* T) {
   const int64_t o = so_, v = sv_, G = sG_, n1 = o * v, D2 = n1 * n1;
   if (!T || !sGph_) throw Error(ERR_STATE, "structure factor: no amplitudes or vertex");
   const int64_t planes = scplx_ ? 2 : 1, pl = n1 + D2;
@@ -144,11 +147,16 @@ void Schedule::structure_factor(const double* T, double* S_dev, double* dGph_dev
     ops::axpby(M + p * D2, 2.0, X + p * D2, 1.0, M + p * D2, 0.0, D2, s_);
   }
   const int64_t gi = scplx_ ? G * n1 : 0, mi = scplx_ ? D2 : 0;
-  {  // W[G][(a,i)] = sum_{b,j} Gamma^hp_Gjb M[(b,j),(a,i)]
-    Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
-    c.A = vw(sGhp_, 0, n1, 1, v); c.B = vw(M, o * n1, n1, 0, 1); c.C = rm(adjW_, n1);
-    zgemm(c, gi, mi, gi, false, false, true);
-  }
+  Contraction c; c.M = G; c.N = n1; c.K = n1; c.Ki = o;
+  c.A = vw(sGhp_, 0, n1, 1, v); c.B = vw(M, o * n1, n1, 0, 1); c.C = rm(adjW_, n1);
+  zgemm(c, gi, mi, gi, false, false, true);
+}
+
+void Schedule::structure_factor(const double* T, double* S_dev, double* dGph_dev) {
+  structure_factor_w(T);
+  const int64_t o = so_, v = sv_, G = sG_, n1 = o * v, D2 = n1 * n1;
+  const int64_t planes = scplx_ ? 2 : 1;
+  const int64_t gi = scplx_ ? G * n1 : 0;
   {  // S[G] = Re sum_r conj(Gamma^ph_G,r) W_G,r   (batched dot products)
     Contraction c; c.M = 1; c.N = 1; c.K = n1; c.batch = G;
     c.A = vw(sGph_, 0, 0, 0, 1, 0, n1); c.B = vw(adjW_, 0, 1, 0, 0, 0, n1);
@@ -157,10 +165,54 @@ void Schedule::structure_factor(const double* T, double* S_dev, double* dGph_dev
   }
   if (dGph_dev) {
     if (scplx_) throw Error(ERR_UNSUPPORTED, "dE/dGamma is provided on the real path only");
+    double* M = adjX_ + planes * D2;
     Contraction c; c.M = G; c.N = n1; c.K = n1;  // dE/dGph = 2 Gph M
     c.A = rm(sGph_, n1); c.B = rm(M, n1); c.C = rm(dGph_dev, n1); c.alpha = 2.0;
     tc_(c);
   }
+  (void)v;
+}
+
+void Schedule::structure_factor_pw(const double* T, const double* Uw, int64_t NGG, int64_t NF,
+                                   double* S_dev) {
+  structure_factor_w(T);
+  const int64_t G = sG_, n1 = so_ * sv_;
+  const int parts = scplx_ ? 1 : static_cast<int>(G / NF);
+  if (G != NF * parts || parts < 1 || parts > 2)
+    throw Error(ERR_BAD_SHAPE, "structure factor: vertex rows do not match the singular vectors");
+  std::vector<double*> tmp;
+  auto tk = [&](int64_t n) { double* p = ops::alloc(n); tmp.push_back(p); return p; };
+  try {
+    double* Qs = tk(scplx_ ? 2 * G * G : G * G);
+    double* Q = tk(2 * NF * NF);
+    double* Y = tk(2 * NGG * NF);
+    {  // Qs[F][F'] = sum_r conj(Gamma^ph_F,r) W_F',r  (vertex rows of this schedule)
+      Contraction c; c.M = G; c.N = G; c.K = n1;
+      c.A = rm(sGph_, n1); c.B = vw(adjW_, 0, 1, 0, n1); c.C = rm(Qs, G);
+      zgemm(c, scplx_ ? G * n1 : 0, scplx_ ? G * n1 : 0, scplx_ ? G * G : 0, scplx_, false);
+    }
+    if (scplx_) {
+      ops::d2d(Q, Qs, 2 * NF * NF, s_);
+    } else {
+      ops::fsc_stacked_to_complex(Q, Q + NF * NF, Qs, NF, parts, s_);
+    }
+    {  // Y[G][F'] = sum_F conj(Uw_GF) Q_FF'
+      Contraction c; c.M = NGG; c.N = NF; c.K = NF;
+      c.A = rm(cp(Uw), NF); c.B = rm(Q, NF); c.C = rm(Y, NF);
+      zgemm(c, NGG * NF, NF * NF, NGG * NF, true, false);
+    }
+    {  // S[G] = Re sum_F' Y[G][F'] Uw[G][F']
+      Contraction c; c.M = 1; c.N = 1; c.K = NF; c.batch = NGG;
+      c.A = vw(Y, 0, 0, 0, 1, 0, NF); c.B = vw(cp(Uw), 0, 1, 0, 0, 0, NF);
+      c.C = vw(S_dev, 0, 0, 0, 0, 0, 1);
+      zgemm(c, NGG * NF, NGG * NF, 0, false, false);
+    }
+    ops::sync(s_);
+  } catch (...) {
+    for (double* p : tmp) ops::release(p);
+    throw;
+  }
+  for (double* p : tmp) ops::release(p);
 }
 
 int Schedule::device_error() {

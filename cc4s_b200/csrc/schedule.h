@@ -53,6 +53,15 @@ class Schedule {
   //                 (real path only; may be null).
   // G runs over the schedule's auxiliary rows (stacked Re/Im rows on the real path).
   void structure_factor(const double* T, double* S_dev, double* dGph_dev);
+  // The plane-wave structure factor of FiniteSizeCorrection.cxx:50-133 with
+  // singular vectors:  S[G] = Re sum_{F,F'} conj(Uw_GF) Q_FF' Uw_GF',
+  //   Q_FF' = sum_r conj(Gamma^ph_F,r) W_F',r   (W as in structure_factor),
+  // Uw = U_GF / sqrt(V(G)) planar complex [2][NGG][NF] (device), NF the caller's
+  // vertex rows (the real path's stacked Re/Im rows are folded back into complex
+  // rows).  Equal to Gamma_G = U Gamma_F followed by structure_factor, without
+  // forming the NGG vertex rows.
+  void structure_factor_pw(const double* T, const double* Uw, int64_t NGG, int64_t NF,
+                           double* S_dev);
   int64_t aux_rows() const { return sG_; }
 
   // ---- reverse mode ---------------------------------------------------------
@@ -104,6 +113,7 @@ class Schedule {
   };
   // A forward buffer and its adjoint (same size and layout).
   struct Region { const double* p; int64_t n; double* bar; };
+  void structure_factor_w(const double* T);
   double* bar_of(const double* p) const;
   View barv(const View& v) const;
   void reverse(const std::vector<TapeOp>& tape);

@@ -13,6 +13,12 @@ CoupledCluster input chain (e.g. test/tests/h2o/dz/cc4s.in):
 * ``VertexCoulombIntegrals``: recorded only; the integrals are formed on the
   device from the vertex slices by the CoupledCluster step;
 * ``CoupledCluster``: the B200 step (cc4s_b200.CoupledCluster);
+* ``PerturbativeTriples`` / ``PerturbativeTriplesReference``: the B200 (T)
+  step (cc4s_b200.PerturbativeTriples) on the amplitudes of a CoupledCluster
+  step (e.g. test/tests/h2o/dz/cc4s.in:49-55);
+* ``FiniteSizeCorrection``: the B200 structure factor and interpolation
+  (cc4s_b200.FiniteSizeCorrection); gridVectors is a [3, NG] tensor whose
+  metaData holds the reciprocal basis Gi, Gj, Gk (FiniteSizeCorrection.cxx:143-183);
 * ``Write``: a tensor to a cc4s tensor file, anything else to YAML.
 
 Any other step name raises ValueError: it is not part of this library.
@@ -25,7 +31,7 @@ import numpy as np
 import yaml
 
 from . import tensor_io
-from .coupled_cluster import CoupledCluster
+from .coupled_cluster import CoupledCluster, FiniteSizeCorrection, PerturbativeTriples
 
 
 def _define_holes_and_particles(eps):
@@ -117,6 +123,48 @@ def run_steps(steps, workdir=".", lib=None, symbols=None):
                     for k, v in res["amplitudes"].items()}
             if "convergenceReached" in out:
                 sym[out["convergenceReached"]] = res["convergenceReached"]
+        elif name in ("PerturbativeTriples", "PerturbativeTriplesReference"):
+            eps = arg(a, "slicedEigenEnergies")
+            vertex = arg(a, "slicedCoulombVertex")
+            if vertex is None:
+                vertex = (arg(a, "coulombIntegrals") or {}).get("slicedCoulombVertex")
+            if vertex is None:
+                raise ValueError("%s: the integrals must come from a VertexCoulombIntegrals "
+                                 "step (the vertex is needed on the device)" % name)
+            md = vertex["hh"].meta_data or {}
+            amps = arg(a, "amplitudes")
+            res = PerturbativeTriples(lib=lib).run({
+                "slicedEigenEnergies": {"h": eps["h"].values, "p": eps["p"].values},
+                "slicedCoulombVertex": {k: t.values for k, t in vertex.items()},
+                "halfGrid": bool(int(md.get("halfGrid", 0))),
+                "amplitudes": {k: getattr(t, "values", t) for k, t in amps.items()},
+                "precision": a.get("precision", "fp64"),
+                "blockSize": a.get("blockSize", 0),
+                "referenceForm": name == "PerturbativeTriplesReference"})
+            sym[out.get("energy", name + "Energy")] = res["energy"]
+        elif name == "FiniteSizeCorrection":
+            eps = arg(a, "slicedEigenEnergies")
+            vertex = arg(a, "slicedCoulombVertex")
+            md = vertex["hh"].meta_data or {}
+            amps = arg(a, "amplitudes")
+            grid = arg(a, "gridVectors")
+            gmd = grid.meta_data or {}
+            basis = np.array([[float(x) for x in gmd[k]] for k in ("Gi", "Gj", "Gk")])
+            U = arg(a, "coulombVertexSingularVectors")
+            V = arg(a, "coulombPotential")
+            res = FiniteSizeCorrection(lib=lib).run({
+                "slicedEigenEnergies": {"h": eps["h"].values, "p": eps["p"].values},
+                "slicedCoulombVertex": {k: t.values for k, t in vertex.items()},
+                "halfGrid": bool(int(md.get("halfGrid", 0))),
+                "amplitudes": {k: getattr(t, "values", t) for k, t in amps.items()},
+                "gridVectors": np.asarray(grid.values).T, "reciprocalBasis": basis,
+                "coulombVertexSingularVectors": None if U is None else U.values,
+                "coulombPotential": None if V is None else V.values,
+                "interpolationGridSize": int(a.get("interpolationGridSize", 20))})
+            sym[out.get("energy", "FiniteSizeEnergy")] = res["energy"]
+            if "transitionStructureFactor" in out:
+                sym[out["transitionStructureFactor"]] = tensor_io.Tensor(
+                    values=res["transitionStructureFactor"], dimension_types=["Momentum"])
         elif name == "Write":
             src = arg(a, "source")
             path = os.path.join(workdir, a.get("fileName", "%s.yaml" % a.get("source")))

@@ -195,6 +195,73 @@ int cc4s_cc_residual_vjp(cc4s_cc_handle* h, const double* T1, const double* T2,
 int cc4s_cc_relaxed_gradient(cc4s_cc_handle* h, int max_iterations, double convergence,
                              double* dE_dGamma, cc4s_cc_lambda_result* out);
 
+/* Options of the perturbative triples step. */
+typedef struct {
+  int64_t block_size;   /* virtual indices per block of the (a,b,c) loop (0: automatic,
+                           the largest block whose (block * No)^3 array fits the L2 cache) */
+  int formulation;      /* complex path: 0 = PerturbativeTriples (atrip, Equations.hpp
+                           getEnergyDistinct: Re conj(W) Z), 1 = PerturbativeTriplesReference
+                           (PerturbativeTriplesReference.cxx:136-173: Re conj(W) conj(Z));
+                           the same on the real path */
+} cc4s_cc_triples_options;
+typedef struct {
+  double correlation;     /* energy.correlation of the step */
+  double seconds;         /* device time of the block loop */
+  double setup_seconds;   /* device time of the integral slices pphh, ppph, hhhp */
+  double flops;           /* 2 No^3 Nv^3 (No + Nv), the reference's count
+                             (PerturbativeTriples.cxx, atripDryRun) */
+  double executed_flops;  /* flops of the contractions launched (whole block triples) */
+  int64_t block_size;
+  int64_t block_triples;  /* blocks A <= B <= C evaluated */
+  double phase_seconds[4];  /* options.profile of the handle: device time of the singles,
+                               particle contractions, hole contractions and energy kernel */
+} cc4s_cc_triples_result;
+void cc4s_cc_triples_default_options(cc4s_cc_triples_options* opt);
+/* Perturbative triples energy at the current amplitudes (after cc4s_cc_run or
+ * cc4s_cc_set_initial_amplitudes).  Replaces the steps
+ *   - name: PerturbativeTriples           (src/main/algorithms/PerturbativeTriples.cxx:27-255,
+ *                                           the atrip tuple loop)
+ *   - name: PerturbativeTriplesReference  (src/main/algorithms/PerturbativeTriplesReference.cxx:56-222,
+ *                                           cT = 0)
+ *     in:  {amplitudes, coulombIntegrals, slicedEigenEnergies}
+ *     out: {energy: {correlation, unit}}
+ * The integral slices pphh, ppph and hhhp are formed on the device from the
+ * vertex given to cc4s_cc_set_inputs; the contractions run in the handle's
+ * precision (FP64 or the split form); on the complex path the hole integrals
+ * enter conjugated as in both reference steps. */
+int cc4s_cc_perturbative_triples(cc4s_cc_handle* h, const cc4s_cc_triples_options* opt,
+                                 cc4s_cc_triples_result* out);
+/* Options of the finite-size correction step. */
+typedef struct {
+  int interpolation_grid_size;  /* "interpolationGridSize" (20), FiniteSizeCorrection.cxx:143 */
+  double unit_factor;           /* product of the reference's unit factors toCoulombVertexUnits *
+                                   (grid unit / Gamma unit^2) = 1 / (grid unit^2 * potential
+                                   unit); 1 for inputs in consistent units */
+} cc4s_cc_fsc_options;
+typedef struct {
+  double correction, uncorrected, corrected;  /* energy.{correction, uncorrected, corrected} */
+  double seconds;                             /* device time (uploads, S(G), interpolation) */
+  int64_t box[3];                             /* lattice box of the interpolated S(G) */
+} cc4s_cc_fsc_result;
+void cc4s_cc_fsc_default_options(cc4s_cc_fsc_options* opt);
+/* Finite-size correction at the current amplitudes.  Replaces the step
+ *   - name: FiniteSizeCorrection  (src/main/algorithms/FiniteSizeCorrection.cxx:28-310)
+ *     in:  {amplitudes, coulombVertexSingularVectors, slicedCoulombVertex, coulombPotential,
+ *           gridVectors, interpolationGridSize}
+ *     out: {transitionStructureFactor, energy: {correction, uncorrected, corrected, unit}}
+ * singular_vectors: U[G,F] column-major complex interleaved (NGG x NG, NG the vertex
+ * rows given to cc4s_cc_set_inputs; NULL: the identity, NGG = NG); coulomb_potential:
+ * V[G] (NULL: 1); grid_vectors: [3, NGG] column-major (the cartesian G vectors);
+ * reciprocal_basis: the rows Gi, Gj, Gk of the gridVectors metaData.  S_of_G
+ * (optional, [NGG]) receives transitionStructureFactor.  The structure factor
+ * (FiniteSizeCorrection.cxx:50-133) is formed on the device without the NGG vertex
+ * rows; the Catmull-Rom tricubic interpolation over the (2N)^3 NGG refined points
+ * runs on the device too (on one rank the reference counts every point). */
+int cc4s_cc_finite_size_correction(cc4s_cc_handle* h, const double* singular_vectors,
+                                   int64_t NGG, const double* coulomb_potential,
+                                   const double* grid_vectors, const double* reciprocal_basis,
+                                   const cc4s_cc_fsc_options* opt, double* S_of_G,
+                                   cc4s_cc_fsc_result* out);
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
 
 /* Correlation energy of amplitudes that already live in device memory, computed

@@ -7,7 +7,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 CSRC = os.path.join(ROOT, "cc4s_b200", "csrc")
 OUT = os.path.join(HERE, "_build", "libcc4s_emu.so")
 SCHEDULE_SOURCES = ("schedule.cpp", "ccsd_real.cpp", "ccsd_complex.cpp", "drccd.cpp",
-                    "driver.cpp", "abi.cpp")
+                    "driver.cpp", "abi.cpp", "triples.cpp")
 
 
 def build():

@@ -5,6 +5,7 @@
 // test library (tests/emu/_build/libcc4s_emu.so) so that the index and stride
 // bookkeeping of every contraction can be checked against the oracle on a
 // machine without a GPU.  The product library never contains this file.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -376,7 +377,14 @@ void lincomb(double* out, const double* const* xs, const double* const* ys, cons
   if (ys && norm2) norm2[0] = s2;
 }
 
-void sum_partials_to(double*, const double*, int, int, Stream) {}
+void sum_partials_to(double* dst, const double* ws, int nparts, int nvals, Stream) {
+  ++g_ops;
+  for (int k = 0; k < nvals; ++k) {
+    double v = 0.0;
+    for (int b = 0; b < nparts; ++b) v += ws[b * nvals + k];
+    dst[k] = v;
+  }
+}
 
 int scan_vertex(const double* p, int64_t n, bool complex_values, Stream) {
   ++g_ops;
@@ -470,6 +478,169 @@ void lincomb_packed(double* out, const double* const* xs, const double* const* y
       }
   }
   if (ys && norm2) norm2[0] = s2;
+}
+
+
+void fsc_prepare_u(double* ore, double* oim, const double* U, const double* V, int64_t NGG,
+                   int64_t NF, Stream) {
+  ++g_ops;
+  for (int64_t G = 0; G < NGG; ++G)
+    for (int64_t F = 0; F < NF; ++F) {
+      const int64_t e = F * NGG + G;
+      const double re = U ? U[2 * e] : (G == F ? 1.0 : 0.0), im = U ? U[2 * e + 1] : 0.0;
+      const double sc = V ? 1.0 / std::sqrt(V[G]) : 1.0;
+      ore[G * NF + F] = re * sc;
+      oim[G * NF + F] = im * sc;
+    }
+}
+
+void fsc_stacked_to_complex(double* Qr, double* Qi, const double* Qs, int64_t NF, int parts,
+                            Stream) {
+  ++g_ops;
+  const int64_t S2 = parts * NF;
+  for (int64_t F = 0; F < NF; ++F)
+    for (int64_t Fp = 0; Fp < NF; ++Fp) {
+      const int64_t e = F * NF + Fp;
+      if (parts == 2) {
+        Qr[e] = Qs[F * S2 + Fp] + Qs[(F + NF) * S2 + Fp + NF];
+        Qi[e] = Qs[F * S2 + Fp + NF] - Qs[(F + NF) * S2 + Fp];
+      } else {
+        Qr[e] = Qs[e];
+        Qi[e] = 0.0;
+      }
+    }
+}
+
+static void fsc_direct_emu(const FscGeometry& g, const double v[3], double x[3]) {
+  for (int d = 0; d < 3; ++d) x[d] = g.A[3 * d] * v[0] + g.A[3 * d + 1] * v[1] + g.A[3 * d + 2] * v[2];
+}
+
+void fsc_box(double* box, const double* S, const double* grid, const FscGeometry& g, Stream) {
+  ++g_ops;
+  std::memset(box, 0, sizeof(double) * g.dims[0] * g.dims[1] * g.dims[2]);
+  for (int64_t e = 0; e < g.NG; ++e) {
+    double x[3];
+    fsc_direct_emu(g, grid + 3 * e, x);
+    int64_t i[3];
+    for (int d = 0; d < 3; ++d) i[d] = static_cast<int64_t>(std::floor(x[d] + 0.5) - g.origin[d]);
+    box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
+  }
+}
+
+static double fsc_tricubic_emu(const double* box, const FscGeometry& g, const double x[3]) {
+  static const double BL[4][4] = {{0.0, -0.5, 1.0, -0.5}, {1.0, 0.0, -2.5, 1.5},
+                                  {0.0, 0.5, 2.0, -1.5}, {0.0, 0.0, -0.5, 0.5}};
+  double w[3][4];
+  int64_t base[3];
+  for (int d = 0; d < 3; ++d) {
+    const double t = x[d] - g.origin[d];
+    int64_t i = static_cast<int64_t>(t);
+    i = std::min<int64_t>(std::max<int64_t>(i, 0), g.dims[d] - 1);
+    const double u = t - static_cast<double>(i);
+    for (int r = 0; r < 4; ++r) w[d][r] = BL[r][0] + BL[r][1] * u + BL[r][2] * u * u + BL[r][3] * u * u * u;
+    base[d] = i - 1;
+  }
+  auto cl = [](int64_t a, int64_t n) { return std::min<int64_t>(std::max<int64_t>(a, 0), n - 1); };
+  double total = 0.0;
+  for (int sl = 0; sl < 4; ++sl)
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c)
+        total += w[0][c] * w[1][r] * w[2][sl] *
+                 box[cl(base[0] + c, g.dims[0]) +
+                     g.dims[0] * (cl(base[1] + r, g.dims[1]) + g.dims[1] * cl(base[2] + sl, g.dims[2]))];
+  return total;
+}
+
+void fsc_sums(const double* box, const double* S, const double* grid, const FscGeometry& g,
+              double*, double* out, Stream) {
+  ++g_ops;
+  double acc0 = 0.0, acc1 = 0.0;
+  for (int64_t e = 0; e < g.NG; ++e) {
+    const double* v = grid + 3 * e;
+    const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    if (std::sqrt(n2) >= 1e-8) acc0 += g.f / n2 * S[e];
+  }
+  const int64_t n2N = 2 * static_cast<int64_t>(g.N);
+  const double inv2N = 1.0 / static_cast<double>(n2N);
+  for (int64_t a = -g.N; a < g.N; ++a)
+    for (int64_t b = -g.N; b < g.N; ++b)
+      for (int64_t c = -g.N; c < g.N; ++c)
+        for (int64_t i = 0; i < g.NG; ++i) {
+          double v[3];
+          for (int d = 0; d < 3; ++d)
+            v[d] = g.B[d] * inv2N * double(a) + g.B[3 + d] * inv2N * double(b) +
+                   g.B[6 + d] * inv2N * double(c) + grid[3 * i + d];
+          const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+          if (std::sqrt(n2) < 1e-8) continue;
+          double x[3];
+          fsc_direct_emu(g, v, x);
+          acc1 += g.f * fsc_tricubic_emu(box, g, x) / n2;
+        }
+  out[0] = acc0;
+  out[1] = acc1;
+}
+
+struct TriplesC { double re, im; };
+
+static TriplesC triples_singles_at(const double* t, const double* ti, const double* V,
+                                   const double* Vi, int64_t n1, int64_t p1, int64_t p2,
+                                   int64_t p3) {
+  const int64_t pr[3][3] = {{p1, p2, p3}, {p2, p1, p3}, {p3, p1, p2}};  // t index, V row, V col
+  TriplesC s{0.0, 0.0};
+  for (const auto& k : pr) {
+    const double tr = t[k[0]], tm = ti ? ti[k[0]] : 0.0;
+    const double vr = V[k[1] * n1 + k[2]], vm = Vi ? Vi[k[1] * n1 + k[2]] : 0.0;
+    s.re += tr * vr - tm * vm;
+    s.im += tr * vm + tm * vr;
+  }
+  return s;
+}
+
+void triples_singles(double* S, double* S_im, const double* t1, const double* t1_im,
+                     const double* V, const double* V_im, const TriplesBlock& b, Stream) {
+  ++g_ops;
+  for (int64_t q1 = 0; q1 < b.L[0]; ++q1)
+    for (int64_t q2 = 0; q2 < b.L[1]; ++q2)
+      for (int64_t q3 = 0; q3 < b.L[2]; ++q3) {
+        const int64_t e = (q1 * b.L[1] + q2) * b.L[2] + q3;
+        const TriplesC x = triples_singles_at(t1, t1_im, V, V_im, b.n1, b.P[0] + q1,
+                                              b.P[1] + q2, b.P[2] + q3);
+        S[e] = x.re;
+        if (S_im) S_im[e] = x.im;
+      }
+}
+
+void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                    const double* V, const double* V_im, const double* eh, const double* ep,
+                    const TriplesBlock& b, const double coef[6], double*, double* out, Stream) {
+  ++g_ops;
+  static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  const int64_t o = b.o;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t q1 = 0; q1 < b.L[0]; ++q1)
+    for (int64_t q2 = 0; q2 < b.L[1]; ++q2)
+      for (int64_t q3 = 0; q3 < b.L[2]; ++q3) {
+        const int64_t x[3] = {q1 / o, q2 / o, q3 / o};
+        const int64_t y[3] = {q1 % o, q2 % o, q3 % o};
+        auto at = [&](const double* A, int64_t r1, int64_t r2, int64_t r3) {
+          return A[(r1 * b.L[1] + r2) * b.L[2] + r3];
+        };
+        const TriplesC sg = triples_singles_at(t1, t1_im, V, V_im, b.n1, b.P[0] + q1,
+                                               b.P[1] + q2, b.P[2] + q3);
+        double d = 0.0;
+        for (int m = 0; m < 3; ++m) d += eh[y[m]] - ep[b.P[m] / o + x[m]];
+        double yr = 0.0, yi = 0.0;
+        for (int k = 0; k < 6; ++k) {
+          const int64_t r1 = x[0] * o + y[perm[k][0]], r2 = x[1] * o + y[perm[k][1]],
+                        r3 = x[2] * o + y[perm[k][2]];
+          yr += coef[k] * at(S, r1, r2, r3);
+          if (S_im) yi += coef[k] * at(S_im, r1, r2, r3);
+        }
+        acc[0] += (at(S, q1, q2, q3) - sg.re) * yr / d;
+        if (S_im) acc[1] += (at(S_im, q1, q2, q3) - sg.im) * yi / d;
+      }
+  out[0] = acc[0];
+  out[1] = acc[1];
 }
 
 }  // namespace ops

@@ -1,0 +1,148 @@
+"""The product's (T) schedule (cc4s_b200/csrc/triples.cpp) and its C-ABI entry,
+linked against the plain-loop CPU emulation of the device operations
+(tests/emu/ops_emu.cpp, test-only) and checked against the oracle's
+restatement of PerturbativeTriplesReference.  This pins the strides of the
+twelve block contractions, the singles, the hole-permutation weights of every
+kind of block triple and the block bookkeeping without a GPU."""
+import os
+import sys
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import inputs, triples
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
+warnings.simplefilter("ignore")
+
+
+@pytest.fixture(scope="module")
+def emu_lib():
+    import build_emu
+    return build_emu.build()
+
+
+def _rand_T(rng, Nv, No):
+    T1 = rng.standard_normal((Nv, No)) * 0.05
+    T2 = rng.standard_normal((Nv, Nv, No, No)) * 0.03
+    return T1, T2 + T2.transpose(1, 0, 3, 2)
+
+
+def _triples(lib, s, T1, T2, block, precision="fp64"):
+    from cc4s_b200.coupled_cluster import Solver
+    sol = Solver({"precision": precision}, lib=lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        sol.set_initial_amplitudes(T1, T2)
+        return sol.perturbative_triples(block)
+    finally:
+        sol.close()
+
+
+@pytest.mark.parametrize("shape", [(3, 10, 16), (2, 7, 9), (4, 6, 20)])
+@pytest.mark.parametrize("block", [1, 2, 3, 4, 0])
+def test_triples_matches_oracle(emu_lib, shape, block):
+    """Every block length, ragged last blocks included, gives the oracle's energy."""
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, seed=No + Nv)
+    rng = np.random.default_rng(NG)
+    T1, T2 = _rand_T(rng, Nv, No)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    r = _triples(emu_lib, s, T1, T2, block)
+    assert abs(r["correlation"] - ref) < 1e-12 * max(1.0, abs(ref)), (r["correlation"], ref)
+    nb = r["block_size"]
+    nbk = -(-Nv // nb)
+    assert r["block_triples"] == nbk * (nbk + 1) * (nbk + 2) // 6
+    assert r["flops"] == 2.0 * No ** 3 * Nv ** 3 * (No + Nv)
+    assert r["executed_flops"] >= r["flops"] * (1 - 1e-12)
+
+
+def test_triples_split_precision(emu_lib):
+    """The split form of the particle contractions stays within 1e-7 of the energy."""
+    s = inputs.synthetic_system(3, 10, 80, seed=4)
+    rng = np.random.default_rng(8)
+    T1, T2 = _rand_T(rng, 10, 3)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    r = _triples(emu_lib, s, T1, T2, 4, precision="split3")
+    assert abs(r["correlation"] - ref) < 1e-7 * abs(ref)
+
+
+def test_triples_requires_amplitudes(emu_lib):
+    from cc4s_b200 import _abi
+    from cc4s_b200.coupled_cluster import CoupledClusterError, Solver
+    s = inputs.synthetic_system(2, 5, 8, seed=1)
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        with pytest.raises(CoupledClusterError) as e:
+            sol.perturbative_triples()
+        assert e.value.status == _abi.ERR_STATE
+        sol.set_initial_amplitudes(*_rand_T(np.random.default_rng(0), 5, 2))
+        with pytest.raises(CoupledClusterError) as e:
+            sol.perturbative_triples(-1)
+        assert e.value.status == _abi.ERR_INVALID_ARGUMENT
+    finally:
+        sol.close()
+
+
+@pytest.mark.parametrize("block", [1, 3, 0])
+def test_triples_complex_both_formulations(emu_lib, block):
+    """Complex path: formulation 0 is the atrip tuple loop (Re conj(W) Z),
+    formulation 1 the array form of PerturbativeTriplesReference
+    (Re conj(W) conj(Z)); on arbitrary complex amplitudes they differ."""
+    from cc4s_b200.coupled_cluster import Solver
+    No, Nv = 3, 8
+    c = inputs.synthetic_system(No, Nv, 14, complex=True, seed=3)
+    rng = np.random.default_rng(2)
+    T1 = (rng.standard_normal((Nv, No)) + 1j * rng.standard_normal((Nv, No))) * 0.05
+    T2 = (rng.standard_normal((Nv, Nv, No, No)) + 1j * rng.standard_normal((Nv, Nv, No, No))) * 0.03
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    V = triples.triples_integrals(c)
+    e_atrip = triples.triples_atrip(T1, T2, V, c.eps_h, c.eps_p)
+    e_ref = triples.triples_reference(T1, T2, V, c.eps_h, c.eps_p)
+    assert abs(e_atrip - e_ref) > 1e-6  # the two conjugations are distinguishable here
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(c.eps_h, c.eps_p, c.gamma, half_grid=False)
+        sol.set_initial_amplitudes(T1, T2)
+        a = sol.perturbative_triples(block)["correlation"]
+        b = sol.perturbative_triples(block, reference_form=True)["correlation"]
+    finally:
+        sol.close()
+    assert abs(a - e_atrip) < 1e-12 * max(1.0, abs(e_atrip)), (a, e_atrip)
+    assert abs(b - e_ref) < 1e-12 * max(1.0, abs(e_ref)), (b, e_ref)
+
+
+def test_block_weights_cover_every_ordering():
+    """The hole-permutation weights of a block triple: the blocked sum over
+    A <= B <= C equals the full sum for symmetric W, S (checked in numpy with
+    the same weights the C++ schedule uses, restated here)."""
+    PERMS = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+
+    def comp(a, b):
+        return tuple(a[b[m]] for m in range(3))
+
+    def inv(a):
+        r = [0, 0, 0]
+        for m in range(3):
+            r[a[m]] = m
+        return tuple(r)
+
+    def coefs(blk):
+        seen, c = set(), np.zeros(6)
+        for sg in PERMS:
+            key = tuple(blk[sg[m]] for m in range(3))
+            if key in seen:
+                continue
+            seen.add(key)
+            c[0] += 4 / 3
+            c[PERMS.index(comp(comp(sg, (0, 2, 1)), inv(sg)))] -= 2
+            c[PERMS.index(comp(comp(sg, (2, 0, 1)), inv(sg)))] += 2 / 3
+        return c
+
+    assert np.allclose(coefs((0, 1, 2)), [8, -4, -4, 2, 2, -4])
+    assert np.allclose(coefs((0, 0, 0)), [4 / 3, -2, 0, 0, 2 / 3, 0])
+    # the weights of each kind of triple sum to zero: a fully symmetric S adds nothing
+    for blk in [(0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 2)]:
+        assert abs(coefs(blk).sum()) < 1e-12

@@ -1,0 +1,149 @@
+"""Parity of the device (T) energy (cc4s_cc_perturbative_triples) with the
+oracle's restatement of PerturbativeTriplesReference on a B200."""
+import json
+import os
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import inputs, triples
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+warnings.simplefilter("ignore")
+
+# FP64: the block sums differ from the oracle's order of summation only by
+# rounding (1e-11 relative).  Split form: 28 bits of every operand in the
+# particle contractions give ~1e-8 relative in the energy (tolerance 1e-6).
+TOL_FP64 = 1e-11
+TOL_SPLIT = 1e-6
+
+
+def _rand_T(rng, Nv, No, scale=0.03):
+    T1 = rng.standard_normal((Nv, No)) * scale
+    T2 = rng.standard_normal((Nv, Nv, No, No)) * scale
+    return T1, T2 + T2.transpose(1, 0, 3, 2)
+
+
+def _triples(s, T1, T2, block=0, precision="fp64"):
+    from cc4s_b200 import Solver
+    sol = Solver({"precision": precision})
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        sol.set_initial_amplitudes(T1, T2)
+        return sol.perturbative_triples(block)
+    finally:
+        sol.close()
+
+
+@pytest.mark.parametrize("shape", [(4, 24, 48), (6, 30, 90), (3, 17, 40)])
+@pytest.mark.parametrize("block", [1, 5, 0])
+def test_triples_matches_oracle(shape, block):
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, seed=No * Nv)
+    rng = np.random.default_rng(NG)
+    T1, T2 = _rand_T(rng, Nv, No)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    r = _triples(s, T1, T2, block)
+    assert abs(r["correlation"] - ref) < TOL_FP64 * abs(ref), (r["correlation"], ref)
+
+
+def test_triples_split_precision_matches_oracle():
+    s = inputs.synthetic_system(6, 30, 90, seed=5)
+    rng = np.random.default_rng(9)
+    T1, T2 = _rand_T(rng, 30, 6)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    r = _triples(s, T1, T2, 4, precision="split3")
+    assert abs(r["correlation"] - ref) < TOL_SPLIT * abs(ref), (r["correlation"], ref)
+
+
+def test_triples_block_invariance_and_split_at_size():
+    """No=16, Nv=128 (beyond the oracle's array form): every block length and
+    the split form give the same energy; the loop covers v^3/6 ordered triples."""
+    s = inputs.synthetic_system(16, 128, 256, seed=3)
+    rng = np.random.default_rng(4)
+    T1, T2 = _rand_T(rng, 128, 16, scale=0.01)
+    a = _triples(s, T1, T2, 0)
+    b = _triples(s, T1, T2, 9)
+    c = _triples(s, T1, T2, 0, precision="split3")
+    assert abs(a["correlation"] - b["correlation"]) < TOL_FP64 * abs(a["correlation"])
+    assert abs(c["correlation"] - a["correlation"]) < TOL_SPLIT * abs(a["correlation"])
+    assert a["flops"] == 2.0 * 16 ** 3 * 128 ** 3 * (16 + 128)
+    assert a["seconds"] > 0
+
+
+def test_c0_triples_golden_after_ccsd():
+    """CCSD on the device, then (T) on the handle's amplitudes: the committed
+    c0 golden (oracle CCSD + tuple-loop (T))."""
+    from cc4s_b200 import Solver
+    g = json.load(open(os.path.join(GOLDEN, "c0_seed0.json")))
+    s = inputs.config_system("c0", seed=g["seed"])
+    sol = Solver(g["options"])
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        r = sol.run()
+        assert r["converged"]
+        t = sol.perturbative_triples()
+    finally:
+        sol.close()
+    assert abs(t["correlation"] - g["triples"]["correlation"]) < 1e-8, t
+
+
+def test_perturbative_triples_operator():
+    """The operator mirror of the reference step: amplitudes in, energy map out."""
+    from cc4s_b200 import PerturbativeTriples
+    s = inputs.synthetic_system(4, 24, 48, seed=2)
+    rng = np.random.default_rng(1)
+    T1, T2 = _rand_T(rng, 24, 4)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    out = PerturbativeTriples().run({
+        "slicedEigenEnergies": {"h": s.eps_h, "p": s.eps_p}, "coulombVertex": s.gamma,
+        "halfGrid": True, "amplitudes": {"ph": T1, "pphh": T2}})
+    assert set(out["energy"]) == {"correlation", "unit"}
+    assert abs(out["energy"]["correlation"] - ref) < TOL_FP64 * abs(ref)
+
+
+@pytest.mark.parametrize("reference_form", [False, True])
+def test_triples_complex_matches_oracle(reference_form):
+    """Complex path, both conjugations: the atrip tuple loop (formulation 0) and the
+    array form of PerturbativeTriplesReference (formulation 1)."""
+    from cc4s_b200 import Solver
+    No, Nv = 4, 20
+    c = inputs.synthetic_system(No, Nv, 40, complex=True, seed=6)
+    rng = np.random.default_rng(3)
+    T1 = (rng.standard_normal((Nv, No)) + 1j * rng.standard_normal((Nv, No))) * 0.03
+    T2 = (rng.standard_normal((Nv, Nv, No, No)) + 1j * rng.standard_normal((Nv, Nv, No, No))) * 0.02
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    V = triples.triples_integrals(c)
+    f = triples.triples_reference if reference_form else triples.triples_atrip
+    ref = f(T1, T2, V, c.eps_h, c.eps_p)
+    sol = Solver({})
+    try:
+        sol.set_inputs(c.eps_h, c.eps_p, c.gamma, half_grid=False)
+        sol.set_initial_amplitudes(T1, T2)
+        e = sol.perturbative_triples(3, reference_form=reference_form)["correlation"]
+    finally:
+        sol.close()
+    assert abs(e - ref) < TOL_FP64 * abs(ref), (e, ref)
+
+
+def test_ueg_triples_after_ccsd_matches_reference_expected_output():
+    """The reference's UEG regression test (complex path): CCSD on the device,
+    then PerturbativeTriplesReference's (T) on the handle's amplitudes, against
+    the expected output in test/tests/ueg/rs1.0-7occ-26virt/correct.out.yaml."""
+    from cc4s_b200 import Solver
+    g = json.load(open(os.path.join(GOLDEN, "ueg_rs1.0_7occ_26virt.json")))
+    s = inputs.ueg_system(7, 26, 1.0)
+    sol = Solver(g["ccsd"]["options"])
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+        r = sol.run()
+        assert r["converged"]
+        a = sol.perturbative_triples(reference_form=True)["correlation"]
+        b = sol.perturbative_triples()["correlation"]
+    finally:
+        sol.close()
+    ref = g["triples"]["energy"]["correlation"]
+    assert abs(a - ref) < 1e-9, (a, ref)
+    assert abs(b - ref) < 1e-9, (b, ref)

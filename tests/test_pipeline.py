@@ -101,4 +101,77 @@ def test_input_chain_runs_coupled_cluster(tmp_path, emu_lib, half_grid, binary):
 def test_unknown_step_is_rejected(tmp_path):
     from cc4s_b200 import pipeline
     with pytest.raises(ValueError, match="not part of"):
-        pipeline.run_steps([{"name": "PerturbativeTriples", "in": {}, "out": {}}], str(tmp_path))
+        pipeline.run_steps([{"name": "UegVertexGenerator", "in": {}, "out": {}}], str(tmp_path))
+
+
+def test_input_chain_runs_perturbative_triples(tmp_path, emu_lib):
+    """... -> CoupledCluster -> PerturbativeTriples (test/tests/h2o/dz/cc4s.in:32-55):
+    the (T) energy on the chain's CCSD amplitudes equals the oracle's."""
+    import yaml
+    from cc4s_b200 import pipeline
+    from oracle import triples
+    s = inputs.synthetic_system(3, 9, 20, seed=2)
+    _write_system(tmp_path, s, True, True)
+    steps = STEPS[:-1] + [
+        {"name": "PerturbativeTriples",
+         "in": {"coulombIntegrals": "CoulombIntegrals", "amplitudes": "Amplitudes",
+                "slicedEigenEnergies": "EigenEnergies"},
+         "out": {"energy": "TriplesEnergy"}}]
+    with open(tmp_path / "cc4s.in", "w") as f:
+        yaml.safe_dump(steps, f, sort_keys=False)
+    sym = pipeline.run_file(str(tmp_path / "cc4s.in"), lib=emu_lib)
+    ref = coupled_cluster.run(s, maxIterations=40, energyConvergence=1e-10,
+                              amplitudesConvergence=1e-8,
+                              mixer=dict(type="DiisMixer", maxResidua=4))
+    T1, T2 = ref["amplitudes"]
+    e = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    assert abs(sym["TriplesEnergy"]["correlation"] - e) < 1e-9 * max(1.0, abs(e))
+
+
+def test_input_chain_runs_finite_size_correction(tmp_path, emu_lib):
+    """... -> CoupledCluster -> FiniteSizeCorrection with grid vectors, Coulomb
+    potential and singular vectors read from tensor files: S(G) and the energies
+    equal the oracle's on the chain's CCSD amplitudes."""
+    import yaml
+    from cc4s_b200 import pipeline, tensor_io
+    from oracle import fsc
+    No, Nv, NF = 2, 6, 10
+    s = inputs.synthetic_system(No, Nv, NF, seed=8)
+    _write_system(tmp_path, s, True, True)
+    rng = np.random.default_rng(3)
+    B = 2 * np.pi / 4.0 * np.eye(3)
+    r = np.arange(4) - 2
+    grid = np.array([(a, b, c) for c in r for b in r for a in r], dtype=float) @ B
+    NGG = grid.shape[0]
+    U = (rng.standard_normal((NGG, NF)) + 1j * rng.standard_normal((NGG, NF))) / 4
+    V = 0.5 + rng.random(NGG)
+    tensor_io.write(str(tmp_path / "GridVectors.yaml"), tensor_io.Tensor(
+        values=grid.T.copy(), dimension_types=["Vector", "Momentum"],
+        meta_data={"Gi": B[0].tolist(), "Gj": B[1].tolist(), "Gk": B[2].tolist()}))
+    tensor_io.write(str(tmp_path / "CoulombPotential.yaml"),
+                    tensor_io.Tensor(values=V, dimension_types=["Momentum"]))
+    tensor_io.write(str(tmp_path / "CoulombVertexSingularVectors.yaml"),
+                    tensor_io.Tensor(values=U, dimension_types=["Momentum", "AuxiliaryField"]))
+    steps = STEPS[:-1] + [
+        {"name": "Read", "in": {"fileName": f + ".yaml"}, "out": {"destination": f}}
+        for f in ("GridVectors", "CoulombPotential", "CoulombVertexSingularVectors")] + [
+        {"name": "FiniteSizeCorrection",
+         "in": {"amplitudes": "Amplitudes", "slicedCoulombVertex": "CoulombVertex",
+                "slicedEigenEnergies": "EigenEnergies", "gridVectors": "GridVectors",
+                "coulombPotential": "CoulombPotential",
+                "coulombVertexSingularVectors": "CoulombVertexSingularVectors",
+                "interpolationGridSize": 2},
+         "out": {"energy": "FscEnergy", "transitionStructureFactor": "SofG"}}]
+    with open(tmp_path / "cc4s.in", "w") as f:
+        yaml.safe_dump(steps, f, sort_keys=False)
+    sym = pipeline.run_file(str(tmp_path / "cc4s.in"), lib=emu_lib)
+    ref = coupled_cluster.run(s, maxIterations=40, energyConvergence=1e-10,
+                              amplitudesConvergence=1e-8,
+                              mixer=dict(type="DiisMixer", maxResidua=4))
+    T1, T2 = ref["amplitudes"]
+    g = np.asarray(s.gamma)
+    S_ref = fsc.transition_structure_factor(T1, T2, g[:, No:, :No], g[:, :No, No:], U, V)
+    E_ref = fsc.interpolation(S_ref, grid, B, N=2)
+    S = sym["SofG"].values
+    assert np.abs(S - S_ref).max() < 1e-8 * np.abs(S_ref).max()
+    assert abs(sym["FscEnergy"]["correction"] - E_ref["correction"]) < 1e-8 * abs(E_ref["corrected"])
