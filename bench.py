@@ -21,7 +21,8 @@ reference itself needs MPI and the Cyclops Tensor Framework, which are not
 installed) timed on this host's cores on a bounded sample of the same
 workload.
 --adjoint: relaxed-gradient (Lambda equations) timing and finite-difference
-check; --converge: converged energies of the FP64, split and refined forms.
+check; --converge: converged energies of the FP64, split and refined forms;
+--triples: the perturbative triples (T) step after CCSD.
 """
 import argparse
 import json
@@ -405,6 +406,135 @@ def run_converge(args, local):
             "forms": out}
 
 
+def cpu_triples_sample(cfg, n=20):
+    """CPU rate of the oracle's (T) tuple loop (the atrip formulation: per tuple
+    twelve o^2 x o x (v or o) contractions, singles and energy), timed on all host
+    cores on the tuples a <= b <= c < n of the workload's shapes with random
+    operands; the reference's flop count per tuple converts it to seconds."""
+    import numpy as np
+    from oracle import triples as otr
+    o, v, G = CONFIG_SHAPES[cfg]
+    rng = np.random.default_rng(0)
+    T1 = rng.standard_normal((n, o)) * 0.01
+    T2 = rng.standard_normal((n, v, o, o)) * 0.01
+    V = {"pphh": rng.standard_normal((n, n, o, o)), "ppph": rng.standard_normal((n, n, v, o)),
+         "hhhp": rng.standard_normal((o, o, o, n))}
+    eh = -1.0 - rng.random(o)
+    ep = 1.0 + rng.random(n)
+    t0 = time.perf_counter()
+    otr.triples_atrip(T1, T2, V, eh, ep)
+    dt = time.perf_counter() - t0
+    tuples = n * (n + 1) * (n + 2) // 6 - n
+    all_tuples = v * (v + 1) * (v + 2) // 6 - v
+    per_tuple = otr.triples_flops(o, v) / all_tuples
+    rate = tuples * per_tuple / dt
+    return dict(seconds=otr.triples_flops(o, v) / rate, rate_tflops=rate / 1e12, cores=os.cpu_count(),
+                sample="oracle tuple loop (numpy/BLAS) on %d of the %d tuples of %s (a<=b<=c<%d), "
+                       "%.1f s; seconds = reference flops / measured rate" % (
+                           tuples, all_tuples, cfg, n, dt))
+
+
+def run_triples(args, local):
+    """(T) after CCSD: two FP64 CCSD iterations give amplitudes with singles; the
+    (T) energy of those amplitudes, device-resident, in the FP64 and the split
+    form (CUDA events inside the library); e2e through the PerturbativeTriples
+    operator from host buffers (vertex and amplitude upload, integral slices,
+    block loop), wall clock."""
+    import numpy as np
+    import torch
+    from cc4s_b200 import PerturbativeTriples, Solver
+    from cc4s_b200.synthetic import config
+    from oracle.triples import triples_flops
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    if cfg in COMPLEX_CONFIGS:
+        raise SystemExit("--triples: real configurations only")
+    if cfg == "custom":
+        from cc4s_b200.synthetic import synthetic
+        eh, ep, g, hg = synthetic(o, v, G, complex=False, seed=0)
+    else:
+        eh, ep, g, hg = config(cfg, seed=0)
+    if args.vertex_scale is not None:
+        g *= args.vertex_scale
+    F = triples_flops(o, v)
+    forms = ["fp64", "split3"] if args.precision == "both" else [args.precision]
+    out = {}
+    so = Solver(dict(maxIterations=2, energyConvergence=-1.0, amplitudesConvergence=-1.0,
+                     mixer=dict(type="DiisMixer", maxResidua=5), device=local))
+    so.set_inputs(eh, ep, g, half_grid=hg)
+    so.run()
+    T = so.amplitudes()
+    so.close()
+    for p in forms:
+        so = Solver(dict(device=local, precision=p, profile=args.profile))
+        so.set_inputs(eh, ep, g, half_grid=hg)
+        so.set_initial_amplitudes(*T)
+        runs = []
+        for k in range(args.warmup + args.steps):
+            with ClockSampler(local) as clk:
+                r = so.perturbative_triples(args.triples_block)
+            runs.append((r, clk.summary()))
+        so.close()
+        timed = runs[args.warmup:]
+        secs = statistics.median(x[0]["seconds"] for x in timed)
+        out[p] = {"seconds": secs, "tflops": F / secs / 1e12, "energy": timed[-1][0]["correlation"],
+                  "setup_seconds": timed[-1][0]["setup_seconds"],
+                  "executed_flops": timed[-1][0]["executed_flops"],
+                  "block_size": timed[-1][0]["block_size"],
+                  "block_triples": timed[-1][0]["block_triples"], "clocks": timed[-1][1],
+                  "phase_seconds": timed[-1][0]["phase_seconds"] if args.profile else None}
+    head = "split3" if "split3" in out else "fp64"
+    hr = out[head]
+    # end to end: host amplitudes and vertex through the operator
+    t0 = time.perf_counter()
+    e = PerturbativeTriples().run({"slicedEigenEnergies": {"h": eh, "p": ep}, "coulombVertex": g,
+                                   "halfGrid": hg, "amplitudes": {"ph": T[0], "pphh": T[1]},
+                                   "precision": head, "blockSize": args.triples_block,
+                                   "device": local})
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    pk = peaks()
+    dpeak = dgemm_peak(local)
+    if head == "split3":
+        achieved = 6.0 * hr["executed_flops"] / hr["seconds"] / 1e12
+        peak = pk.get("bf16_tflops", 1686.1)
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "whole (T) block loop: split_kernel particle contractions, FP64 hole "
+                          "contractions, singles and energy kernels (six FP16 slice products per "
+                          "executed FP64 multiply-add)",
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)"}
+    else:
+        achieved = hr["executed_flops"] / hr["seconds"] / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
+                "frac": achieved / dpeak, "traffic": None,
+                "kernel": "whole (T) block loop (gemm_f64_kernel contractions + bandwidth kernels)",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured)"}
+    line = {"metric": "(T) perturbative triples energy TFLOP/s (reference flop count) on 1 B200",
+            "value": F / hr["seconds"] / 1e12, "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * hr["seconds"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator; amplitudes after two CCSD iterations)",
+            "config": {"workload": "(T) %s: No=%d Nv=%d NG=%d real, %s" % (cfg, o, v, G, head),
+                       "flops_reference": F, "forms": out, "fp64_dgemm_peak_tflops": dpeak,
+                       "abs_dE_split_vs_fp64": abs(out["split3"]["energy"] - out["fp64"]["energy"])
+                       if len(out) == 2 else None,
+                       "split_speedup_vs_fp64": out["fp64"]["seconds"] / out["split3"]["seconds"]
+                       if len(out) == 2 else None},
+            "e2e": {"value": F / t_e2e / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": int(g.nbytes + eh.nbytes + ep.nbytes + T[0].nbytes +
+                                              T[1].nbytes),
+                    "d2h_bytes_per_step": 8, "seconds": t_e2e,
+                    "energy": e["energy"]["correlation"]},
+            "roofline": roof, "clocks": hr["clocks"]}
+    if not args.no_cpu_baseline:
+        c = cpu_triples_sample(cfg)
+        line["cpu_baseline"] = {"value": F / c["seconds"] / 1e12, "unit": "TFLOP/s",
+                                "cores": c["cores"], "kind": "port", "sample": c["sample"]}
+    return line
+
+
 def run_reference(args, world, rank):
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
@@ -446,11 +576,24 @@ def main():
                     help="converge FP64, split and refined split forms and compare energies")
     ap.add_argument("--refine", type=float, default=1e-5,
                     help="residuum norm below which the refined split form switches to FP64")
+    ap.add_argument("--triples", action="store_true",
+                    help="time the perturbative triples (T) step instead (real configurations)")
+    ap.add_argument("--triples-block", type=int, default=0,
+                    help="virtual indices per (T) block (0: automatic)")
+    ap.add_argument("--shape", default=None,
+                    help="No,Nv,NG of a real synthetic system instead of --config (profiling of "
+                         "small cases)")
+    ap.add_argument("--profile", action="store_true",
+                    help="--triples: device time of each phase of the block loop")
     ap.add_argument("--vertex-scale", type=float, default=None,
                     help="scale of the synthetic vertex (default 1; 0.3 for --converge and "
                          "--adjoint: CCSD on the unscaled synthetic vertex diverges at these "
                          "sizes, strongly correlated)")
     args = ap.parse_args()
+    if args.shape:
+        o_, v_, g_ = (int(x) for x in args.shape.split(","))
+        CONFIG_SHAPES["custom"] = (o_, v_, g_)
+        args.config = "custom"
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
@@ -459,9 +602,12 @@ def main():
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return
     world, rank, local = dist_setup()
-    if args.adjoint or args.converge:
+    if args.adjoint or args.converge or args.triples:
         if rank == 0:
-            line = run_adjoint(args, local) if args.adjoint else run_converge(args, local)
+            if args.triples:
+                line = run_triples(args, local)
+            else:
+                line = run_adjoint(args, local) if args.adjoint else run_converge(args, local)
             print(json.dumps(line), flush=True)
         return
     line = run_ours(args, world, rank, local)
