@@ -245,6 +245,9 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
     co[h] = n < p.N ? p.Cn.off(static_cast<uint32_t>(n)) : 0;
     co2[h] = (C2b && n < p.N) ? p.C2n.off(static_cast<uint32_t>(n)) : 0;
   }
+  // Accumulating stores: the eight old values of a fragment row are loaded before
+  // any of them is stored, so the reads are in flight together (a store followed
+  // by a load through another pointer would serialise them: the two may alias).
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
@@ -253,20 +256,30 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
       if (m >= p.M) continue;
       const int64_t ro = p.Cm.off(static_cast<uint32_t>(m));
       const int64_t ro2 = C2b ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
+      double val[8], old[8];
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt)
+      for (int h = 0; h < 8; ++h) {
+        const int64_t n = n0 + wn + (h >> 1) * 8 + 2 * t + (h & 1);
+        val[h] = p.alpha * acc[mt][h >> 1][hh * 2 + (h & 1)];
+        old[h] = (p.beta != 0.0 && n < p.N) ? Cb[ro + co[h]] : 0.0;
+      }
 #pragma unroll
-        for (int par = 0; par < 2; ++par) {
-          const int64_t n = n0 + wn + nt * 8 + 2 * t + par;
-          if (n >= p.N) continue;
-          const double v = p.alpha * acc[mt][nt][hh * 2 + par];
-          double* c = Cb + ro + co[nt * 2 + par];
-          *c = (p.beta != 0.0) ? v + p.beta * *c : v;
-          if (C2b) {
-            double* c2 = C2b + ro2 + co2[nt * 2 + par];
-            *c2 = (p.beta != 0.0) ? v + p.beta * *c2 : v;
-          }
+      for (int h = 0; h < 8; ++h) {
+        const int64_t n = n0 + wn + (h >> 1) * 8 + 2 * t + (h & 1);
+        if (n < p.N) Cb[ro + co[h]] = val[h] + p.beta * old[h];
+      }
+      if (C2b) {
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          const int64_t n = n0 + wn + (h >> 1) * 8 + 2 * t + (h & 1);
+          old[h] = (p.beta != 0.0 && n < p.N) ? C2b[ro2 + co2[h]] : 0.0;
         }
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          const int64_t n = n0 + wn + (h >> 1) * 8 + 2 * t + (h & 1);
+          if (n < p.N) C2b[ro2 + co2[h]] = val[h] + p.beta * old[h];
+        }
+      }
     }
 }
 

@@ -200,6 +200,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// Accumulating store of NB output elements: every old value is loaded before the
+// first store, so the NB reads are in flight together (a store followed by a load
+// through another pointer would otherwise serialise them: the two may alias).
+template <int NB>
+__device__ __forceinline__ void rmw_store(double* const (&ptr)[NB], const double (&v)[NB],
+                                          double beta) {
+  if (beta != 0.0) {
+    double old[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) old[j] = ptr[j] ? *ptr[j] : 0.0;
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+      if (ptr[j]) *ptr[j] = v[j] + beta * old[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+      if (ptr[j]) *ptr[j] = v[j];
+  }
+}
 
 struct SplitParams {
   int64_t M, N, K;                 // logical extents
@@ -375,16 +394,20 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         const Ax& On = out == 0 ? p.Cn : p.C2n;
         const bool n_contig = On.s_i == 1 && On.inner > 1;
         for (int q = 0; q < 16; ++q) {
+          double* ptr[4];
+          double val[4];
+#pragma unroll
           for (int b = 0; b < 4; ++b) {
             // n-contiguous: warp row r, lanes along columns; otherwise warp column, lanes along rows
             const int r = n_contig ? ew + 8 * q : 32 * b + lane;
             const int cc = n_contig ? 32 * b + lane : ew + 8 * q;
             const int64_t mm = m0 + r, nn = n0 + cc;
-            if (mm >= p.M || nn >= p.N) continue;
-            double* ptr = O + Om.off(static_cast<uint32_t>(mm)) + On.off(static_cast<uint32_t>(nn));
-            const double v = T[r * LDT + cc];
-            *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+            const bool in = mm < p.M && nn < p.N;
+            ptr[b] = in ? O + Om.off(static_cast<uint32_t>(mm)) + On.off(static_cast<uint32_t>(nn))
+                        : nullptr;
+            val[b] = T[r * LDT + cc];
           }
+          rmw_store<4>(ptr, val, p.beta);
         }
       }
     }
@@ -568,15 +591,25 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
       if (m_major) {
         // lanes are consecutive rows: store column by column straight from registers
 #pragma unroll
-        for (int j = 0; j < 64; ++j) {
-          const int64_t n = n0 + 64 * half + j;
-          if (m >= p.M || n >= p.N) continue;
-          const double v = acc[j] * sa * ldexp(1.0, p.eb[n]);
-          double* ptr = p.C + rowoff + p.Cn.off(static_cast<uint32_t>(n));
-          *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+        for (int j0 = 0; j0 < 64; j0 += 4) {
+          double* ptr[4];
+          double val[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t n = n0 + 64 * half + j0 + j;
+            const bool in = m < p.M && n < p.N;
+            val[j] = in ? acc[j0 + j] * sa * ldexp(1.0, p.eb[n]) : 0.0;
+            ptr[j] = in ? p.C + rowoff + p.Cn.off(static_cast<uint32_t>(n)) : nullptr;
+          }
+          rmw_store<4>(ptr, val, p.beta);
           if (p.C2) {
-            double* p2 = p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n));
-            *p2 = p.beta != 0.0 ? v + p.beta * *p2 : v;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int64_t n = n0 + 64 * half + j0 + j;
+              ptr[j] = (m < p.M && n < p.N) ? p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n))
+                                            : nullptr;
+            }
+            rmw_store<4>(ptr, val, p.beta);
           }
         }
       } else {
@@ -590,18 +623,31 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
             wb[lane * 16 + (j ^ (lane & 15))] = v;
           }
           __syncwarp();
-#pragma unroll 4
-          for (int k = 0; k < 16; ++k) {
-            const int r = 2 * k + (lane >> 4), cc = lane & 15;  // row within the warp, column
-            const int64_t mm = m0 + quad * 32 + r;
+#pragma unroll 1
+          for (int k0 = 0; k0 < 16; k0 += 4) {
+            double* ptr[4];
+            double val[4];
+            const int cc = lane & 15;  // column within the piece
             const int64_t nn = n0 + 64 * half + 16 * piece + cc;
-            if (mm >= p.M || nn >= p.N) continue;
-            const double v = wb[r * 16 + (cc ^ (r & 15))];
-            double* ptr = p.C + p.Cm.off(static_cast<uint32_t>(mm)) + p.Cn.off(static_cast<uint32_t>(nn));
-            *ptr = p.beta != 0.0 ? v + p.beta * *ptr : v;
+            const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int r = 2 * (k0 + k) + (lane >> 4);  // row within the warp
+              const int64_t mm = m0 + quad * 32 + r;
+              const bool in = mm < p.M && nn < p.N;
+              val[k] = wb[r * 16 + (cc ^ (r & 15))];
+              ptr[k] = in ? p.C + p.Cm.off(static_cast<uint32_t>(mm)) + cn : nullptr;
+            }
+            rmw_store<4>(ptr, val, p.beta);
             if (p.C2) {
-              double* p2 = p.C2 + p.C2m.off(static_cast<uint32_t>(mm)) + p.C2n.off(static_cast<uint32_t>(nn));
-              *p2 = p.beta != 0.0 ? v + p.beta * *p2 : v;
+              const int64_t cn2 = nn < p.N ? p.C2n.off(static_cast<uint32_t>(nn)) : 0;
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const int64_t mm = m0 + quad * 32 + 2 * (k0 + k) + (lane >> 4);
+                ptr[k] = (mm < p.M && nn < p.N) ? p.C2 + p.C2m.off(static_cast<uint32_t>(mm)) + cn2
+                                                : nullptr;
+              }
+              rmw_store<4>(ptr, val, p.beta);
             }
           }
           __syncwarp();
