@@ -200,6 +200,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+// 2^e as an exact double: built from its exponent bits in the normal range.
+__device__ __forceinline__ double pow2i(int e) {
+  if (e >= -1022 && e <= 1023) return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+  return ldexp(1.0, e);
+}
 // Accumulating store of NB output elements: every old value is loaded before the
 // first store, so the NB reads are in flight together (a store followed by a load
 // through another pointer would otherwise serialise them: the two may alias).
@@ -583,69 +588,78 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
         mbar_arrive(smem_u32(&bars[2 * NST + 1]));  // TMEM free: the next chunk may start
       }
       if (!ok) { atomicExch(&abort_flag, 1); break; }
-      // store this warp's 32 rows x 64 columns (the MMA issuer is already on the next tile)
+      // store this warp's 32 rows x 64 columns (the MMA issuer is already on the next tile).
+      // The offset of a row belongs to the lane of that row; the offset and the
+      // power-of-two scale of a column are computed by one lane per group of 32 (or 16)
+      // columns; both reach the lanes that store an element through warp shuffles
+      // (offset -1: outside the output).
       const int64_t m = m0 + row;
       const double sa = m < p.M ? ldexp(p.alpha, p.ea[m]) : 0.0;
-      const int64_t rowoff = m < p.M ? p.Cm.off(static_cast<uint32_t>(m)) : 0;
-      const int64_t rowoff2 = (m < p.M && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : 0;
+      const int64_t rowoff = m < p.M ? p.Cm.off(static_cast<uint32_t>(m)) : -1;
+      const int64_t rowoff2 = (m < p.M && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : -1;
       if (m_major) {
         // lanes are consecutive rows: store column by column straight from registers
 #pragma unroll
-        for (int j0 = 0; j0 < 64; j0 += 4) {
-          double* ptr[4];
-          double val[4];
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int64_t nl = n0 + 64 * half + 32 * h2 + lane;  // this lane's column of the group
+          const int64_t colL = nl < p.N ? p.Cn.off(static_cast<uint32_t>(nl)) : -1;
+          const double scL = nl < p.N ? pow2i(p.eb[nl]) : 0.0;
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int64_t n = n0 + 64 * half + j0 + j;
-            const bool in = m < p.M && n < p.N;
-            val[j] = in ? acc[j0 + j] * sa * ldexp(1.0, p.eb[n]) : 0.0;
-            ptr[j] = in ? p.C + rowoff + p.Cn.off(static_cast<uint32_t>(n)) : nullptr;
-          }
-          rmw_store<4>(ptr, val, p.beta);
-          if (p.C2) {
+          for (int j0 = 0; j0 < 32; j0 += 4) {
+            double* ptr[4];
+            double val[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-              const int64_t n = n0 + 64 * half + j0 + j;
-              ptr[j] = (m < p.M && n < p.N) ? p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n))
-                                            : nullptr;
+              const int64_t col = __shfl_sync(0xffffffffu, colL, j0 + j);
+              const double sc = __shfl_sync(0xffffffffu, scL, j0 + j);
+              val[j] = acc[32 * h2 + j0 + j] * sa * sc;
+              ptr[j] = (rowoff >= 0 && col >= 0) ? p.C + rowoff + col : nullptr;
             }
             rmw_store<4>(ptr, val, p.beta);
+            if (p.C2) {
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int64_t n = n0 + 64 * half + 32 * h2 + j0 + j;
+                ptr[j] = (rowoff2 >= 0 && n < p.N)
+                             ? p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n)) : nullptr;
+              }
+              rmw_store<4>(ptr, val, p.beta);
+            }
           }
         }
       } else {
         // 16-column pieces through the warp's buffer; lanes then run along columns
 #pragma unroll
         for (int piece = 0; piece < 4; ++piece) {
+          const int cc = lane & 15;  // this lane's column within the piece
+          const int64_t nn = n0 + 64 * half + 16 * piece + cc;
+          const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
+          const double scL = nn < p.N ? pow2i(p.eb[nn]) : 0.0;
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const int64_t n = n0 + 64 * half + 16 * piece + j;
-            const double v = (m < p.M && n < p.N) ? acc[16 * piece + j] * sa * ldexp(1.0, p.eb[n]) : 0.0;
-            wb[lane * 16 + (j ^ (lane & 15))] = v;
+            const double sc = __shfl_sync(0xffffffffu, scL, j);
+            wb[lane * 16 + (j ^ (lane & 15))] = acc[16 * piece + j] * sa * sc;
           }
           __syncwarp();
 #pragma unroll 1
           for (int k0 = 0; k0 < 16; k0 += 4) {
             double* ptr[4];
             double val[4];
-            const int cc = lane & 15;  // column within the piece
-            const int64_t nn = n0 + 64 * half + 16 * piece + cc;
-            const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
               const int r = 2 * (k0 + k) + (lane >> 4);  // row within the warp
-              const int64_t mm = m0 + quad * 32 + r;
-              const bool in = mm < p.M && nn < p.N;
+              const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
               val[k] = wb[r * 16 + (cc ^ (r & 15))];
-              ptr[k] = in ? p.C + p.Cm.off(static_cast<uint32_t>(mm)) + cn : nullptr;
+              ptr[k] = (ro >= 0 && cn >= 0) ? p.C + ro + cn : nullptr;
             }
             rmw_store<4>(ptr, val, p.beta);
             if (p.C2) {
-              const int64_t cn2 = nn < p.N ? p.C2n.off(static_cast<uint32_t>(nn)) : 0;
+              const int64_t cn2 = nn < p.N ? p.C2n.off(static_cast<uint32_t>(nn)) : -1;
 #pragma unroll
               for (int k = 0; k < 4; ++k) {
-                const int64_t mm = m0 + quad * 32 + 2 * (k0 + k) + (lane >> 4);
-                ptr[k] = (mm < p.M && nn < p.N) ? p.C2 + p.C2m.off(static_cast<uint32_t>(mm)) + cn2
-                                                : nullptr;
+                const int r = 2 * (k0 + k) + (lane >> 4);
+                const int64_t r2 = __shfl_sync(0xffffffffu, rowoff2, r);
+                ptr[k] = (r2 >= 0 && cn2 >= 0) ? p.C2 + r2 + cn2 : nullptr;
               }
               rmw_store<4>(ptr, val, p.beta);
             }
