@@ -22,7 +22,8 @@ installed) timed on this host's cores on a bounded sample of the same
 workload.
 --adjoint: relaxed-gradient (Lambda equations) timing and finite-difference
 check; --converge: converged energies of the FP64, split and refined forms;
---triples: the perturbative triples (T) step after CCSD.
+--triples: the perturbative triples (T) step after CCSD; --fsc: the
+FiniteSizeCorrection step.
 """
 import argparse
 import json
@@ -471,10 +472,12 @@ def run_triples(args, local):
         so.set_inputs(eh, ep, g, half_grid=hg)
         so.set_initial_amplitudes(*T)
         runs = []
+        st0 = so.stats()
         for k in range(args.warmup + args.steps):
             with ClockSampler(local) as clk:
                 r = so.perturbative_triples(args.triples_block)
             runs.append((r, clk.summary()))
+        st1 = so.stats()
         so.close()
         timed = runs[args.warmup:]
         secs = statistics.median(x[0]["seconds"] for x in timed)
@@ -483,7 +486,10 @@ def run_triples(args, local):
                   "executed_flops": timed[-1][0]["executed_flops"],
                   "block_size": timed[-1][0]["block_size"],
                   "block_triples": timed[-1][0]["block_triples"], "clocks": timed[-1][1],
-                  "phase_seconds": timed[-1][0]["phase_seconds"] if args.profile else None}
+                  "phase_seconds": timed[-1][0]["phase_seconds"] if args.profile else None,
+                  "launches": ((st1["gemm_launches"] - st0["gemm_launches"]) +
+                               (st1["other_launches"] - st0["other_launches"])) /
+                              (args.warmup + args.steps)}
     head = "split3" if "split3" in out else "fp64"
     hr = out[head]
     # end to end: host amplitudes and vertex through the operator
@@ -527,11 +533,100 @@ def run_triples(args, local):
                                               T[1].nbytes),
                     "d2h_bytes_per_step": 8, "seconds": t_e2e,
                     "energy": e["energy"]["correlation"]},
-            "roofline": roof, "clocks": hr["clocks"]}
+            "roofline": roof, "clocks": hr["clocks"], "gpu_launches": int(round(hr["launches"]))}
     if not args.no_cpu_baseline:
         c = cpu_triples_sample(cfg)
         line["cpu_baseline"] = {"value": F / c["seconds"] / 1e12, "unit": "TFLOP/s",
                                 "cores": c["cores"], "kind": "port", "sample": c["sample"]}
+    return line
+
+
+def run_fsc(args, local):
+    """FiniteSizeCorrection after CCSD: two FP64 CCSD iterations give the
+    amplitudes; plane-wave grid of n^3 vectors (n = 16 by default) of a skewed reciprocal
+    lattice, random complex singular vectors U [NGG, NG] and potential V(G);
+    device time of the step (uploads, structure factor, interpolation over
+    (2N)^3 NGG points); e2e through the operator from host buffers; CPU: the
+    oracle's interpolation on a bounded sample of the refined points."""
+    import numpy as np
+    import torch
+    from cc4s_b200 import FiniteSizeCorrection, Solver
+    from cc4s_b200.synthetic import config
+    from oracle import fsc as ofsc
+    torch.cuda.set_device(local)
+    cfg = args.config
+    o, v, G = CONFIG_SHAPES[cfg]
+    if cfg in COMPLEX_CONFIGS:
+        raise SystemExit("--fsc: real configurations only")
+    if cfg == "custom":
+        from cc4s_b200.synthetic import synthetic
+        eh, ep, g, hg = synthetic(o, v, G, complex=False, seed=0)
+    else:
+        eh, ep, g, hg = config(cfg, seed=0)
+    rng = np.random.default_rng(0)
+    n = args.fsc_grid
+    B = 2 * np.pi / 6.0 * (np.eye(3) + 0.05 * rng.standard_normal((3, 3)))
+    r = np.arange(n) - n // 2
+    grid = np.array([(a, b, c) for c in r for b in r for a in r], dtype=float) @ B
+    NGG = grid.shape[0]
+    U = (rng.standard_normal((NGG, G)) + 1j * rng.standard_normal((NGG, G))) / np.sqrt(G)
+    V = 0.5 + rng.random(NGG)
+    N = args.fsc_n
+    so = Solver(dict(maxIterations=2, energyConvergence=-1.0, amplitudesConvergence=-1.0,
+                     mixer=dict(type="DiisMixer", maxResidua=5), device=local))
+    so.set_inputs(eh, ep, g, half_grid=hg)
+    so.run()
+    T = so.amplitudes()
+    st0 = so.stats()
+    secs = []
+    for k in range(args.warmup + args.steps):
+        e, S = so.finite_size_correction(grid, B, U, V, grid_size=N)
+        secs.append(e["seconds"])
+    st1 = so.stats()
+    so.close()
+    t = statistics.median(secs[args.warmup:])
+    points = (2 * N) ** 3 * NGG
+    launches = ((st1["gemm_launches"] - st0["gemm_launches"]) +
+                (st1["other_launches"] - st0["other_launches"])) / (args.warmup + args.steps)
+    t0 = time.perf_counter()
+    out = FiniteSizeCorrection().run({
+        "slicedEigenEnergies": {"h": eh, "p": ep}, "coulombVertex": g, "halfGrid": hg,
+        "amplitudes": {"ph": T[0], "pphh": T[1]}, "gridVectors": grid, "reciprocalBasis": B,
+        "coulombVertexSingularVectors": U, "coulombPotential": V, "interpolationGridSize": N,
+        "device": local})
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    line = {"metric": "FiniteSizeCorrection: interpolated points per second (tricubic, (2N)^3 NGG)",
+            "value": points / t, "unit": "points/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded grid, singular vectors, potential; amplitudes after two "
+                    "CCSD iterations)",
+            "config": {"workload": "FSC %s: No=%d Nv=%d NG=%d, NGG=%d plane waves, N=%d" % (
+                cfg, o, v, G, NGG, N), "points": points, "box": e["box"],
+                       "correction": e["correction"], "uncorrected": e["uncorrected"]},
+            "gpu_launches": int(round(launches)),
+            "e2e": {"value": points / t_e2e, "unit": "points/s",
+                    "h2d_bytes_per_step": int(g.nbytes + T[0].nbytes + T[1].nbytes + U.nbytes +
+                                              V.nbytes + grid.nbytes),
+                    "d2h_bytes_per_step": int(S.nbytes + 24), "seconds": t_e2e}}
+    if not args.no_cpu_baseline:
+        # oracle interpolation on a sample of the refined points (same box and S)
+        A, omega, dims, origin, direct = ofsc.box_of(grid, B)
+        box = np.zeros(int(np.prod(dims)))
+        for i in range(NGG):
+            idx = np.floor(direct[i] + 0.5).astype(int) - origin.astype(int)
+            box[idx[0] + dims[0] * (idx[1] + dims[1] * idx[2])] = S[i]
+        sample = 20000
+        t0 = time.perf_counter()
+        for k in range(sample):
+            gv = grid[k % NGG] + B[0] * ((k // NGG) % 7 - 3) / (2.0 * N)
+            ofsc.tricubic(box, dims, origin, A @ gv)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample / dt, "unit": "points/s", "cores": 1,
+                                "kind": "port",
+                                "sample": "oracle tricubic interpolation (Python) on %d refined "
+                                          "points, %.1f s" % (sample, dt)}
     return line
 
 
@@ -578,6 +673,11 @@ def main():
                     help="residuum norm below which the refined split form switches to FP64")
     ap.add_argument("--triples", action="store_true",
                     help="time the perturbative triples (T) step instead (real configurations)")
+    ap.add_argument("--fsc", action="store_true",
+                    help="time the FiniteSizeCorrection step instead (real configurations)")
+    ap.add_argument("--fsc-grid", type=int, default=16,
+                    help="--fsc: plane-wave grid of n^3 vectors")
+    ap.add_argument("--fsc-n", type=int, default=20, help="--fsc: interpolationGridSize")
     ap.add_argument("--triples-block", type=int, default=0,
                     help="virtual indices per (T) block (0: automatic)")
     ap.add_argument("--shape", default=None,
@@ -602,9 +702,11 @@ def main():
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return
     world, rank, local = dist_setup()
-    if args.adjoint or args.converge or args.triples:
+    if args.adjoint or args.converge or args.triples or args.fsc:
         if rank == 0:
-            if args.triples:
+            if args.fsc:
+                line = run_fsc(args, local)
+            elif args.triples:
                 line = run_triples(args, local)
             else:
                 line = run_adjoint(args, local) if args.adjoint else run_converge(args, local)
