@@ -172,18 +172,21 @@ def dist_setup():
 
 
 def all_max(x, world):
+    """Maximum of x over the ranks (NCCL on the GPUs; gloo ranks on the host use CPU tensors)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
 def barrier(world):
     import torch
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
