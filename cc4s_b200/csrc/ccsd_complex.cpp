@@ -86,9 +86,8 @@ void CcsdComplex::zaxpby(double* out, double a, const double* x, double b, const
 // Iteration-independent integrals (VertexCoulombIntegrals.cxx:143-190).
 void CcsdComplex::build_integrals() {
   const int64_t o = sys_.o, v = sys_.v, G = sys_.G, n1 = v * o, D2 = D2_;
-  const int64_t gpp = G * v * v, gph = G * n1, ghh = G * o * o;
-  double *Gpp = sys_.Gpp, *Gph = sys_.Gph, *Ghh = sys_.Ghh, *Ghp = sys_.Ghp;
-  (void)Gpp; (void)ghh; (void)gpp;
+  const int64_t gph = G * n1;
+  double *Gph = sys_.Gph, *Ghh = sys_.Ghh, *Ghp = sys_.Ghp;
   {  // Vd[(a,i),(b,j)] = V_abij = sum_G conj(Ghp[G][i][a]) Gph[G][b][j]
     Contraction c; c.M = n1; c.N = n1; c.K = G; c.Mi = o;
     c.A = vw(Ghp, 1, v, 0, n1);
