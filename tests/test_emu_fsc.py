@@ -127,3 +127,29 @@ def test_structure_factor_with_identity_is_the_backward_one():
     a = fsc.transition_structure_factor(T1, T2, g[:, 3:, :3], g[:, :3, 3:])
     b = properties.structure_factor(s, (T1, T2))
     assert np.abs(a - b).max() < 1e-13 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("N,NF", [(1, 80), (3, 5)])
+def test_fsc_grid_sizes_and_default_potential(emu_lib, N, NF):
+    """interpolationGridSize 1 and 3, more vertex rows than plane waves (NF = 80 >
+    NGG = 64) and fewer (NF = 5), V(G) = 1 when no potential is given."""
+    from cc4s_b200.coupled_cluster import Solver
+    No, Nv = 2, 4
+    B, grid = lattice(4, seed=3)
+    NGG = grid.shape[0]
+    s = inputs.synthetic_system(No, Nv, NF, seed=9)
+    rng = np.random.default_rng(2)
+    T1, T2 = _amps(rng, No, Nv, False)
+    U = (rng.standard_normal((NGG, NF)) + 1j * rng.standard_normal((NGG, NF))) / 4
+    g = np.asarray(s.gamma)
+    S_ref = fsc.transition_structure_factor(T1, T2, g[:, No:, :No], g[:, :No, No:], U, None)
+    E_ref = fsc.interpolation(S_ref, grid, B, N=N)
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        sol.set_initial_amplitudes(T1, T2)
+        e, S = sol.finite_size_correction(grid, B, U, None, grid_size=N)
+    finally:
+        sol.close()
+    assert np.abs(S - S_ref).max() < 1e-12 * np.abs(S_ref).max()
+    assert abs(e["correction"] - E_ref["correction"]) < 1e-11 * abs(E_ref["corrected"])

@@ -146,3 +146,21 @@ def test_block_weights_cover_every_ordering():
     # the weights of each kind of triple sum to zero: a fully symmetric S adds nothing
     for blk in [(0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 2)]:
         assert abs(coefs(blk).sum()) < 1e-12
+
+
+@pytest.mark.parametrize("shape,block", [((1, 4, 6), 0), ((1, 5, 7), 2), ((3, 1, 5), 0),
+                                         ((2, 3, 4), 5)])
+def test_triples_edge_shapes(emu_lib, shape, block):
+    """One hole (all hole permutations coincide), one virtual (every triple has
+    a = b = c: the energy vanishes), a block longer than Nv."""
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, seed=7)
+    rng = np.random.default_rng(11)
+    T1, T2 = _rand_T(rng, Nv, No)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    r = _triples(emu_lib, s, T1, T2, block)
+    if Nv == 1:
+        assert abs(ref) < 1e-15 and abs(r["correlation"]) < 1e-15
+    else:
+        assert abs(r["correlation"] - ref) < 1e-12 * max(1.0, abs(ref)), (r["correlation"], ref)
+    assert r["block_size"] == (min(block, Nv) if block > 0 else r["block_size"])
