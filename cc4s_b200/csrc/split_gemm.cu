@@ -758,7 +758,7 @@ void pack(const View& v, bool rows_are_m, const Contraction& g, int64_t R, int64
 // Packed slices of both operands are limited to this many bytes: a longer K is
 // cut into panels (multiples of KCHUNK where possible), each packed and
 // multiplied in turn and accumulated into C in FP64.
-constexpr size_t kPanelBytes = size_t(9) << 28;  // 2.25 GiB
+constexpr size_t kPanelBytes = size_t(3) << 30;  // 3 GiB: one panel for the ladder contractions
 
 // CC4S_SPLIT_PANEL_BYTES (at least 1 MiB) overrides the limit, e.g. to trade
 // scratch memory for fewer, longer panels.

@@ -22,7 +22,7 @@ int main(int argc, char** argv) {
                 {7168, 1568, 256, 0, 0, 1.0, 2}};
   const int64_t L = 224, o = 32;
   int* err; cudaMalloc(&err, 4); cudaMemset(err, 0, 4);
-  SplitScratch ws; ws.bytes = size_t(3) << 30; cudaMalloc(&ws.p, ws.bytes); ws.error = err;
+  SplitScratch ws; ws.bytes = size_t(4) << 30; cudaMalloc(&ws.p, ws.bytes); ws.error = err;  // >= any panel
   GemmScratch gs; gs.elems = 1 << 24; cudaMalloc(&gs.p, gs.elems * 8);
   const int only = argc > 1 ? atoi(argv[1]) : -1;
   int idx = -1;
