@@ -175,3 +175,38 @@ def test_input_chain_runs_finite_size_correction(tmp_path, emu_lib):
     S = sym["SofG"].values
     assert np.abs(S - S_ref).max() < 1e-8 * np.abs(S_ref).max()
     assert abs(sym["FscEnergy"]["correction"] - E_ref["correction"]) < 1e-8 * abs(E_ref["corrected"])
+
+
+def test_tensor_file_rejections(tmp_path):
+    """TensorIo header checks (TensorIo.cxx:142-247): version, scalar type,
+    block-sparse files, element count, elements type."""
+    import yaml
+    from cc4s_b200 import tensor_io
+    base = {"type": "Tensor", "scalarType": "Real64", "version": 100,
+            "dimensions": {0: {"length": 3, "type": "State"}},
+            "elements": {"type": "TextFile"}, "unit": 1.0}
+    (tmp_path / "T.elements").write_text("1\n2\n3\n")
+
+    def write_header(h):
+        with open(tmp_path / "T.yaml", "w") as f:
+            yaml.safe_dump(h, f)
+
+    write_header(base)
+    assert np.array_equal(tensor_io.read(str(tmp_path / "T.yaml")).values, [1.0, 2.0, 3.0])
+    for bad, msg in [(dict(base, version=99), "version"), (dict(base, scalarType="Real32"), "scalarType"),
+                     (dict(base, nonZeroCondition={"all": []}), "block-sparse"),
+                     (dict(base, elements={"type": "Hdf5"}), "elements type"),
+                     (dict(base, dimensions={0: {"length": 4}}), "elements, expecting")]:
+        write_header(bad)
+        with pytest.raises(ValueError, match=msg):
+            tensor_io.read(str(tmp_path / "T.yaml"))
+
+
+def test_tensor_file_text_complex(tmp_path):
+    """Complex text elements are (re,im) per line, first index fastest."""
+    from cc4s_b200 import tensor_io
+    v = np.array([[1 + 2j, 3 - 1j], [0.5j, -2.0]])
+    tensor_io.write(str(tmp_path / "C.yaml"), tensor_io.Tensor(values=v), binary=False)
+    lines = (tmp_path / "C.elements").read_text().split()
+    assert lines[0] == "(1,2)" and lines[1] == "(0,0.5)"   # column-major: v[0,0], v[1,0]
+    assert np.array_equal(tensor_io.read(str(tmp_path / "C.yaml")).values, v)
