@@ -410,32 +410,62 @@ def run_converge(args, local):
             "forms": out}
 
 
-def cpu_triples_sample(cfg, n=20):
+_TRIPLES_SAMPLE = {}
+
+
+def _triples_worker_init(arrays):
+    _TRIPLES_SAMPLE.update(arrays)
+
+
+def _triples_worker(chunk):
+    from oracle import triples as otr
+    d = _TRIPLES_SAMPLE
+    return sum(otr.tuple_energy(a, b, c, d["T1"], d["T2"], d["V"], d["eh"], d["ep"])
+               for a, b, c in chunk)
+
+
+def cpu_triples_sample(cfg, n=32):
     """CPU rate of the oracle's (T) tuple loop (the atrip formulation: per tuple
-    twelve o^2 x o x (v or o) contractions, singles and energy), timed on all host
-    cores on the tuples a <= b <= c < n of the workload's shapes with random
-    operands; the reference's flop count per tuple converts it to seconds."""
+    twelve o^2 x o x (v or o) contractions, singles and energy), tuples spread
+    over all host cores like atrip spreads them over ranks (one process per core,
+    one BLAS thread each; spawned, so safe after GPU work), timed on the tuples
+    a <= b <= c < n of the workload's shapes with random operands; the
+    reference's flop count per tuple converts the rate to seconds."""
+    import multiprocessing as mp
     import numpy as np
     from oracle import triples as otr
     o, v, G = CONFIG_SHAPES[cfg]
+    n = min(n, v)
     rng = np.random.default_rng(0)
-    T1 = rng.standard_normal((n, o)) * 0.01
-    T2 = rng.standard_normal((n, v, o, o)) * 0.01
-    V = {"pphh": rng.standard_normal((n, n, o, o)), "ppph": rng.standard_normal((n, n, v, o)),
-         "hhhp": rng.standard_normal((o, o, o, n))}
-    eh = -1.0 - rng.random(o)
-    ep = 1.0 + rng.random(n)
-    t0 = time.perf_counter()
-    otr.triples_atrip(T1, T2, V, eh, ep)
-    dt = time.perf_counter() - t0
-    tuples = n * (n + 1) * (n + 2) // 6 - n
+    arrays = {"T1": rng.standard_normal((n, o)) * 0.01,
+              "T2": rng.standard_normal((n, v, o, o)) * 0.01,
+              "V": {"pphh": rng.standard_normal((n, n, o, o)),
+                    "ppph": rng.standard_normal((n, n, v, o)),
+                    "hhhp": rng.standard_normal((o, o, o, n))},
+              "eh": -1.0 - rng.random(o), "ep": 1.0 + rng.random(n)}
+    work = otr.tuples(n)
+    cores = os.cpu_count() or 1
+    chunks = [work[k::cores] for k in range(cores)]
+    old = os.environ.get("OPENBLAS_NUM_THREADS")
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    try:
+        with mp.get_context("spawn").Pool(cores, _triples_worker_init, (arrays,)) as pool:
+            pool.map(_triples_worker, [c[:2] for c in chunks])   # start-up, imports
+            t0 = time.perf_counter()
+            pool.map(_triples_worker, chunks)
+            dt = time.perf_counter() - t0
+    finally:
+        if old is None:
+            os.environ.pop("OPENBLAS_NUM_THREADS", None)
+        else:
+            os.environ["OPENBLAS_NUM_THREADS"] = old
     all_tuples = v * (v + 1) * (v + 2) // 6 - v
     per_tuple = otr.triples_flops(o, v) / all_tuples
-    rate = tuples * per_tuple / dt
-    return dict(seconds=otr.triples_flops(o, v) / rate, rate_tflops=rate / 1e12, cores=os.cpu_count(),
-                sample="oracle tuple loop (numpy/BLAS) on %d of the %d tuples of %s (a<=b<=c<%d), "
-                       "%.1f s; seconds = reference flops / measured rate" % (
-                           tuples, all_tuples, cfg, n, dt))
+    rate = len(work) * per_tuple / dt
+    return dict(seconds=otr.triples_flops(o, v) / rate, rate_tflops=rate / 1e12, cores=cores,
+                sample="oracle tuple loop (numpy, one BLAS thread per process) on %d of the %d "
+                       "tuples of %s (a<=b<=c<%d) spread over %d processes, %.1f s; seconds = "
+                       "reference flops / measured rate" % (len(work), all_tuples, cfg, n, cores, dt))
 
 
 def run_triples(args, local):

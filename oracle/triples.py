@@ -87,12 +87,13 @@ def _atrip_doubles(a, b, c, T2, Vppph, Vhhhp, cplx):
     return W
 
 
-def triples_atrip(T1, T2, V, eps_h, eps_p):
-    """Atrip.cxx:447-525, 640: -sum over tuples of getEnergyDistinct / getEnergySame."""
+def tuple_energy(a, b, c, T1, T2, V, eps_h, eps_p):
+    """Contribution of one tuple a <= b <= c (not all equal) to the sum of
+    Atrip.cxx:500-525 (getEnergyDistinct / getEnergySame), before the final sign."""
     Vpphh, Vppph, Vhhhp = V["pphh"], V["ppph"], V["hhhp"]
     cplx = np.iscomplexobj(T2) or np.iscomplexobj(Vppph)
     cj = np.conj if cplx else (lambda x: x)
-    Nv, No = T1.shape
+    No = T1.shape[1]
     eh = np.asarray(eps_h, dtype=float)
     ep = np.asarray(eps_p, dtype=float)
     i, j, k = np.meshgrid(np.arange(No), np.arange(No), np.arange(No), indexing="ij")
@@ -100,31 +101,35 @@ def triples_atrip(T1, T2, V, eps_h, eps_p):
     i, j, k = i[keep], j[keep], k[keep]
     fac = np.where(i == j, 0.5, 1.0) * np.where(j == k, 0.5, 1.0)
     eijk = eh[i] + eh[j] + eh[k]
-    total = 0.0
-    for a in range(Nv):
-        for b in range(a, Nv):
-            for c in range(b, Nv):
-                if a == b == c:
-                    continue
-                Wt = _atrip_doubles(a, b, c, T2, Vppph, Vhhhp, cplx)
-                Zt = (Wt + es("i,jk->ijk", T1[a], Vpphh[b, c]) + es("j,ik->ijk", T1[b], Vpphh[a, c])
-                      + es("k,ij->ijk", T1[c], Vpphh[a, b]))
-                den = ep[a] + ep[b] + ep[c] - eijk
-                U, Vv, Ww, X, Y, Z = (Zt[i, j, k], Zt[i, k, j], Zt[j, i, k], Zt[j, k, i],
-                                       Zt[k, i, j], Zt[k, j, i])
-                A, B, C, Dd, E, F = (cj(Wt[i, j, k]), cj(Wt[i, k, j]), cj(Wt[j, i, k]),
-                                     cj(Wt[j, k, i]), cj(Wt[k, i, j]), cj(Wt[k, j, i]))
-                if a != b and b != c:
-                    value = (3.0 * (A * U + B * Vv + C * Ww + Dd * X + E * Y + F * Z)
-                             + ((U + X + Y) - 2.0 * (Vv + Ww + Z)) * (A + Dd + E)
-                             + ((Vv + Ww + Z) - 2.0 * (U + X + Y)) * (B + C + F))
-                else:
-                    # getEnergySame: U, V, W = Z[ijk], Z[jki], Z[kij]
-                    U3, V3, W3 = Zt[i, j, k], Zt[j, k, i], Zt[k, i, j]
-                    A3, B3, C3 = cj(Wt[i, j, k]), cj(Wt[j, k, i]), cj(Wt[k, i, j])
-                    value = 3.0 * (A3 * U3 + B3 * V3 + C3 * W3) - (A3 + B3 + C3) * (U3 + V3 + W3)
-                total += float(np.real(np.sum(2.0 * value / den * fac)))
-    return -total
+    Wt = _atrip_doubles(a, b, c, T2, Vppph, Vhhhp, cplx)
+    Zt = (Wt + es("i,jk->ijk", T1[a], Vpphh[b, c]) + es("j,ik->ijk", T1[b], Vpphh[a, c])
+          + es("k,ij->ijk", T1[c], Vpphh[a, b]))
+    den = ep[a] + ep[b] + ep[c] - eijk
+    if a != b and b != c:
+        U, Vv, Ww, X, Y, Z = (Zt[i, j, k], Zt[i, k, j], Zt[j, i, k], Zt[j, k, i],
+                               Zt[k, i, j], Zt[k, j, i])
+        A, B, C, Dd, E, F = (cj(Wt[i, j, k]), cj(Wt[i, k, j]), cj(Wt[j, i, k]),
+                             cj(Wt[j, k, i]), cj(Wt[k, i, j]), cj(Wt[k, j, i]))
+        value = (3.0 * (A * U + B * Vv + C * Ww + Dd * X + E * Y + F * Z)
+                 + ((U + X + Y) - 2.0 * (Vv + Ww + Z)) * (A + Dd + E)
+                 + ((Vv + Ww + Z) - 2.0 * (U + X + Y)) * (B + C + F))
+    else:
+        # getEnergySame: U, V, W = Z[ijk], Z[jki], Z[kij]
+        U3, V3, W3 = Zt[i, j, k], Zt[j, k, i], Zt[k, i, j]
+        A3, B3, C3 = cj(Wt[i, j, k]), cj(Wt[j, k, i]), cj(Wt[k, i, j])
+        value = 3.0 * (A3 * U3 + B3 * V3 + C3 * W3) - (A3 + B3 + C3) * (U3 + V3 + W3)
+    return float(np.real(np.sum(2.0 * value / den * fac)))
+
+
+def tuples(Nv):
+    """The tuples of Tuples.hpp:158-185: a <= b <= c < Nv without a == b == c."""
+    return [(a, b, c) for a in range(Nv) for b in range(a, Nv) for c in range(b, Nv)
+            if not a == b == c]
+
+
+def triples_atrip(T1, T2, V, eps_h, eps_p):
+    """Atrip.cxx:447-525, 640: -sum over tuples of getEnergyDistinct / getEnergySame."""
+    return -sum(tuple_energy(a, b, c, T1, T2, V, eps_h, eps_p) for a, b, c in tuples(T1.shape[0]))
 
 
 def triples_flops(No, Nv):
