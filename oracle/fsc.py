@@ -85,6 +85,29 @@ def tricubic(F, bounds, origin, x):
     return total
 
 
+def tricubic_many(F, bounds, origin, X):
+    """``tricubic`` at many points at once (X [n, 3]), the same arithmetic vectorised."""
+    nb = np.asarray(bounds, dtype=np.int64)
+    X = np.asarray(X, dtype=float)
+    idx, w = [], []
+    for d in range(3):
+        t = X[:, d] - origin[d]
+        i = np.clip(np.trunc(t).astype(np.int64), 0, nb[d] - 1)
+        u = t - i
+        pw = np.stack([np.ones_like(u), u, u * u, u * u * u], axis=1)   # [n, 4]
+        w.append(pw @ CATMULL_ROM.T)                                     # [n, 4]
+        idx.append(i - 1)
+    total = np.zeros(X.shape[0])
+    for s in range(4):
+        z = np.clip(idx[2] + s, 0, nb[2] - 1)
+        for r in range(4):
+            y = np.clip(idx[1] + r, 0, nb[1] - 1)
+            for c in range(4):
+                x = np.clip(idx[0] + c, 0, nb[0] - 1)
+                total += w[0][:, c] * w[1][:, r] * w[2][:, s] * F[x + nb[0] * (y + nb[1] * z)]
+    return total
+
+
 def box_of(grid, B):
     """Inverse basis A, box dimensions, origin and the S(G) placement indices."""
     B = np.asarray(B, dtype=float)

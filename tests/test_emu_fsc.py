@@ -153,3 +153,14 @@ def test_fsc_grid_sizes_and_default_potential(emu_lib, N, NF):
         sol.close()
     assert np.abs(S - S_ref).max() < 1e-12 * np.abs(S_ref).max()
     assert abs(e["correction"] - E_ref["correction"]) < 1e-11 * abs(E_ref["corrected"])
+
+
+def test_vectorised_tricubic_equals_the_scalar_one():
+    rng = np.random.default_rng(4)
+    dims = np.array([6, 5, 7])
+    origin = np.array([-3.0, -2.0, -3.0])
+    F = rng.standard_normal(dims.prod())
+    X = origin + rng.random((200, 3)) * (dims + 2) - 1.0   # inside, near and beyond the edges
+    a = fsc.tricubic_many(F, dims, origin, X)
+    b = np.array([fsc.tricubic(F, dims, origin, x) for x in X])
+    assert np.abs(a - b).max() < 1e-13 * np.abs(b).max()
