@@ -7,9 +7,6 @@ import socket
 import subprocess
 import sys
 
-import numpy as np
-import pytest
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
 
