@@ -896,9 +896,13 @@ __global__ void fsc_box_kernel(double* box, const double* S, const double* grid,
     double x[3];
     fsc_direct(g, v, x);
     int64_t i[3];
+    bool in = true;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) i[d] = static_cast<int64_t>(floor(x[d] + 0.5) - g.origin[d]);
-    box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
+    for (int d = 0; d < 3; ++d) {
+      i[d] = static_cast<int64_t>(floor(x[d] + 0.5) - g.origin[d]);
+      in = in && i[d] >= 0 && i[d] < g.dims[d];  // the box was sized on the host: never write outside
+    }
+    if (in) box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
   }
 }
 

@@ -522,8 +522,12 @@ void fsc_box(double* box, const double* S, const double* grid, const FscGeometry
     double x[3];
     fsc_direct_emu(g, grid + 3 * e, x);
     int64_t i[3];
-    for (int d = 0; d < 3; ++d) i[d] = static_cast<int64_t>(std::floor(x[d] + 0.5) - g.origin[d]);
-    box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
+    bool in = true;
+    for (int d = 0; d < 3; ++d) {
+      i[d] = static_cast<int64_t>(std::floor(x[d] + 0.5) - g.origin[d]);
+      in = in && i[d] >= 0 && i[d] < g.dims[d];
+    }
+    if (in) box[i[0] + g.dims[0] * (i[1] + g.dims[1] * i[2])] = S[e];
   }
 }
 
