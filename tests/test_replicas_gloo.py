@@ -64,3 +64,56 @@ def test_two_gloo_replicas(tmp_path):
     for r in res:
         assert abs(r["energy"] - ref["energy"]["correlation"]) < 1e-10 * max(1.0, abs(r["energy"]))
         assert r["launches"] > 0
+
+
+RUN_OURS_SCRIPT = r"""
+import json, os, sys, argparse
+sys.path.insert(0, os.environ["REPO_ROOT"])
+import torch, torch.distributed as dist
+dist.init_process_group("gloo", init_method="env://")
+torch.cuda.set_device = lambda *a, **k: None     # host-only stand-ins for the device calls
+torch.cuda.synchronize = lambda *a, **k: None
+import bench
+from cc4s_b200 import coupled_cluster as ccm
+_stats = ccm.Solver.stats
+def _floored_stats(self):                        # emulated events read 0 s
+    d = _stats(self)
+    for k in ("gemm_seconds", "split_seconds", "top_seconds"):
+        d[k] = max(d[k], 1e-3)
+    return d
+ccm.Solver.stats = _floored_stats
+bench.dgemm_peak = lambda local: 35.0
+_all_max = bench.all_max
+bench.all_max = lambda x, world: max(_all_max(x, world), 1e-3)  # emulated events read 0 s
+bench.CONFIG_SHAPES["custom"] = (3, 9, 14)
+args = argparse.Namespace(config="custom", steps=1, warmup=1, precision="both", vertex_scale=None)
+line = bench.run_ours(args, dist.get_world_size(), dist.get_rank(), 0)
+json.dump(line, open(os.environ["OUT_PREFIX"] + str(dist.get_rank()) + ".json", "w"))
+dist.destroy_process_group()
+"""
+
+
+def test_two_gloo_ranks_run_the_bench_replica_line(tmp_path):
+    """The whole replica line of bench.py at world size 2: both ranks take the same
+    collective steps, only the headline split form is timed, n_gpus and the
+    aggregate value count both replicas."""
+    import build_emu
+    lib = build_emu.build()
+    port = _free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2",
+                   RANK=str(rank), LOCAL_RANK="0", CC4S_B200_LIB=lib, REPO_ROOT=ROOT,
+                   OUT_PREFIX=str(tmp_path / "line"))
+        procs.append(subprocess.Popen([sys.executable, "-c", RUN_OURS_SCRIPT], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
+    for p in procs:
+        out, _ = p.communicate(timeout=300)
+        assert p.returncode == 0, out.decode()[-3000:]
+    lines = [json.load(open(tmp_path / ("line%d.json" % r))) for r in range(2)]
+    for line in lines:
+        assert line["n_gpus"] == 2
+        assert line["config"]["parallelism"] == "replicas"
+        assert line["config"]["precision"] == "split3"
+        assert "fp64_s_per_iter" not in line["config"]
+    assert lines[0]["value"] == lines[1]["value"]
