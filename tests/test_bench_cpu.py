@@ -1,0 +1,68 @@
+"""The JSON lines of bench.py's secondary modes (--triples, --fsc) and of the
+reference arm, produced on the host: the library calls go to the CPU emulation
+library (tests/emu), the device-only calls are stood in for, and the emulated
+device times (0 s) are floored.  This checks the keys of each line, not numbers."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
+
+SCRIPT = r"""
+import json, os, sys
+sys.path.insert(0, os.environ["REPO_ROOT"])
+import torch
+torch.cuda.set_device = lambda *a, **k: None
+torch.cuda.synchronize = lambda *a, **k: None
+import bench
+_median = bench.statistics.median
+bench.statistics.median = lambda xs: max(_median(list(xs)), 1e-3)
+bench.dgemm_peak = lambda local: 35.0
+sys.argv = ["bench.py"] + json.loads(os.environ["BENCH_ARGS"])
+if __name__ == "__main__":
+    bench.main()
+"""
+
+COMMON = {"metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+          "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config", "e2e"}
+
+
+def _line(lib, args):
+    env = dict(os.environ, CC4S_B200_LIB=lib, REPO_ROOT=ROOT, BENCH_ARGS=json.dumps(args))
+    out = subprocess.run([sys.executable, "-c", SCRIPT], env=env, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def test_triples_line():
+    import build_emu
+    line = _line(build_emu.build(), ["--triples", "--shape", "2,6,10", "--warmup", "1",
+                                      "--steps", "1"])
+    assert COMMON <= set(line)
+    assert {"roofline", "cpu_baseline", "gpu_launches", "clocks"} <= set(line)
+    assert set(line["config"]["forms"]) == {"fp64", "split3"}
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] > 0
+
+
+def test_fsc_line():
+    import build_emu
+    line = _line(build_emu.build(), ["--fsc", "--shape", "2,6,10", "--fsc-grid", "4",
+                                      "--fsc-n", "2", "--warmup", "1", "--steps", "1"])
+    assert COMMON <= set(line)
+    assert line["config"]["points"] == (2 * 2) ** 3 * 64
+    assert line["config"]["box"] == [4, 4, 4]
+    assert {"cpu_baseline", "gpu_launches"} <= set(line)
+
+
+def test_reference_line():
+    import build_emu
+    line = _line(build_emu.build(), ["--impl", "reference", "--config", "c0", "--warmup", "1",
+                                      "--steps", "1"])
+    assert line["impl"] == "reference"
+    assert COMMON <= set(line)
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["value"] == line["value"]
