@@ -20,6 +20,16 @@ import bench
 _median = bench.statistics.median
 bench.statistics.median = lambda xs: max(_median(list(xs)), 1e-3)
 bench.dgemm_peak = lambda local: 35.0
+from cc4s_b200 import coupled_cluster as ccm
+_stats = ccm.Solver.stats
+def _floored_stats(self):
+    d = _stats(self)
+    for k in ("gemm_seconds", "split_seconds", "top_seconds"):
+        d[k] = max(d[k], 1e-3)
+    return d
+ccm.Solver.stats = _floored_stats
+_all_max = bench.all_max
+bench.all_max = lambda x, world: max(_all_max(x, world), 1e-3)
 sys.argv = ["bench.py"] + json.loads(os.environ["BENCH_ARGS"])
 if __name__ == "__main__":
     bench.main()
@@ -66,3 +76,16 @@ def test_reference_line():
     assert COMMON <= set(line)
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["cpu_baseline"]["value"] == line["value"]
+
+
+def test_ccsd_line():
+    """The default line (both forms at one GPU) on a small custom shape."""
+    import build_emu
+    line = _line(build_emu.build(), ["--shape", "3,9,14", "--warmup", "3", "--steps", "1"])
+    assert COMMON <= set(line)
+    assert {"roofline", "cpu_baseline", "gpu_launches", "clocks"} <= set(line)
+    assert {"bound", "achieved", "peak", "unit", "frac", "traffic"} <= set(line["roofline"])
+    assert {"value", "unit", "cores", "kind", "sample"} <= set(line["cpu_baseline"])
+    assert {"value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"} <= set(line["e2e"])
+    assert "split_speedup_vs_fp64" in line["config"] and line["n_gpus"] == 1
+    assert line["warmup"] == 3 and line["steps"] == 1
