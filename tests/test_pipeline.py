@@ -210,3 +210,28 @@ def test_tensor_file_text_complex(tmp_path):
     lines = (tmp_path / "C.elements").read_text().split()
     assert lines[0] == "(1,2)" and lines[1] == "(0,0.5)"   # column-major: v[0,0], v[1,0]
     assert np.array_equal(tensor_io.read(str(tmp_path / "C.yaml")).values, v)
+
+
+@pytest.mark.parametrize("step", ["PerturbativeTriples", "PerturbativeTriplesReference"])
+def test_input_chain_complex_triples_step_names(tmp_path, emu_lib, step):
+    """Complex chain: the step name selects the conjugation of the (T) energy
+    (atrip's Re conj(W) Z or the array form's Re conj(W) conj(Z))."""
+    import yaml
+    from cc4s_b200 import pipeline
+    from oracle import triples
+    s = inputs.synthetic_system(2, 6, 12, complex=True, seed=5)
+    _write_system(tmp_path, s, False, True)
+    steps = STEPS[:-1] + [
+        {"name": step,
+         "in": {"coulombIntegrals": "CoulombIntegrals", "amplitudes": "Amplitudes",
+                "slicedEigenEnergies": "EigenEnergies"},
+         "out": {"energy": "TriplesEnergy"}}]
+    with open(tmp_path / "cc4s.in", "w") as f:
+        yaml.safe_dump(steps, f, sort_keys=False)
+    sym = pipeline.run_file(str(tmp_path / "cc4s.in"), lib=emu_lib)
+    T1 = sym["Amplitudes"]["ph"].values
+    T2 = sym["Amplitudes"]["pphh"].values
+    V = triples.triples_integrals(s)
+    f = triples.triples_reference if step.endswith("Reference") else triples.triples_atrip
+    e = f(T1, T2, V, s.eps_h, s.eps_p)
+    assert abs(sym["TriplesEnergy"]["correlation"] - e) < 1e-11 * max(1.0, abs(e))
