@@ -2,24 +2,33 @@
 
 A "step" is one CCSD iteration (residual, Jacobi update, DIIS, energy) on a
 seeded synthetic system.  Default workload: No=64, Nv=640, NG=2560, real
-(T2 13.4 GB), both the split-precision tensor-core form (headline) and the
-FP64 form, W warm-up and K timed iterations each.  T2 and the vertex are far
-larger than L2, so no flush is needed between iterations.
+(T2 13.4 GB), vertex scaled by 0.3 (CCSD diverges on the unscaled synthetic
+vertex; the cost of an iteration does not depend on the scale).  T2 and the
+vertex are far larger than L2, so no flush is needed between iterations.
+
+Order of the CCSD line (single GPU):
+ 1. the headline split-precision form: W warm-up + K timed iterations (the
+    first warm-up is the cheap R = V iteration), with CUDA events around every
+    contraction launch on the library stream for the roofline;
+ 2. e2e: the same metric through the C ABI from host buffers: set_inputs
+    (vertex upload and integral build) + the first iteration + a bounded
+    number of full iterations (--e2e-iterations) + amplitude download, wall
+    clock; only the full iterations' flops count;
+ 3. the FP64 form for the speed-up, a bounded number of iterations
+    (--fp64-warmup, --fp64-steps), skipped if it would pass --time-budget;
+ 4. the CPU baseline: one full oracle iteration of a quarter-size system.
 
 value: reference-equivalent TFLOP/s = F_ref / (s per iteration), with F_ref
 the flop count of the reference's formulation (cc4s_b200.flops), timed with
 CUDA events on the library's stream inside the library, max over ranks.
-e2e: the same metric through the C ABI from host buffers: set_inputs (vertex
-upload and integral build) + the first (MP2) iteration + K full iterations +
-amplitude download, wall clock; only the K full iterations' flops count.
 
 Multi-GPU: every rank runs its own replica of the workload (weak scaling, no
 collective on the data path); value is the sum over ranks.
 
 --impl reference: the CPU restatement of the reference (the oracle; the
 reference itself needs MPI and the Cyclops Tensor Framework, which are not
-installed) timed on this host's cores on a bounded sample of the same
-workload.
+installed), one full iteration of a quarter-size system per step, on all host
+cores.
 --adjoint: relaxed-gradient (Lambda equations) timing and finite-difference
 check; --converge: converged energies of the FP64, split and refined forms;
 --triples: the perturbative triples (T) step after CCSD; --fsc: the
@@ -120,41 +129,71 @@ def dgemm_peak(device):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_sample(cfg, target=2e12):
-    """CPU rate of the oracle on the workload's dominant contractions (bounded sample).
+def cores_available():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
-    Times, with the oracle's numpy/BLAS restatement on all host cores, a block of
-    the (vo)^3 ring contraction (virtual indices a, b restricted to n values) and
-    one particle-particle-ladder slice pair (sl x sl virtual pairs, occupied pairs
-    restricted to m x m), each sized to about `target` flops, on random operands
-    of the workload's shapes; the measured rate converts the reference
-    formulation's flops into seconds per iteration.
-    """
-    import numpy as np
-    from oracle import ccsd as occ
-    from cc4s_b200.flops import reference_flops
+
+def sample_shape(cfg):
+    """The CPU sample system: the workload's generator at a quarter of each
+    dimension (c2: No=16, Nv=160, NG=640), so that one full oracle iteration
+    takes seconds instead of hours."""
     o, v, G = CONFIG_SHAPES[cfg]
-    rng = np.random.default_rng(0)
-    n = int(min(v, max(1, (target / (2.0 * v * o ** 3)) ** 0.5)))
-    Y = rng.standard_normal((n, o, o, v))
-    X = rng.standard_normal((v, n, o, o))
-    m = min(o, 16)
-    sl = int(min(o, max(1, (target / (2.0 * v * v * (G + m * m))) ** 0.5)))
-    dG = rng.standard_normal((G, 2 * sl, v)) * 0.1 * G ** -0.25
-    Xl = rng.standard_normal((v, v, m, m))
-    t0 = time.perf_counter()
-    occ.es("akic,cbkj->abij", Y, X)
-    V = occ.es("Gxc,Gyd->xycd", dG[:, :sl, :], dG[:, sl:, :])
-    occ.es("xycd,cdij->xyij", V, Xl)
-    t1 = time.perf_counter()
-    flops = 2.0 * n * n * v * o ** 3 + 2.0 * sl * sl * v * v * (G + m * m)
-    rate = flops / (t1 - t0)
-    s_iter = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS) / rate
-    return dict(s_per_iter=s_iter, rate_tflops=rate / 1e12, sample_seconds=t1 - t0,
-                cores=os.cpu_count(),
-                sample="oracle numpy/BLAS on %s: ring block a,b < %d of akic,cbkj->abij and one "
-                       "ladder slice pair (%d x %d virtuals, %d x %d occupied pairs), %.2g flops; "
-                       "s/iter = reference flops / measured rate" % (cfg, n, sl, sl, m, m, flops))
+    return max(2, o // 4), max(4, v // 4), max(8, G // 4)
+
+
+class OracleSteps:
+    """One CoupledCluster iteration per step of the oracle (the CPU restatement
+    of CoupledCluster.cxx:129-175 with the Ccsd residual of Ccsd.cxx:77-378 and
+    the DIIS mixer of DiisMixer.cxx), numpy/BLAS on all host cores, on the
+    sample system of `cfg` (same seeded generator and vertex scale).  The first
+    step is the cheap first iteration (R = V); every later one is a full
+    iteration."""
+
+    def __init__(self, cfg, vertex_scale):
+        from oracle import coupled_cluster, inputs
+        from cc4s_b200.flops import reference_flops
+        from cc4s_b200.synthetic import synthetic
+        self.cfg = cfg
+        self.shape = sample_shape(cfg)
+        o, v, G = self.shape
+        cplx = cfg in COMPLEX_CONFIGS
+        eh, ep, g, hg = synthetic(o, v, G, complex=cplx, seed=0)
+        g *= vertex_scale
+        self.system = inputs.System(eh, ep, g, half_grid=hg)
+        self.flops = reference_flops(o, v, G, complex=cplx)
+        self.it = coupled_cluster.iterations(self.system, None, method="Ccsd",
+                                             mixer=dict(type="DiisMixer", maxResidua=5),
+                                             energyConvergence=-1.0, amplitudesConvergence=-1.0)
+        self.steps = 0
+
+    def step(self):
+        t0 = time.perf_counter()
+        next(self.it)
+        dt = time.perf_counter() - t0
+        self.steps += 1
+        return dt
+
+    def describe(self, seconds):
+        o, v, G = self.shape
+        return ("oracle (numpy/BLAS, %d threads): full CoupledCluster iterations (Ccsd residual, "
+                "Jacobi, DIIS 5, energy) of the %s generator at a quarter of each dimension "
+                "(No=%d Nv=%d NG=%d, %.3g reference flops per iteration), %.2f s per iteration"
+                % (cores_available(), self.cfg, o, v, G, self.flops, seconds))
+
+
+def cpu_sample(cfg, vertex_scale, full_iterations=1):
+    """Bounded CPU baseline: the first (cheap) iteration and `full_iterations`
+    full iterations of OracleSteps; the rate of the full ones in TFLOP/s of the
+    reference formulation."""
+    run = OracleSteps(cfg, vertex_scale)
+    run.step()
+    secs = [run.step() for _ in range(full_iterations)]
+    s = statistics.median(secs)
+    return dict(rate_tflops=run.flops / s / 1e12, seconds=s, cores=cores_available(),
+                sample=run.describe(s))
 
 
 def dist_setup():
@@ -192,7 +231,7 @@ def barrier(world):
         dist.barrier()
 
 
-def timed_run(opts, inputs, W, K, world, local, keep_amplitudes=True):
+def timed_run(opts, inputs, W, K, world, local, keep_amplitudes=False):
     """W + K iterations; the last K are timed (CUDA events on the library stream)."""
     from cc4s_b200 import Solver
     eh, ep, g, hg = inputs
@@ -210,13 +249,52 @@ def timed_run(opts, inputs, W, K, world, local, keep_amplitudes=True):
                 (st1["other_launches"] - st0["other_launches"])) / (W + K)
     T = sol.amplitudes() if keep_amplitudes else None
     sol.close()
-    return dict(t=t, r=r, launches=launches, T=T, clocks=clk.summary())
+    return dict(t=t, r=r, launches=launches, T=T, clocks=clk.summary(), stats=st1,
+                secs=secs)
+
+
+# Default vertex scale of the CCSD line: the synthetic systems of c1, c2 and c4
+# are strongly correlated and CCSD from T = 0 diverges on the unscaled vertex
+# (E_c of about -3200 Eh after four iterations at c2); at 0.3 it converges.  The
+# cost of an iteration does not depend on the scale.
+DEFAULT_VERTEX_SCALE = 0.3
+# Upper bound of the FP64 form's time per iteration relative to the split form,
+# used only to decide whether the FP64 comparison still fits the time budget
+# (measured at c2: 3.3).
+FP64_OVER_SPLIT_BOUND = 4.5
+
+
+# Measured on one B200 at c2 (No=64, Nv=640, NG=2560, real): seconds per full
+# iteration of each form (CUDA events), and wall seconds of the host-side input
+# generation, of one handle's set-up (vertex upload, integral build) and of the
+# CPU baseline leg.  projected_seconds() uses them to check that the driver's
+# command fits its time limit.
+MEASURED_C2 = {"split3": 20.96, "fp64": 69.68, "inputs": 60.0, "setup": 30.0, "cpu": 40.0,
+               "download": 15.0}
+
+
+def projected_seconds(W, K, e2e_iterations=2, fp64_warmup=2, fp64_steps=2, m=MEASURED_C2):
+    """Projected wall seconds of each leg of the c2 CCSD line."""
+    s, s64 = m["split3"], m["fp64"]
+    n_e2e = max(1, min(K, e2e_iterations))
+    return {"inputs": m["inputs"],
+            "headline": m["setup"] + (W - 1 + K) * s + 0.1 * s,
+            "e2e": m["setup"] + n_e2e * s + 0.1 * s + m["download"],
+            "fp64": m["setup"] + (max(1, fp64_warmup) - 1 + fp64_steps) * s64 + 0.1 * s64,
+            "dgemm_peak": 5.0, "cpu_baseline": m["cpu"]}
 
 
 def run_ours(args, world, rank, local):
+    """The CCSD line: headline form first (W warm-up + K timed iterations, the
+    contractions' per-launch CUDA events recorded inside the timed region),
+    then an e2e leg of a bounded number of iterations from host buffers, then
+    the FP64 comparison (1 warm-up + a bounded number of timed iterations) if
+    it fits the remaining time budget."""
     import torch
     from cc4s_b200 import Solver, reference_flops
     from cc4s_b200.synthetic import config
+    t_begin = time.perf_counter()
+    deadline = t_begin + args.time_budget
     torch.cuda.set_device(local)
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
@@ -226,33 +304,53 @@ def run_ours(args, world, rank, local):
     else:
         inputs = config(cfg, seed=0)
     eh, ep, g, hg = inputs
-    if args.vertex_scale is not None:
-        g *= args.vertex_scale
+    scale = DEFAULT_VERTEX_SCALE if args.vertex_scale is None else args.vertex_scale
+    if scale != 1.0:
+        g *= scale
     F = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS)
     K, W = args.steps, args.warmup
-    base = dict(maxIterations=W + K, energyConvergence=-1.0, amplitudesConvergence=-1.0,
+    base = dict(energyConvergence=-1.0, amplitudesConvergence=-1.0,
                 mixer=dict(type="DiisMixer", maxResidua=5), device=local)
-    # the FP64 form is the single-GPU comparison of the two forms; replicas under
-    # torchrun time the headline form only, so the GPUs are held for less time
-    if args.precision == "both":
-        forms = ["fp64", "split3"] if world == 1 else ["split3"]
-    else:
-        forms = [args.precision]
-    head = "split3" if "split3" in forms else "fp64"
-    runs = {p: timed_run(dict(base, precision=p), inputs, W, K, world, local,
-                         keep_amplitudes=(p == head)) for p in forms}
-    hr = runs[head]
+    head = "fp64" if args.precision == "fp64" else "split3"
+    # 1. headline form, with per-launch events on the library stream
+    hr = timed_run(dict(base, precision=head, maxIterations=W + K, profile=True), inputs, W, K,
+                   world, local)
     t = hr["t"]
-    # dominant kernel: per-launch CUDA events around every contraction of one
-    # residual, evaluated at the amplitudes the timed run ended with
-    prof = Solver(dict(base, precision=head, profile=True, maxIterations=1))
-    prof.set_inputs(eh, ep, g, half_grid=hg)
-    prof.set_initial_amplitudes(*hr["T"])
-    hr["T"] = None
-    prof.run()
-    ps = prof.stats()
-    prof.close()
+    ps = hr["stats"]
     pk = peaks()
+    # 2. end to end through the C ABI from host buffers: vertex upload and
+    # integral build, the cheap first iteration, n_e2e full iterations and the
+    # amplitude download; only the full iterations' flops are counted
+    n_e2e = max(1, min(K, args.e2e_iterations))
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e = Solver(dict(base, precision=head, maxIterations=n_e2e + 1))
+    e2e.set_inputs(eh, ep, g, half_grid=hg)
+    re = e2e.run()
+    A1, A2 = e2e.amplitudes()
+    torch.cuda.synchronize()
+    t_e2e = all_max(time.perf_counter() - t0, world)
+    e2e.close()
+    h2d = (g.nbytes + eh.nbytes + ep.nbytes) / n_e2e
+    d2h = (A1.nbytes + A2.nbytes) / n_e2e + 5 * 8 + 8
+    del A1, A2
+    # 3. FP64 comparison (single GPU): args.fp64_warmup warm-up iterations (the
+    # first one is the cheap R = V iteration) and args.fp64_steps timed full
+    # iterations, if the projection fits the budget
+    runs = {head: hr}
+    fp64_note = None
+    W64 = max(1, args.fp64_warmup)
+    if world == 1 and args.precision == "both":
+        s_split = t / K
+        projected = ((W64 - 1 + args.fp64_steps) * FP64_OVER_SPLIT_BOUND * s_split +
+                     max(0.0, t_e2e - (n_e2e + 1) * s_split) + 60.0)
+        if time.perf_counter() + projected < deadline:
+            runs["fp64"] = timed_run(dict(base, precision="fp64",
+                                          maxIterations=W64 + args.fp64_steps),
+                                     inputs, W64, args.fp64_steps, world, local)
+        else:
+            fp64_note = ("skipped: projected %.0f s would pass the %.0f s time budget"
+                         % (projected, args.time_budget))
     dpeak = dgemm_peak(local)
     if head == "split3":
         # executed FP16 tensor work: six slice products per FP64-equivalent multiply-add
@@ -260,61 +358,55 @@ def run_ours(args, world, rank, local):
         peak = pk.get("bf16_tflops_sustained", 1405.3)
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": "split_kernel (tcgen05.mma kind::f16, TMEM, TMA) incl. operand slicing, "
-                          "%d launches of one residual" % ps["split_launches"],
+                "kernel": "split_kernel_persistent (tcgen05.mma kind::f16, TMEM, TMA) incl. operand "
+                          "slicing: %d launches of the last timed iteration, CUDA events on the "
+                          "library stream" % ps["split_launches"],
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
                 "fp64_equivalent_tflops": ps["split_flops"] / ps["split_seconds"] / 1e12}
     else:
         achieved = ps["gemm_flops"] / ps["gemm_seconds"] / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
                 "frac": achieved / dpeak, "traffic": None,
-                "kernel": "gemm_f64_kernel (mma.sync m16n8k16 f64), all %d contraction launches "
-                          "of one residual" % ps["gemm_profiled_launches"],
+                "kernel": "gemm_f64_kernel (mma.sync m16n8k16 f64): all %d contraction launches "
+                          "of the last timed iteration" % ps["gemm_profiled_launches"],
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured; no FP64 "
                                "entry in MEASURED_PEAKS.json)",
                 "top_launch_tflops": ps["top_flops"] / ps["top_seconds"] / 1e12}
-    # end to end through the C ABI from host buffers
-    barrier(world)
-    t0 = time.perf_counter()
-    # the first iteration is the cheap one (R = V, the MP2 step); K full
-    # iterations follow it, and only their flops are counted
-    e2e = Solver(dict(base, precision=head, maxIterations=K + 1))
-    e2e.set_inputs(eh, ep, g, half_grid=hg)
-    re = e2e.run()
-    A1, A2 = e2e.amplitudes()
-    torch.cuda.synchronize()
-    t_e2e = all_max(time.perf_counter() - t0, world)
-    e2e.close()
-    h2d = (g.nbytes + eh.nbytes + ep.nbytes) / K
-    d2h = (A1.nbytes + A2.nbytes) / K + 5 * 8 + 8
     kind = "complex" if cfg in COMPLEX_CONFIGS else "real"
     conf = {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, %s" % (cfg, o, v, G, kind, head),
-            "precision": head, "s_per_iter": t / K,
+            "precision": head, "s_per_iter": t / K, "vertex_scale": scale,
+            "s_per_iter_all": hr["secs"][W:W + K],
             "flops_per_iter_reference_formulation": F,
             "flops_per_iter_executed": hr["r"]["flops_per_iteration"],
-            "l2": "inputs larger than L2 (T2 %.2f GB)" % ((v * o) ** 2 * 8 / 1e9),
+            "l2": "inputs larger than L2 (T2 %.2f GB), no flush" % ((v * o) ** 2 * 8 / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
             "energy_after_steps": hr["r"]["correlation"],
-            "fp64_dgemm_peak_tflops": dpeak}
-    if "fp64" in runs and "split3" in runs:
+            "residuum_norm_after_steps": hr["r"]["history"][-1]["dR"],
+            "fp64_dgemm_peak_tflops": dpeak, "e2e_iterations": n_e2e,
+            "time_budget_s": args.time_budget}
+    if "fp64" in runs:
         t64 = runs["fp64"]["t"]
-        conf.update({"fp64_s_per_iter": t64 / K, "fp64_tflops": world * F / (t64 / K) / 1e12,
-                     "split_speedup_vs_fp64": t64 / t,
-                     "abs_dE_after_steps_split_vs_fp64":
-                         abs(runs["split3"]["r"]["correlation"] - runs["fp64"]["r"]["correlation"])})
+        s64 = t64 / args.fp64_steps
+        conf.update({"fp64_s_per_iter": s64, "fp64_tflops": F / s64 / 1e12,
+                     "fp64_timed_iterations": args.fp64_steps, "fp64_warmup": W64,
+                     "split_speedup_vs_fp64": s64 / (t / K)})
+    elif fp64_note:
+        conf["fp64"] = fp64_note
     line = {
         "metric": METRIC, "value": world * F / (t / K) / 1e12, "unit": "TFLOP/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": 1e3 * t / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded generator of the workload's distributions)",
+        "data": "synthetic (seeded generator of the workload's distributions, vertex x%g)" % scale,
         "config": conf,
-        "e2e": {"value": world * F * K / t_e2e / 1e12, "unit": "TFLOP/s",
+        "e2e": {"value": world * F * n_e2e / t_e2e / 1e12, "unit": "TFLOP/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "seconds": t_e2e, "iterations": re["iterations"]},
+                "seconds": t_e2e, "iterations": re["iterations"],
+                "counted_iterations": n_e2e},
         "gpu_launches": int(round(hr["launches"] * K)),
         "roofline": roof,
         "clocks": hr["clocks"],
     }
+    line["config"]["wall_seconds_to_line"] = time.perf_counter() - t_begin
     return line
 
 
@@ -681,26 +773,44 @@ def run_fsc(args, local):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference's algorithm on the host cores.  The
+    reference itself (CTF + MPI + yaml-cpp) cannot be built here, so its CPU
+    restatement (the oracle, numpy/BLAS on all host threads) runs instead: each
+    step is one full CoupledCluster iteration of the workload's generator at a
+    quarter of each dimension (OracleSteps), and value is the reference
+    formulation's flops of that iteration per second.  ms_per_step and steps
+    describe those iterations; the c2 time per iteration at that rate is
+    reported under config as an extrapolation."""
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
     from cc4s_b200.flops import reference_flops
+    scale = DEFAULT_VERTEX_SCALE if args.vertex_scale is None else args.vertex_scale
     F = reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS)
-    for _ in range(args.warmup):
-        cpu_sample(cfg)
-    samples = [cpu_sample(cfg) for _ in range(max(1, args.steps))]
-    s_iter = statistics.median(x["s_per_iter"] for x in samples)
-    c = samples[0]
-    val = F / s_iter / 1e12
+    run = OracleSteps(cfg, scale)
+    run.step()                      # the first, cheap iteration (R = V) is not a full one
+    for _ in range(max(0, args.warmup - 1)):
+        run.step()
+    secs = [run.step() for _ in range(max(1, args.steps))]
+    total = sum(secs)
+    s_iter = total / len(secs)
+    val = run.flops / s_iter / 1e12
+    kind = "complex" if cfg in COMPLEX_CONFIGS else "real"
+    sample = run.describe(s_iter)
     return {"impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": len(secs), "warmup": max(1, args.warmup),
             "ms_per_step": 1e3 * s_iter, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "CCSD FP64 %s: No=%d Nv=%d NG=%d %s" % (
-                cfg, o, v, G, "complex" if cfg in COMPLEX_CONFIGS else "real"),
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator of the workload's distributions, vertex x%g)" % scale,
+            "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5" % (cfg, o, v, G, kind),
                        "implementation": "CPU restatement of the reference (oracle, numpy/BLAS); "
-                                         "the reference build needs MPI + CTF, not installed"},
-            "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": c["cores"],
-                             "kind": "port", "sample": c["sample"]},
+                                         "the reference build needs MPI + CTF, not installed",
+                       "sample_shape": list(run.shape), "sample_flops_per_iter": run.flops,
+                       "sample_s_per_iter_all": secs,
+                       "extrapolated_s_per_iter_at_workload": F / (val * 1e12),
+                       "extrapolation": "reference flops of the workload / the sample's measured "
+                                        "rate (CPU rates grow with size, so this is an estimate)"},
+            "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": cores_available(),
+                             "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -714,6 +824,16 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIG_SHAPES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "split3"])
+    ap.add_argument("--time-budget", type=float, default=1500.0,
+                    help="CCSD line: seconds after which optional legs (the FP64 comparison) "
+                         "are skipped")
+    ap.add_argument("--e2e-iterations", type=int, default=2,
+                    help="CCSD line: full iterations of the e2e leg (at most --steps)")
+    ap.add_argument("--fp64-steps", type=int, default=2,
+                    help="CCSD line: timed iterations of the FP64 comparison")
+    ap.add_argument("--fp64-warmup", type=int, default=2,
+                    help="CCSD line: warm-up iterations of the FP64 comparison (the first is "
+                         "the cheap R = V iteration)")
     ap.add_argument("--adjoint", action="store_true",
                     help="time and check the adjoint form (relaxed gradient) instead")
     ap.add_argument("--fd-directions", type=int, default=2)
@@ -736,9 +856,10 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="--triples: device time of each phase of the block loop")
     ap.add_argument("--vertex-scale", type=float, default=None,
-                    help="scale of the synthetic vertex (default 1; 0.3 for --converge and "
-                         "--adjoint: CCSD on the unscaled synthetic vertex diverges at these "
-                         "sizes, strongly correlated)")
+                    help="scale of the synthetic vertex (default 0.3 for the CCSD line, the "
+                         "reference arm, --converge and --adjoint: CCSD on the unscaled "
+                         "synthetic vertex diverges at these sizes, strongly correlated; 1 for "
+                         "--triples and --fsc)")
     args = ap.parse_args()
     if args.shape:
         o_, v_, g_ = (int(x) for x in args.shape.split(","))
@@ -765,13 +886,10 @@ def main():
     line = run_ours(args, world, rank, local)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            c = cpu_sample(args.config)
-            from cc4s_b200.flops import reference_flops
-            o, v, G = CONFIG_SHAPES[args.config]
-            cfg = args.config
-            line["cpu_baseline"] = {"value": reference_flops(o, v, G, complex=cfg in COMPLEX_CONFIGS) / c["s_per_iter"] / 1e12,
-                                    "unit": "TFLOP/s", "cores": c["cores"], "kind": "port",
-                                    "sample": c["sample"]}
+            scale = line["config"]["vertex_scale"]
+            c = cpu_sample(args.config, scale)
+            line["cpu_baseline"] = {"value": c["rate_tflops"], "unit": "TFLOP/s",
+                                    "cores": c["cores"], "kind": "port", "sample": c["sample"]}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

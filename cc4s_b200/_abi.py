@@ -110,8 +110,9 @@ _LIBS = {}
 
 
 def load(path=None):
-    """Loads the C-ABI library.  Raises if it is missing: there is no fallback."""
-    path = os.path.abspath(path or os.environ.get("CC4S_B200_LIB", DEFAULT_LIB))
+    """Loads the C-ABI library (the in-tree build unless `path` names another
+    build of the same ABI).  Raises if it is missing: there is no fallback."""
+    path = os.path.abspath(path or DEFAULT_LIB)
     if path in _LIBS:
         return _LIBS[path]
     if not os.path.exists(path):

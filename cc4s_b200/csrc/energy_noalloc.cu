@@ -31,7 +31,11 @@ constexpr int kVals = 4;                    // Re/Im of direct and exchange
 // device that loads the library until the process exits.
 __device__ __align__(256) double g_energy_scratch[kMaxPairs * kVals];
 
-// Per-device address of g_energy_scratch, set up once per device.
+// Per-device address of g_energy_scratch.  It is looked up again on every call
+// made outside stream capture (the lookup allocates nothing), so a device reset
+// or another context on the same device never leaves a stale address here;
+// calls made while the stream is being captured use the address of the last
+// call outside capture on that device.
 double* g_scratch_addr[64] = {nullptr};
 std::mutex g_scratch_mutex;
 
@@ -126,10 +130,21 @@ int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t 
     *err = "no current CUDA device";
     return ERR_CUDA;
   }
+  // An error left pending by the caller's earlier work is reported as such and
+  // left in place for the caller; nothing is launched then.
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    *err = "a CUDA error from earlier work is pending on this thread; nothing was launched";
+    return ERR_CUDA;
+  }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess) {
+    *err = "cudaStreamIsCapturing failed";
+    return ERR_CUDA;
+  }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    if (capture == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_energy_scratch);
       if (e != cudaSuccess || !p) {
@@ -137,12 +152,16 @@ int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t 
         return ERR_CUDA;
       }
       g_scratch_addr[dev] = static_cast<double*>(p);
+    } else if (!g_scratch_addr[dev]) {
+      *err = "the first call on a device must come before any stream capture";
+      return ERR_STATE;
     }
     scratch = g_scratch_addr[dev];
   }
   energy_pairs_kernel<<<static_cast<unsigned>(No * No), 256, 0, stream>>>(
       T1, T2, V, No, Nv, is_complex ? 1 : 0, scratch);
   energy_finish_kernel<<<1, 256, 0, stream>>>(scratch, No * No, out);
+  // no error was pending before the launches, so this one is theirs
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     *err = cudaGetErrorString(e);

@@ -275,11 +275,15 @@ int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out);
  * with correlation = direct + exchange as in CoupledCluster::getEnergy.
  * Temporary data lives in a fixed 2 MiB device array (nothing in it, nor in
  * energy, has to start at zero), so No <= 256
- * (larger systems are rejected with CC4S_ERR_BAD_SHAPE).  The first call on a
- * device looks up that array's device address; make that first call before
- * any stream capture.  Every call shares the array: calls whose kernels
- * overlap on the GPU (different streams, no ordering) race.  stream is a
- * cudaStream_t (NULL: the legacy default stream).  Errors: cc4s_cc_last_error(NULL). */
+ * (larger systems are rejected with CC4S_ERR_BAD_SHAPE).  Each call made outside
+ * stream capture looks up that array's device address (allocating nothing);
+ * calls during capture reuse the last address found on the device, so make the
+ * first call on a device before any stream capture (else CC4S_ERR_STATE).  A
+ * CUDA error already pending from the caller's earlier work is reported as
+ * CC4S_ERR_CUDA without launching and is left pending for the caller.  Every
+ * call shares the array: calls whose kernels overlap on the GPU (different
+ * streams, no ordering) race.  stream is a cudaStream_t (NULL: the legacy
+ * default stream).  Errors: cc4s_cc_last_error(NULL). */
 int cc4s_cc_energy_noalloc(const double* T1, const double* T2, const double* Vpphh, int64_t No,
                            int64_t Nv, int is_complex, double* energy, void* stream);
 

@@ -63,13 +63,10 @@ class Result(dict):
     pass
 
 
-def run(sys: System, initial_amplitudes=None, **opts):
-    """CoupledCluster::run<F,TE>, CoupledCluster.cxx:56-191.
-
-    Returns a dict with 'energy' (correlation, direct, exchange,
-    secondOrder), 'convergenceReached', 'amplitudes' (T1, T2), 'iterations'
-    and the per-iteration history (energy, dE, residuum norm).
-    """
+def iterations(sys: System, initial_amplitudes=None, **opts):
+    """The loop body of CoupledCluster::run<F,TE> (CoupledCluster.cxx:129-175) as a
+    generator: each next() performs one iteration (residuum, Jacobi update, mixer,
+    energy) and yields (T, history entry, second_order_flag, converged_flag)."""
     o = dict(DEFAULTS)
     o.update(opts)
     method = o["method"]
@@ -88,17 +85,12 @@ def run(sys: System, initial_amplitudes=None, **opts):
     else:
         raise ValueError("Unknown method: '%s'" % method)
     mixer = make_mixer(o["mixer"])
-    maxIt = int(o["maxIterations"])
     e_conv = float(o["energyConvergence"])
     a_conv = float(o["amplitudesConvergence"])
     shift = float(o["levelShift"])
     T = initial_amplitudes
-    energy = {}
-    e = 0.0
     previousE = 0.0
-    history = []
-    i = 0
-    while i < maxIt:
+    while True:
         R = res_fn(T)
         R = residuum_to_amplitudes(R, T, sys, shift)
         if T is not None:
@@ -111,13 +103,39 @@ def run(sys: System, initial_amplitudes=None, **opts):
         T = mixer.get()
         norm = mixer.getResiduumNorm()
         e, D, X = get_energy(T, inp.V["pphh"])
-        history.append(dict(energy=float(np.real(e)), dE=float(np.real(e - previousE)), dR=norm))
-        if second:
-            energy["secondOrder"] = float(np.real(e))
-        if abs(e - previousE) < e_conv and norm < a_conv:
-            break
+        h = dict(energy=float(np.real(e)), dE=float(np.real(e - previousE)), dR=norm)
+        converged = abs(e - previousE) < e_conv and norm < a_conv
         previousE = e
-        i += 1
+        yield T, h, second, converged, inp
+
+
+def run(sys: System, initial_amplitudes=None, **opts):
+    """CoupledCluster::run<F,TE>, CoupledCluster.cxx:56-191.
+
+    Returns a dict with 'energy' (correlation, direct, exchange,
+    secondOrder), 'convergenceReached', 'amplitudes' (T1, T2), 'iterations'
+    and the per-iteration history (energy, dE, residuum norm).
+    """
+    o = dict(DEFAULTS)
+    o.update(opts)
+    maxIt = int(o["maxIterations"])
+    T = initial_amplitudes
+    energy = {}
+    history = []
+    i = 0
+    inp = None
+    if maxIt > 0:
+        for T, h, second, converged, inp in iterations(sys, initial_amplitudes, **opts):
+            history.append(h)
+            if second:
+                energy["secondOrder"] = h["energy"]
+            if converged:
+                break
+            i += 1
+            if i >= maxIt:
+                break
+    if inp is None:
+        inp = ccsd_mod.CcsdInputs(sys)
     e, D, X = get_energy(T, inp.V["pphh"])
     energy.update(correlation=float(np.real(e)), direct=float(np.real(D)),
                   exchange=float(np.real(X)), unit=1.0)

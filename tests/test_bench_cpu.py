@@ -13,6 +13,8 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
 SCRIPT = r"""
 import json, os, sys
 sys.path.insert(0, os.environ["REPO_ROOT"])
+from cc4s_b200 import _abi
+_abi.DEFAULT_LIB = os.environ["EMU_LIB"]   # the CPU emulation build of the same ABI
 import torch
 torch.cuda.set_device = lambda *a, **k: None
 torch.cuda.synchronize = lambda *a, **k: None
@@ -40,7 +42,7 @@ COMMON = {"metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
 
 
 def _line(lib, args):
-    env = dict(os.environ, CC4S_B200_LIB=lib, REPO_ROOT=ROOT, BENCH_ARGS=json.dumps(args))
+    env = dict(os.environ, EMU_LIB=lib, REPO_ROOT=ROOT, BENCH_ARGS=json.dumps(args))
     out = subprocess.run([sys.executable, "-c", SCRIPT], env=env, capture_output=True,
                          text=True, timeout=300)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
@@ -89,3 +91,17 @@ def test_ccsd_line():
     assert {"value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"} <= set(line["e2e"])
     assert "split_speedup_vs_fp64" in line["config"] and line["n_gpus"] == 1
     assert line["warmup"] == 3 and line["steps"] == 1
+
+
+def test_driver_command_fits_its_limit():
+    """`bench.py --gpus 1 --steps 20 --warmup 5` at c2 (the measured seconds per
+    iteration of both forms) projects well inside the 1800 s limit of a bench
+    step, and the FP64 comparison is not skipped by the default 1500 s budget."""
+    import bench
+    legs = bench.projected_seconds(5, 20)
+    total = sum(legs.values())
+    assert total < 1200, legs
+    before_fp64 = total - legs["fp64"] - legs["dgemm_peak"] - legs["cpu_baseline"]
+    projected_fp64 = ((2 - 1 + 2) * bench.FP64_OVER_SPLIT_BOUND * bench.MEASURED_C2["split3"]
+                      + 60.0)
+    assert before_fp64 + projected_fp64 < 1500

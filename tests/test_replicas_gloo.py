@@ -13,6 +13,8 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
 RANK_SCRIPT = r"""
 import json, os, sys
 sys.path.insert(0, os.environ["REPO_ROOT"])
+from cc4s_b200 import _abi
+_abi.DEFAULT_LIB = os.environ["EMU_LIB"]   # the CPU emulation build of the same ABI
 import torch.distributed as dist
 dist.init_process_group("gloo", init_method="env://")
 rank, world = dist.get_rank(), dist.get_world_size()
@@ -46,7 +48,7 @@ def test_two_gloo_replicas(tmp_path):
     procs = []
     for rank in range(2):
         env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2",
-                   RANK=str(rank), LOCAL_RANK="0", CC4S_B200_LIB=lib, REPO_ROOT=ROOT,
+                   RANK=str(rank), LOCAL_RANK="0", EMU_LIB=lib, REPO_ROOT=ROOT,
                    OUT_PREFIX=str(tmp_path / "rank"))
         procs.append(subprocess.Popen([sys.executable, "-c", RANK_SCRIPT], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
@@ -69,6 +71,8 @@ def test_two_gloo_replicas(tmp_path):
 RUN_OURS_SCRIPT = r"""
 import json, os, sys, argparse
 sys.path.insert(0, os.environ["REPO_ROOT"])
+from cc4s_b200 import _abi
+_abi.DEFAULT_LIB = os.environ["EMU_LIB"]   # the CPU emulation build of the same ABI
 import torch, torch.distributed as dist
 dist.init_process_group("gloo", init_method="env://")
 torch.cuda.set_device = lambda *a, **k: None     # host-only stand-ins for the device calls
@@ -86,7 +90,8 @@ bench.dgemm_peak = lambda local: 35.0
 _all_max = bench.all_max
 bench.all_max = lambda x, world: max(_all_max(x, world), 1e-3)  # emulated events read 0 s
 bench.CONFIG_SHAPES["custom"] = (3, 9, 14)
-args = argparse.Namespace(config="custom", steps=1, warmup=1, precision="both", vertex_scale=None)
+args = argparse.Namespace(config="custom", steps=1, warmup=1, precision="both", vertex_scale=None,
+                          time_budget=1500.0, e2e_iterations=2, fp64_steps=2, fp64_warmup=2)
 line = bench.run_ours(args, dist.get_world_size(), dist.get_rank(), 0)
 json.dump(line, open(os.environ["OUT_PREFIX"] + str(dist.get_rank()) + ".json", "w"))
 dist.destroy_process_group()
@@ -103,7 +108,7 @@ def test_two_gloo_ranks_run_the_bench_replica_line(tmp_path):
     procs = []
     for rank in range(2):
         env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2",
-                   RANK=str(rank), LOCAL_RANK="0", CC4S_B200_LIB=lib, REPO_ROOT=ROOT,
+                   RANK=str(rank), LOCAL_RANK="0", EMU_LIB=lib, REPO_ROOT=ROOT,
                    OUT_PREFIX=str(tmp_path / "line"))
         procs.append(subprocess.Popen([sys.executable, "-c", RUN_OURS_SCRIPT], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT))

@@ -58,13 +58,21 @@ def test_energy_noalloc_matches_run_entry(cplx):
     t1, t2, vv = _to_device(T1), _to_device(T2), _to_device(V)
     out = torch.zeros(4, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    for _ in range(2):  # two calls in a row share the static scratch array
+    free_after_first = None
+    for k in range(2):  # two calls in a row share the static scratch array
         out.zero_()
+        torch.cuda.synchronize()
         st = lib.cc4s_cc_energy_noalloc(t1.data_ptr(), t2.data_ptr(), vv.data_ptr(),
                                         s.No, s.Nv, int(cplx), out.data_ptr(),
                                         ctypes.c_void_p(stream))
         assert st == 0, lib.cc4s_cc_last_error(None)
         torch.cuda.synchronize()
+        free = torch.cuda.mem_get_info()[0]
+        if k == 0:
+            free_after_first = free
+        else:
+            # the second call took no device memory (the first may load the module)
+            assert free == free_after_first
         d, x, di, xi = out.cpu().numpy()
         assert abs(d - ref["direct"]) < TOL_E
         assert abs(x - ref["exchange"]) < TOL_E
