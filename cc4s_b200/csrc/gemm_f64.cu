@@ -18,6 +18,7 @@ namespace cc4s_b200 {
 namespace {
 
 constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256;
+constexpr int64_t RASTER_M = 8;  // tile rows per raster group
 
 static std::atomic<uint64_t> g_launches{0};
 
@@ -144,8 +145,21 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_f64_kernel(KParams p) {
   const int g = lane >> 2, t = lane & 3;
   const int wm = (warp >> 2) * 64, wn = (warp & 3) * 32;
 
-  const int64_t n0 = static_cast<int64_t>(blockIdx.x) * BN;
-  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * BM;
+  // Grouped tile order: the blocks launched together cover RASTER_M tile rows
+  // and sweep the tile columns, so each B column tile is read from DRAM once per
+  // group of RASTER_M tile rows (and served from L2 for the others) instead of
+  // once per tile row.
+  int64_t m0, n0;
+  {
+    const int64_t nN = gridDim.x, nM = gridDim.y;
+    const int64_t lin = static_cast<int64_t>(blockIdx.y) * nN + blockIdx.x;
+    const int64_t per_group = RASTER_M * nN, group = lin / per_group;
+    const int64_t first = group * RASTER_M;
+    const int64_t rows = nM - first < RASTER_M ? nM - first : RASTER_M;
+    const int64_t in = lin - group * per_group;
+    m0 = (first + in % rows) * BM;
+    n0 = (in / rows) * BN;
+  }
   const int64_t z = blockIdx.z;
   const int64_t b = z % p.batch;
   const int split = static_cast<int>(z / p.batch);

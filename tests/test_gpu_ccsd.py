@@ -108,6 +108,59 @@ def test_c1_size_independent_properties(Solver):
     assert all(np.isfinite(h["energy"]) for h in r["history"])
 
 
+def _summary_check(A, g, arrays, name, seed, tol):
+    """A against the fixture's norm, seeded weighted checksum and element sample
+    (tests/golden/make_large_golden.py): every difference relative to the
+    fixture's largest element (sample) or norm (norm, checksum)."""
+    flat = np.asarray(A).reshape(-1, order="F")
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(flat.size, size=arrays[name + "_idx"].size, replace=False))
+    assert np.array_equal(idx, arrays[name + "_idx"])
+    w = rng.standard_normal(flat.size)
+    assert np.abs(flat[idx] - arrays[name + "_val"]).max() < tol * g[name + "_max"]
+    assert abs(np.sqrt((flat * flat).sum()) - g[name + "_norm"]) < tol * g[name + "_norm"]
+    assert abs(w @ flat - g[name + "_checksum"]) < tol * g[name + "_norm"]
+
+
+def test_c1_parity_trajectory(Solver):
+    """The FP64 parity configuration (No=32, Nv=256, NG=1024, seed 0, unscaled
+    generator): four iterations from T = 0 with DIIS depth 5 against the oracle's
+    committed fixture -- every iteration's energy within 1e-9 Eh, the final
+    direct/exchange energies likewise, and the final amplitudes within 1e-9
+    relative (element sample, norm and a seeded weighted checksum of all elements)."""
+    g = json.load(open(os.path.join(GOLDEN, "c1_seed0_4it.json")))
+    arrays = np.load(os.path.join(GOLDEN, "c1_seed0_4it.npz"))
+    s = inputs.config_system("c1", seed=g["seed"])
+    sol = Solver(g["options"])
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    r = sol.run()
+    assert r["iterations"] == g["iterations"]
+    for h, e, dr in zip(r["history"], g["history_energy"], g["history_dR"]):
+        assert abs(h["energy"] - e) < TOL_E
+        assert abs(h["dR"] - dr) < TOL_AMP * dr
+    for k in ("correlation", "direct", "exchange", "secondOrder"):
+        assert abs(r[k] - g["energy"][k]) < TOL_E
+    T1, T2 = sol.amplitudes()
+    sol.close()
+    _summary_check(T1, g, arrays, "T1", g["sample_seeds"]["T1"], TOL_AMP)
+    _summary_check(T2, g, arrays, "T2", g["sample_seeds"]["T2"], TOL_AMP)
+
+
+def test_c4_residual_parity(Solver):
+    """One residual at the c4 shape (No=32, Nv=320, NG=1600, seed 0) at seeded
+    random amplitudes against the oracle's committed fixture, to 1e-12 relative."""
+    g = json.load(open(os.path.join(GOLDEN, "c4_seed0_residual.json")))
+    arrays = np.load(os.path.join(GOLDEN, "c4_seed0_residual.npz"))
+    s = inputs.config_system("c4", seed=g["seed"])
+    T = _rand_T(np.random.default_rng(4), s.Nv, s.No)
+    sol = Solver({})
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+    R1, R2 = sol.residual(T)
+    sol.close()
+    _summary_check(R1, g, arrays, "R1", g["sample_seeds"]["R1"], TOL_RES)
+    _summary_check(R2, g, arrays, "R2", g["sample_seeds"]["R2"], TOL_RES)
+
+
 def test_ueg_reference_energies(Solver):
     """cc4s's own expected CCSD energies of its UEG regression test
     (test/tests/ueg/rs1.0-7occ-26virt), reproduced on the GPU."""
