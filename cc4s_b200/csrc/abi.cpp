@@ -307,6 +307,9 @@ CcsdReal* Handle::adjoint_schedule() {
     ro.adjoint = true;
     adj.reset(new CcsdReal(sys, ro, stream));
   }
+  // the handle's precision: the split form runs the recorded residual and the
+  // large contractions of every reverse sweep on the tensor cores
+  adj->set_precision(opt.precision != CC4S_PRECISION_FP64 ? 3 : 0);
   return static_cast<CcsdReal*>(adj.get());
 }
 

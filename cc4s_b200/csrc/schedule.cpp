@@ -56,11 +56,11 @@ void Schedule::gemm_(const Contraction& c) {
   gemm(c, s_, scratch_);
 }
 
-void Schedule::tc_(const Contraction& c) {
-  if (precision_ == 0 || taping_ || c.batch != 1 || c.K < 64 || c.M < 64 || c.N < 64) {
-    gemm_(c);
-    return;
-  }
+bool Schedule::split_ok(const Contraction& c) const {
+  return precision_ != 0 && c.batch == 1 && c.K >= 64 && c.M >= 64 && c.N >= 64;
+}
+
+void Schedule::split_exec(const Contraction& c) {
   const size_t need = gemm_split_scratch_bytes(c);
   if (need > split_.bytes) {
     ops::sync(s_);
@@ -73,6 +73,27 @@ void Schedule::tc_(const Contraction& c) {
     split_.error = reinterpret_cast<int*>(split_mem_);
     ops::zero(split_mem_, 2, s_);
   }
+  gemm_split(c, s_, split_);
+}
+
+// A contraction of the reverse sweep (or a recomputed forward one): split
+// precision under the same rule as tc_, else FP64; neither recorded nor counted.
+void Schedule::exec_(const Contraction& c) {
+  if (split_ok(c)) split_exec(c);
+  else gemm(c, s_, scratch_);
+}
+
+void Schedule::tc_(const Contraction& c) {
+  if (!split_ok(c)) {
+    gemm_(c);
+    return;
+  }
+  if (taping_) {
+    TapeOp op;
+    op.kind = TapeOp::GEMM;
+    op.c = c;
+    tape_.push_back(op);
+  }
   const double f = 2.0 * double(c.M) * double(c.N) * double(c.K);
   if (count_flops_) flops_ += f;
   if (profile_ && count_flops_) {
@@ -82,11 +103,11 @@ void Schedule::tc_(const Contraction& c) {
     ev_split_.push_back(1);
     ev_shape_.push_back({c.M, c.N, c.K, c.batch});
     ops::event_record(ev_[2 * k], s_);
-    gemm_split(c, s_, split_);
+    split_exec(c);
     ops::event_record(ev_[2 * k + 1], s_);
     return;
   }
-  gemm_split(c, s_, split_);
+  split_exec(c);
 }
 
 void Schedule::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA,
@@ -372,14 +393,14 @@ void Schedule::reverse_gemm(const Contraction& c) {
     throw Error(ERR_UNSUPPORTED, "reverse mode: contraction with beta other than 0 or 1");
   auto run = [&](Contraction d) {
     const bool shared = d.batch > 1 && d.C.s_bo == 0 && d.C.s_bi == 0;
-    if (!shared) { gemm(d, s_, scratch_); return; }
+    if (!shared) { exec_(d); return; }
     if (d.Ki == 0 && d.Bi == 0 && d.A.s_bo == 0 && d.B.s_bo == 0) {
       // sum over the batch as part of the contraction: k' = (b, k)
       Contraction e = d;
       e.K = d.K * d.batch; e.Ki = d.K; e.batch = 1;
       e.A.s_co = d.A.s_bi; e.B.s_ro = d.B.s_bi;
       e.A.s_bi = e.B.s_bi = e.C.s_bi = 0;
-      gemm(e, s_, scratch_);
+      exec_(e);
       return;
     }
     const int64_t Bi = d.Bi > 0 ? d.Bi : d.batch;
@@ -423,7 +444,7 @@ void Schedule::reverse(const std::vector<TapeOp>& tape) {
     switch (op.kind) {
       case TapeOp::GEMM: {
         if (op.recompute) {
-          gemm(op.pre, s_, scratch_);
+          exec_(op.pre);
           if (double* zb = bar_of(op.zero_p)) ops::zero(zb, op.zero_n, s_);
         }
         reverse_gemm(op.c);

@@ -41,7 +41,9 @@ class Schedule {
 
   void set_profile(bool on) { profile_ = on; }
   // 0: FP64 throughout; 3: the large ladder / ring / vertex contractions run as
-  // three-slice split-precision products on the tcgen05 tensor cores.
+  // three-slice split-precision products on the tcgen05 tensor cores (in adjoint
+  // mode also the recorded forward pass and the large contractions of the
+  // reverse sweep).
   void set_precision(int slices) { precision_ = slices; }
   // Non-zero if a bounded wait inside a tensor-core kernel expired (synchronises).
   int device_error();
@@ -66,8 +68,9 @@ class Schedule {
 
   // ---- reverse mode ---------------------------------------------------------
   // Vector-Jacobian products of the residual at fixed amplitudes, for schedules
-  // built in adjoint mode.  prepare_vjp(T) evaluates the residual once in FP64
-  // with every device operation recorded (buffers that the fast path reuses are
+  // built in adjoint mode.  prepare_vjp(T) evaluates the residual once (in FP64,
+  // or with the large contractions in split precision when set_precision(3) was
+  // given) with every device operation recorded (buffers that the fast path reuses are
   // separate allocations then, so every recorded value survives);
   // vjp(Rbar, Tbar, gbar) replays the record backwards:
   //   Tbar = Rbar^T dR/dT   (amplitude-vector layout, T2 part symmetrised),
@@ -138,7 +141,11 @@ class Schedule {
   double* take(size_t elems);
   void gemm_(const Contraction& c);
   // A large contraction: split precision when enabled (batch 1), else FP64.
+  // Recorded on the tape when taping, like gemm_.
   void tc_(const Contraction& c);
+  bool split_ok(const Contraction& c) const;
+  void split_exec(const Contraction& c);
+  void exec_(const Contraction& c);
   // C = alpha * op(A) op(B) + beta * C on planar complex operands: the
   // imaginary plane of each operand sits at the given element offset (0: the
   // operand is real); conjA / conjB conjugate an operand.  Four real

@@ -1,5 +1,6 @@
 """cc4s tensor files (cc4s_b200.tensor_io) and the CoupledCluster input chain
-(cc4s_b200.pipeline) on the CPU emulation of the device operations."""
+(cc4s_b200.pipeline): every chain test runs on the CPU emulation of the device
+operations and, marked gpu, on the CUDA library itself (the c0 system there)."""
 import os
 import sys
 import warnings
@@ -13,8 +14,12 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "emu"))
 warnings.simplefilter("ignore")
 
 
-@pytest.fixture(scope="module")
-def emu_lib():
+@pytest.fixture(scope="module", params=["emulated", pytest.param("device", marks=pytest.mark.gpu)])
+def emu_lib(request):
+    """The library the chain calls: the CPU emulation build, or (gpu) None, i.e.
+    the in-tree CUDA library."""
+    if request.param == "device":
+        return None
     import build_emu
     return build_emu.build()
 
@@ -76,14 +81,19 @@ STEPS = [
 ]
 
 
-@pytest.mark.parametrize("half_grid,binary", [(True, True), (False, False)])
+@pytest.mark.parametrize("half_grid,binary", [(True, True), (False, False), (True, False),
+                                             (False, True)])
 def test_input_chain_runs_coupled_cluster(tmp_path, emu_lib, half_grid, binary):
     """Read -> DefineHolesAndParticles -> SliceOperator -> VertexCoulombIntegrals ->
     CoupledCluster -> Write, from files in the reference's tensor format; the energy
     equals the oracle's on the same inputs (real half-grid path and complex path)."""
     import yaml
     from cc4s_b200 import pipeline
-    s = inputs.synthetic_system(4, 12, 20, complex=not half_grid, seed=6)
+    if emu_lib is None:   # the device library: the c0 system (No=8, Nv=40, NG=200)
+        c = inputs.CONFIGS["c0"]
+        s = inputs.synthetic_system(c["No"], c["Nv"], c["NG"], complex=not half_grid, seed=0)
+    else:
+        s = inputs.synthetic_system(4, 12, 20, complex=not half_grid, seed=6)
     _write_system(tmp_path, s, half_grid, binary)
     with open(tmp_path / "cc4s.in", "w") as f:
         yaml.safe_dump(STEPS, f, sort_keys=False)
