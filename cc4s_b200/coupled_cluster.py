@@ -211,7 +211,7 @@ class Solver:
         return dict(correlation=r.correlation, seconds=r.seconds,
                     setup_seconds=r.setup_seconds, flops=r.flops,
                     executed_flops=r.executed_flops, block_size=r.block_size,
-                    block_triples=r.block_triples,
+                    block_triples=r.block_triples, mp2_energy=r.mp2_energy,
                     phase_seconds=dict(zip(("singles", "particle", "hole", "energy"),
                                            list(r.phase_seconds))))
 
@@ -311,8 +311,12 @@ class PerturbativeTriples:
     (the integral slices are formed on the device, so coulombIntegrals is not
     needed), halfGrid; plus precision ('fp64' or 'split3'), blockSize and
     referenceForm (the complex-path conjugation of PerturbativeTriplesReference;
-    the pipeline sets it for that step name).
-    Returns {'energy': {'correlation', 'unit'}} like the reference.
+    the pipeline sets it for that step name), and optionally mp2PairEnergies
+    (the complete-basis-set estimates of the MP2 pair energies, any shape).
+    Returns {'energy': {'correlation', 'unit'}} like the reference, with
+    'starCorrection' = (sum of mp2PairEnergies) / E_MP2 * correlation when
+    mp2PairEnergies is given (the (T*) correction, PerturbativeTriplesStar.hpp:34-108,
+    E_MP2 the second-order energy of the integrals, computed on the device).
     """
 
     def __init__(self, lib=None):
@@ -331,7 +335,11 @@ class PerturbativeTriples:
                                        reference_form=bool(arguments.get("referenceForm", False)))
         finally:
             s.close()
-        return {"energy": {"correlation": r["correlation"], "unit": 1.0}, "stats": r}
+        energy = {"correlation": r["correlation"], "unit": 1.0}
+        if arguments.get("mp2PairEnergies") is not None:
+            cbs = float(np.real(np.sum(np.asarray(arguments["mp2PairEnergies"]))))
+            energy["starCorrection"] = cbs / r["mp2_energy"] * r["correlation"]
+        return {"energy": energy, "stats": r}
 
 
 class FiniteSizeCorrection:

@@ -481,6 +481,13 @@ void Handle::triples(const cc4s_cc_triples_options& o, cc4s_cc_triples_result* o
   out->block_size = r.block;
   out->block_triples = r.block_triples;
   for (int k = 0; k < 4; ++k) out->phase_seconds[k] = r.phase_seconds[k];
+  // the basis MP2 energy of the (T*) ratio (PerturbativeTriplesStar.hpp:79-99)
+  ops::mp2_energy(solver->Vd(), solver->Vd_im(), sys.eh, sys.ep, shape.o, shape.v, scal, ws,
+                  stream);
+  double mp2[2];
+  ops::d2h(mp2, scal, 2, stream);
+  ops::sync(stream);
+  out->mp2_energy = mp2[0] + mp2[1];
 }
 
 // Finite-size correction at the current amplitudes: the plane-wave structure

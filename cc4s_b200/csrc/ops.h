@@ -89,6 +89,14 @@ void jacobi_packed(double* Tnew_p, double* dT_p, const double* R, const double* 
 void energy(const double* T, const double* Vd_re, const double* Vd_im, const double* Ve_re,
             const double* Ve_im, const AmpShape& sh, double* out_dev, double* ws, Stream s);
 
+// Second-order (MP2) energy of the integrals V_abij (pair layout, planar complex
+// when Vd_im is given), PerturbativeTriplesStar.hpp:79-99:
+//   out_dev[0] = 2 sum Re(conj(V_abij) V_abij) / D_abij,
+//   out_dev[1] =  -sum Re(conj(V_abij) V_abji) / D_abij,
+// D_abij = eps_i + eps_j - eps_a - eps_b; deterministic order.
+void mp2_energy(const double* Vd_re, const double* Vd_im, const double* eh, const double* ep,
+                int64_t o, int64_t v, double* out_dev, double* ws, Stream s);
+
 // out_dev[k] = sum_e x[e] * ys[k][e] for k < ny (ny <= 8), deterministic order.
 void dots(const double* x, const double* const* ys, int ny, int64_t n, double* out_dev,
           double* ws, Stream s);

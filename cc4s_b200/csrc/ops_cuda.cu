@@ -290,6 +290,36 @@ __global__ void energy_kernel(EnergyArgs a) {
     for (int k = 0; k < 4; ++k) a.ws[blockIdx.x * 4 + k] = acc[k];
 }
 
+struct Mp2Args {
+  const double* Vr;
+  const double* Vi;
+  const double* eh;
+  const double* ep;
+  int64_t o, v;
+  double* ws;
+};
+
+// Per-block partial sums of Re(conj(V_abij) V_abij) / D and Re(conj(V_abij) V_abji) / D
+// over the pair layout [a][i][b][j]; V_abji = V[(a,j),(b,i)].
+__global__ void mp2_energy_kernel(Mp2Args a) {
+  const int64_t n1 = a.v * a.o, n2 = n1 * n1;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n2;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n1, c = e - r * n1;
+    const int64_t aa = r / a.o, i = r - aa * a.o, b = c / a.o, j = c - b * a.o;
+    const double d = a.eh[i] + a.eh[j] - a.ep[aa] - a.ep[b];
+    const int64_t ex = (aa * a.o + j) * n1 + b * a.o + i;
+    const double vr = a.Vr[e], xr = a.Vr[ex];
+    const double vi = a.Vi ? a.Vi[e] : 0.0, xi = a.Vi ? a.Vi[ex] : 0.0;
+    acc[0] += (vr * vr + vi * vi) / d;
+    acc[1] += (vr * xr + vi * xi) / d;
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 2; ++k) a.ws[blockIdx.x * 2 + k] = acc[k];
+}
+
 // Fixed-order sum of per-block partials: dst[k] = scale[k] * sum_b ws[b*nvals + k].
 __global__ void finish_kernel(double* dst, const double* ws, int nparts, int nvals,
                               double s0, double s1, double s2, double s3) {
@@ -791,6 +821,17 @@ void energy(const double* T, const double* Vd_re, const double* Vd_im, const dou
   CC_LAUNCH_CHECK();
   // direct = 2 * sum X V_ijab, exchange = -sum X V_ijba  (CoupledCluster.cxx:223-232)
   finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 4, 2.0, -1.0, 2.0, -1.0);
+  CC_LAUNCH_CHECK();
+  count();
+  count();
+}
+
+void mp2_energy(const double* Vd_re, const double* Vd_im, const double* eh, const double* ep,
+                int64_t o, int64_t v, double* out_dev, double* ws, Stream s) {
+  Mp2Args a{Vd_re, Vd_im, eh, ep, o, v, ws};
+  mp2_energy_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 2.0, -1.0, 1.0, 1.0);
   CC_LAUNCH_CHECK();
   count();
   count();

@@ -133,6 +133,7 @@ def run_steps(steps, workdir=".", lib=None, symbols=None):
                                  "step (the vertex is needed on the device)" % name)
             md = vertex["hh"].meta_data or {}
             amps = arg(a, "amplitudes")
+            pairs = arg(a, "mp2PairEnergies") if "mp2PairEnergies" in a else None
             res = PerturbativeTriples(lib=lib).run({
                 "slicedEigenEnergies": {"h": eps["h"].values, "p": eps["p"].values},
                 "slicedCoulombVertex": {k: t.values for k, t in vertex.items()},
@@ -140,7 +141,8 @@ def run_steps(steps, workdir=".", lib=None, symbols=None):
                 "amplitudes": {k: getattr(t, "values", t) for k, t in amps.items()},
                 "precision": a.get("precision", "fp64"),
                 "blockSize": a.get("blockSize", 0),
-                "referenceForm": name == "PerturbativeTriplesReference"})
+                "referenceForm": name == "PerturbativeTriplesReference",
+                "mp2PairEnergies": getattr(pairs, "values", pairs)})
             sym[out.get("energy", name + "Energy")] = res["energy"]
         elif name == "FiniteSizeCorrection":
             eps = arg(a, "slicedEigenEnergies")

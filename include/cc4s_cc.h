@@ -215,6 +215,11 @@ typedef struct {
   int64_t block_triples;  /* blocks A <= B <= C evaluated */
   double phase_seconds[4];  /* options.profile of the handle: device time of the singles,
                                particle contractions, hole contractions and energy kernel */
+  double mp2_energy;      /* second-order energy of the handle's integrals in its basis,
+                             sum Re(2 M_abij V_abij - M_abij V_abji), M = conj(V)/D
+                             (PerturbativeTriplesStar.hpp:79-99): the denominator of the
+                             (T*) ratio; starCorrection = (sum of the caller's CBS pair
+                             energies) / mp2_energy * correlation */
 } cc4s_cc_triples_result;
 void cc4s_cc_triples_default_options(cc4s_cc_triples_options* opt);
 /* Perturbative triples energy at the current amplitudes (after cc4s_cc_run or

@@ -136,3 +136,17 @@ def triples_flops(No, Nv):
     """Doubles flops of the tuple loop as the reference counts them
     (PerturbativeTriples.cxx, atripDryRun: No^3 Nv^3 (No + Nv) * 2)."""
     return 2.0 * No ** 3 * Nv ** 3 * (No + Nv)
+
+
+def triples_star(Vpphh, eps_h, eps_p, mp2_pair_energies_cbs, triples_energy):
+    """(T*) correction, computeCssdPtStar (PerturbativeTriplesStar.hpp:34-108):
+    M_abij = conj(V_abij) / (e_i + e_j - e_a - e_b), basis pair energies
+    2 M_abij V_abij - M_abij V_abji summed to E_MP2; returns
+    (sum of the CBS pair energies) / Re E_MP2 * E_(T) and E_MP2."""
+    D = (eps_h[None, None, :, None] + eps_h[None, None, None, :]
+         - eps_p[:, None, None, None] - eps_p[None, :, None, None])
+    M = np.conj(Vpphh) / D
+    pairs = 2.0 * np.einsum("abij,abij->ij", M, Vpphh) - np.einsum("abij,abji->ij", M, Vpphh)
+    e_mp2 = float(np.real(pairs.sum()))
+    cbs = float(np.real(np.sum(mp2_pair_energies_cbs)))
+    return cbs / e_mp2 * triples_energy, e_mp2

@@ -273,6 +273,23 @@ void jacobi(double* Tnew, double* dT, const double* R, const double* Told, const
   }
 }
 
+void mp2_energy(const double* Vr, const double* Vi, const double* eh, const double* ep,
+                int64_t o, int64_t v, double* out, double*, Stream) {
+  ++g_ops;
+  const int64_t n1 = v * o;
+  double acc[2] = {0, 0};
+  for (int64_t r = 0; r < n1; ++r)
+    for (int64_t c = 0; c < n1; ++c) {
+      const int64_t e = r * n1 + c, a = r / o, i = r % o, b = c / o, j = c % o;
+      const double d = eh[i] + eh[j] - ep[a] - ep[b];
+      const int64_t ex = (a * o + j) * n1 + b * o + i;
+      acc[0] += (Vr[e] * Vr[e] + (Vi ? Vi[e] * Vi[e] : 0.0)) / d;
+      acc[1] += (Vr[e] * Vr[ex] + (Vi ? Vi[e] * Vi[ex] : 0.0)) / d;
+    }
+  out[0] = 2.0 * acc[0];
+  out[1] = -acc[1];
+}
+
 void energy(const double* T, const double* Vdr, const double* Vdi, const double* Ver,
             const double* Vei, const AmpShape& sh, double* out, double*, Stream) {
   ++g_ops;

@@ -164,3 +164,28 @@ def test_triples_edge_shapes(emu_lib, shape, block):
     else:
         assert abs(r["correlation"] - ref) < 1e-12 * max(1.0, abs(ref)), (r["correlation"], ref)
     assert r["block_size"] == (min(block, Nv) if block > 0 else r["block_size"])
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_triples_star_correction(emu_lib, cplx):
+    """mp2PairEnergies given: starCorrection = (sum of the CBS pair energies) / E_MP2
+    * E_(T), E_MP2 the basis second-order energy formed on the device
+    (PerturbativeTriplesStar.hpp:34-108), against the oracle's restatement."""
+    from cc4s_b200 import PerturbativeTriples
+    s = inputs.synthetic_system(3, 8, 14, complex=cplx, seed=3)
+    rng = np.random.default_rng(9)
+    T1, T2 = _rand_T(rng, 8, 3)
+    if cplx:
+        T1 = T1 + 1j * _rand_T(rng, 8, 3)[0]
+        T2 = T2 + 1j * _rand_T(rng, 8, 3)[1]
+    pairs = -0.01 * rng.random((3, 3))
+    r = PerturbativeTriples(lib=emu_lib).run({
+        "slicedEigenEnergies": {"h": s.eps_h, "p": s.eps_p}, "coulombVertex": s.gamma,
+        "halfGrid": not cplx, "amplitudes": {"ph": T1, "pphh": T2}, "mp2PairEnergies": pairs})
+    V = inputs.coulomb_integrals(s, ["pphh"])["pphh"]
+    e_t = r["energy"]["correlation"]
+    star, e_mp2 = triples.triples_star(V, s.eps_h, s.eps_p, pairs, e_t)
+    assert abs(r["stats"]["mp2_energy"] - e_mp2) < 1e-12 * abs(e_mp2)
+    assert abs(r["energy"]["starCorrection"] - star) < 1e-12 * abs(star)
+    from oracle import properties
+    assert abs(e_mp2 - properties.mp2(s)[0]) < 1e-12 * abs(e_mp2)

@@ -147,3 +147,25 @@ def test_ueg_triples_after_ccsd_matches_reference_expected_output():
     ref = g["triples"]["energy"]["correlation"]
     assert abs(a - ref) < 1e-9, (a, ref)
     assert abs(b - ref) < 1e-9, (b, ref)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_triples_star_correction_on_device(cplx):
+    """(T*) on the B200: starCorrection = (sum of the CBS pair energies) / E_MP2 *
+    E_(T) with the basis MP2 energy reduced on the device, against the oracle's
+    restatement of PerturbativeTriplesStar.hpp:34-108 (1e-11 relative)."""
+    from cc4s_b200 import PerturbativeTriples
+    s = inputs.synthetic_system(6, 30, 90, complex=cplx, seed=3)
+    rng = np.random.default_rng(9)
+    T1, T2 = _rand_T(rng, 30, 6)
+    if cplx:
+        T1 = T1 + 1j * _rand_T(rng, 30, 6)[0]
+        T2 = T2 + 1j * _rand_T(rng, 30, 6)[1]
+    pairs = -0.01 * rng.random((6, 6))
+    r = PerturbativeTriples().run({
+        "slicedEigenEnergies": {"h": s.eps_h, "p": s.eps_p}, "coulombVertex": s.gamma,
+        "halfGrid": not cplx, "amplitudes": {"ph": T1, "pphh": T2}, "mp2PairEnergies": pairs})
+    V = inputs.coulomb_integrals(s, ["pphh"])["pphh"]
+    star, e_mp2 = triples.triples_star(V, s.eps_h, s.eps_p, pairs, r["energy"]["correlation"])
+    assert abs(r["stats"]["mp2_energy"] - e_mp2) < TOL_FP64 * abs(e_mp2)
+    assert abs(r["energy"]["starCorrection"] - star) < TOL_FP64 * abs(star)
