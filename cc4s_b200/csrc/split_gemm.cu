@@ -31,9 +31,22 @@ namespace cc4s_b200 {
 
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 32, NST = 4, NSLICE = 3;
+// Stage geometry.  Wide stages: k-blocks of 64 (128-byte rows, 128-byte swizzle),
+// two 96 KB stages, half as many TMA row requests per byte as the narrow form
+// (k-blocks of 32, 64-byte rows and swizzle, four 48 KB stages).
+#ifndef CC4S_SPLIT_WIDE_STAGES
+#define CC4S_SPLIT_WIDE_STAGES 0
+#endif
+#if CC4S_SPLIT_WIDE_STAGES
+constexpr int TK = 64, NST = 2;
+constexpr uint32_t ROW_BYTES = 128;               // smem row of one k-block (bytes)
+#else
+constexpr int TK = 32, NST = 4;
+constexpr uint32_t ROW_BYTES = 64;
+#endif
+constexpr int TM = 128, TN = 128, NSLICE = 3;
 constexpr int KCHUNK = 4096;                      // exact FP32 span of the leading group
-constexpr int TILE_BYTES = TM * TK * 2;           // 8 KB per slice tile
+constexpr int TILE_BYTES = TM * TK * 2;           // one slice tile: 8 KB (narrow), 16 KB (wide)
 constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;
 constexpr int SMEM_BYTES = NST * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t WAIT_LIMIT = 1u << 28;         // bounded mbarrier waits
@@ -163,14 +176,15 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1)
       : "memory");
 }
-// Shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 B apart.
+// Shared-memory matrix descriptor: K-major, swizzled rows of ROW_BYTES (64 or 128),
+// 8-row groups 8 * ROW_BYTES apart.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);        // start address
   d |= static_cast<uint64_t>(1) << 16;                       // leading byte offset (16 B)
-  d |= static_cast<uint64_t>(512 >> 4) << 32;                // stride byte offset
+  d |= static_cast<uint64_t>((8 * ROW_BYTES) >> 4) << 32;    // stride byte offset
   d |= static_cast<uint64_t>(1) << 46;                       // descriptor version (sm100)
-  d |= static_cast<uint64_t>(4) << 61;                       // SWIZZLE_64B
+  d |= static_cast<uint64_t>(ROW_BYTES == 128 ? 2 : 4) << 61;  // SWIZZLE_128B / SWIZZLE_64B
   return d;
 }
 // Instruction descriptors: D = F32, A = B = F16, both K-major, M = 128, N = 128 or 256.
@@ -321,7 +335,7 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         const uint32_t st = smem_u32(base + s * STAGE_BYTES);
 #pragma unroll
         for (int kk = 0; kk < TK / 16; ++kk) {
-          // 32 bytes per 16-element K step inside the 64-byte swizzled rows
+          // 32 bytes per 16-element K step inside the swizzled rows
           const uint32_t koff = kk * 32;
           // Groups of equal weight live at TMEM columns 0 (S1S1), 128 (S1S2 + S2S1)
           // and 256 (S1S3 + S2S2 + S3S1).  B slices 1 and 2 are adjacent in shared
@@ -698,7 +712,8 @@ EncodeFn encode_fn() {
   return fn;
 }
 
-// 2-D map over packed slices [3*Rp][Kp] FP16, box 32 (k) x 128 (rows), 64-byte swizzle.
+// 2-D map over packed slices [3*Rp][Kp] FP16, box TK (k) x 128 (rows), rows of
+// ROW_BYTES swizzled like the MMA descriptors expect.
 CUtensorMap make_map(void* base, int64_t rows, int64_t Kp) {
   CUtensorMap m;
   const cuuint64_t dims[2] = {static_cast<cuuint64_t>(Kp), static_cast<cuuint64_t>(rows)};
@@ -706,7 +721,8 @@ CUtensorMap make_map(void* base, int64_t rows, int64_t Kp) {
   const cuuint32_t box[2] = {TK, 128};
   const cuuint32_t es[2] = {1, 1};
   CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, es,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           ROW_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(ERR_CUDA, "cuTensorMapEncodeTiled failed");
   return m;

@@ -105,3 +105,14 @@ def test_driver_command_fits_its_limit():
     projected_fp64 = ((2 - 1 + 2) * bench.FP64_OVER_SPLIT_BOUND * bench.MEASURED_C2["split3"]
                       + 60.0)
     assert before_fp64 + projected_fp64 < 1500
+
+
+def test_adjoint_line():
+    """--adjoint: both backward forms, their finite-difference checks and timings."""
+    import build_emu
+    line = _line(build_emu.build(), ["--adjoint", "--shape", "2,32,40", "--fd-directions", "1"])
+    assert set(line["forms"]) == {"fp64", "split3"}
+    for f in line["forms"].values():
+        assert f["lambda_converged"] and len(f["fd_directions"]) == 1
+        assert f["fd_max_rel_err"] < 1e-5
+    assert "max_abs_diff_vs_fp64_over_max" in line["forms"]["split3"]
