@@ -56,6 +56,10 @@ void Schedule::gemm_(const Contraction& c) {
   gemm(c, s_, scratch_);
 }
 
+namespace {
+constexpr size_t kSplitDataOffset = 128;  // doubles: 1 KiB
+}  // namespace
+
 bool Schedule::split_ok(const Contraction& c) const {
   return precision_ != 0 && c.batch == 1 && c.K >= 64 && c.M >= 64 && c.N >= 64;
 }
@@ -66,9 +70,12 @@ void Schedule::split_exec(const Contraction& c) {
     ops::sync(s_);
     if (split_mem_) ops::release(split_mem_);
     split_mem_ = nullptr;
-    const size_t doubles = (need + 7) / 8 + 2;
+    // The error word sits in the first double; the packed slices start 1 KiB in,
+    // so every TMA row request of the contraction kernel begins on a sector and
+    // line boundary (a 16-byte offset made each 64-byte row touch three sectors).
+    const size_t doubles = (need + 7) / 8 + kSplitDataOffset;
     split_mem_ = ops::alloc(doubles);
-    split_.p = split_mem_ + 2;
+    split_.p = split_mem_ + kSplitDataOffset;
     split_.bytes = need;
     split_.error = reinterpret_cast<int*>(split_mem_);
     ops::zero(split_mem_, 2, s_);
