@@ -510,44 +510,83 @@ def run_adjoint(args, local):
 
 
 def run_converge(args, local):
-    """Accuracy of the split form at convergence: FP64, pure split and split with
-    FP64 refinement, each to energyConvergence 1e-10 (DIIS 5, at most 80
-    iterations); reports |E_split - E_fp64|, iterations and time to solution.
-    The synthetic vertex is scaled (default 0.3): unscaled, CCSD diverges at
-    these sizes."""
+    """Accuracy of the split form at convergence.  Forms, each to
+    energyConvergence --converge-energy (DIIS 5, at most 100 iterations):
+      split3          the split form from T = 0;
+      fp64_from_split FP64 iterations started from the split form's converged
+                      amplitudes (converges to the FP64 fixed point);
+      fp64            the FP64 form from T = 0 (skipped with --converge-skip-fp64).
+    Reports |E_split - E_fp64|, the per-iteration energies and residuum norms,
+    the final amplitudes' difference (max and norm, relative), iterations and
+    time to solution.  The synthetic vertex is scaled (default 0.3): unscaled,
+    CCSD diverges at these sizes."""
+    import numpy as np
     import torch
     from cc4s_b200 import Solver
     from cc4s_b200.synthetic import config
     torch.cuda.set_device(local)
     cfg = args.config
     o, v, G = CONFIG_SHAPES[cfg]
-    eh, ep, g, hg = config(cfg, seed=0)
+    if cfg == "custom":
+        from cc4s_b200.synthetic import synthetic
+        eh, ep, g, hg = synthetic(o, v, G, complex=False, seed=0)
+    else:
+        eh, ep, g, hg = config(cfg, seed=0)
     scale = args.vertex_scale if args.vertex_scale is not None else 0.3
     g *= scale
-    base = dict(maxIterations=80, energyConvergence=1e-10, amplitudesConvergence=1e-8,
-                mixer=dict(type="DiisMixer", maxResidua=5), device=local)
-    forms = {"fp64": {}, "split3": dict(precision="split3"),
-             "split3_refined": dict(precision="split3", precisionRefinement=args.refine)}
-    out = {}
-    for name, extra in forms.items():
-        so = Solver(dict(base, **extra))
+    base = dict(maxIterations=100, energyConvergence=args.converge_energy,
+                amplitudesConvergence=1e-7, mixer=dict(type="DiisMixer", maxResidua=5),
+                device=local)
+
+    def solve(precision, start=None):
+        so = Solver(dict(base, precision=precision))
         so.set_inputs(eh, ep, g, half_grid=hg)
+        if start is not None:
+            so.set_initial_amplitudes(*start)
         r = so.run()
+        T = so.amplitudes()
         so.close()
-        out[name] = {"energy": r["correlation"], "iterations": r["iterations"],
-                     "converged": r["converged"], "seconds": sum(h["seconds"] for h in r["history"]),
-                     "refined_from": r["refined_from"],
-                     "s_per_iter": [h["seconds"] for h in r["history"]]}
-    e64 = out["fp64"]["energy"]
-    for name in ("split3", "split3_refined"):
+        return r, T
+
+    def summary(r):
+        return {"energy": r["correlation"], "iterations": r["iterations"],
+                "converged": r["converged"], "seconds": sum(h["seconds"] for h in r["history"]),
+                "history_energy": [h["energy"] for h in r["history"]],
+                "history_residuum_norm": [h["dR"] for h in r["history"]],
+                "s_per_iter": [h["seconds"] for h in r["history"]]}
+
+    out = {}
+    rs, Ts = solve("split3")
+    out["split3"] = summary(rs)
+    rf, Tf = solve("fp64", start=Ts)
+    out["fp64_from_split"] = summary(rf)
+    T64, r64 = Tf, rf
+    if not args.converge_skip_fp64:
+        r0, T0 = solve("fp64")
+        out["fp64"] = summary(r0)
+        out["fp64"]["abs_dE_vs_fp64_from_split"] = abs(r0["correlation"] - rf["correlation"])
+        T64, r64 = T0, r0
+    e64 = r64["correlation"]
+    for name, T in (("split3", Ts), ("fp64_from_split", Tf)):
+        if name == "fp64_from_split" and T is T64:
+            continue
         out[name]["abs_dE_vs_fp64"] = abs(out[name]["energy"] - e64)
+        for k, (A, B) in enumerate(zip(T, T64)):
+            d = np.abs(A - B).max() / np.abs(B).max()
+            n = float(np.linalg.norm((A - B).ravel()) / np.linalg.norm(B.ravel()))
+            out[name]["T%d_max_rel_diff" % (k + 1)] = float(d)
+            out[name]["T%d_norm_rel_diff" % (k + 1)] = n
     kind = "complex" if cfg in COMPLEX_CONFIGS else "real"
+    ref = "fp64" if "fp64" in out else "fp64_from_split"
     return {"metric": "CCSD converged |dE_c| split-precision vs FP64 (bound 1e-6 Eh)",
-            "value": out["split3_refined"]["abs_dE_vs_fp64"], "unit": "Eh",
+            "value": out["split3"]["abs_dE_vs_fp64"], "unit": "Eh",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, energyConvergence 1e-10"
-                                   % (cfg, o, v, G, kind),
-                       "precision_refinement": args.refine, "vertex_scale": scale},
+            "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d %s, DIIS 5, energyConvergence %g"
+                                   % (cfg, o, v, G, kind, args.converge_energy),
+                       "vertex_scale": scale, "fp64_reference": ref,
+                       "split_time_to_solution_vs_fp64":
+                           out["split3"]["seconds"] / out[ref]["seconds"]
+                           if out[ref]["seconds"] > 0 else None},
             "forms": out}
 
 
@@ -879,8 +918,11 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=8)
     ap.add_argument("--converge", action="store_true",
                     help="converge FP64, split and refined split forms and compare energies")
-    ap.add_argument("--refine", type=float, default=1e-5,
-                    help="residuum norm below which the refined split form switches to FP64")
+    ap.add_argument("--converge-energy", type=float, default=1e-9,
+                    help="--converge: energyConvergence of every form")
+    ap.add_argument("--converge-skip-fp64", action="store_true",
+                    help="--converge: no FP64 solve from T = 0 (the FP64 reference is then the "
+                         "FP64 iteration started from the split form's amplitudes)")
     ap.add_argument("--triples", action="store_true",
                     help="time the perturbative triples (T) step instead (real configurations)")
     ap.add_argument("--fsc", action="store_true",

@@ -18,6 +18,8 @@ void Schedule::release_all() {
   if (split_mem_) ops::release(split_mem_);
   split_mem_ = nullptr;
   split_ = SplitScratch();
+  split_extra_ = nullptr;
+  split_extra_bytes_ = 0;
   for (double* p : owned_) ops::release(p);
   owned_.clear();
   owned_n_.clear();
@@ -64,23 +66,57 @@ bool Schedule::split_ok(const Contraction& c) const {
   return precision_ != 0 && c.batch == 1 && c.K >= 64 && c.M >= 64 && c.N >= 64;
 }
 
+void Schedule::split_reserve(size_t regular, size_t extra) {
+  regular = (regular + 1023) / 1024 * 1024;
+  extra = (extra + 1023) / 1024 * 1024;
+  if (regular <= split_.bytes && extra <= split_extra_bytes_) return;
+  regular = std::max(regular, split_.bytes);
+  extra = std::max(extra, split_extra_bytes_);
+  ops::sync(s_);
+  if (split_mem_) ops::release(split_mem_);
+  split_mem_ = nullptr;
+  split_extra_ = nullptr;
+  split_extra_bytes_ = 0;
+  // The error word sits in the first double; the packed slices start 1 KiB in,
+  // so every TMA row request of the contraction kernel begins on a sector and
+  // line boundary (a 16-byte offset made each 64-byte row touch three sectors).
+  const size_t doubles = (regular + extra) / 8 + kSplitDataOffset;
+  split_mem_ = ops::alloc(doubles);
+  split_.p = split_mem_ + kSplitDataOffset;
+  split_.bytes = regular;
+  split_.error = reinterpret_cast<int*>(split_mem_);
+  if (extra) {
+    split_extra_ = static_cast<unsigned char*>(split_.p) + regular;
+    split_extra_bytes_ = extra;
+  }
+  ops::zero(split_mem_, 2, s_);
+}
+
 void Schedule::split_exec(const Contraction& c) {
   const size_t need = gemm_split_scratch_bytes(c);
   if (need > split_.bytes) {
-    ops::sync(s_);
-    if (split_mem_) ops::release(split_mem_);
-    split_mem_ = nullptr;
-    // The error word sits in the first double; the packed slices start 1 KiB in,
-    // so every TMA row request of the contraction kernel begins on a sector and
-    // line boundary (a 16-byte offset made each 64-byte row touch three sectors).
-    const size_t doubles = (need + 7) / 8 + kSplitDataOffset;
-    split_mem_ = ops::alloc(doubles);
-    split_.p = split_mem_ + kSplitDataOffset;
-    split_.bytes = need;
-    split_.error = reinterpret_cast<int*>(split_mem_);
-    ops::zero(split_mem_, 2, s_);
+    split_extra_bytes_ = 0;   // reallocated without the extra region
+    split_reserve(need, 0);
   }
   gemm_split(c, s_, split_);
+}
+
+void Schedule::tc_packed_b_(const Contraction& c, const SplitPackedB& b) {
+  if (taping_) throw Error(ERR_STATE, "pre-packed split operands are not recorded");
+  const double f = 2.0 * double(c.M) * double(c.N) * double(c.K);
+  if (count_flops_) flops_ += f;
+  if (profile_ && count_flops_) {
+    const size_t k = ev_flops_.size();
+    while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
+    ev_flops_.push_back(f);
+    ev_split_.push_back(1);
+    ev_shape_.push_back({c.M, c.N, c.K, c.batch});
+    ops::event_record(ev_[2 * k], s_);
+    gemm_split_packed_b(c, b, s_, split_);
+    ops::event_record(ev_[2 * k + 1], s_);
+    return;
+  }
+  gemm_split_packed_b(c, b, s_, split_);
 }
 
 // A contraction of the reverse sweep (or a recomputed forward one): split

@@ -145,6 +145,13 @@ class Schedule {
   void tc_(const Contraction& c);
   bool split_ok(const Contraction& c) const;
   void split_exec(const Contraction& c);
+  // Makes the split scratch hold `regular` bytes for per-contraction packing plus a
+  // second region of `extra` bytes (split_extra_) that survives those calls; may
+  // reallocate (synchronises).  A later split_exec that needs more than `regular`
+  // reallocates and drops the extra region.
+  void split_reserve(size_t regular, size_t extra);
+  // One split contraction whose B was sliced by split_pack_b (recorded like tc_).
+  void tc_packed_b_(const Contraction& c, const SplitPackedB& b);
   void exec_(const Contraction& c);
   // C = alpha * op(A) op(B) + beta * C on planar complex operands: the
   // imaginary plane of each operand sits at the given element offset (0: the
@@ -156,6 +163,8 @@ class Schedule {
   int precision_ = 0;
   SplitScratch split_;
   double* split_mem_ = nullptr;
+  void* split_extra_ = nullptr;
+  size_t split_extra_bytes_ = 0;
   // vertex description for the adjoint (set by each schedule)
   int64_t so_ = 0, sv_ = 0, sG_ = 0;
   bool scplx_ = false;

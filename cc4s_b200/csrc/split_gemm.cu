@@ -79,55 +79,117 @@ struct PackArgs {
   int r_contig;           // 1: the row index is the contiguous one in memory
 };
 
-// Tile 32 rows x 32 k through shared memory; mode 0: row maxima, mode 1: slices.
-template <int MODE>
-__global__ void pack_kernel(PackArgs a) {
-  __shared__ double tile[32][33];
-  const int64_t tr = (a.Rp + 31) / 32, tk = (a.Kp + 31) / 32;
-  for (int64_t blk = blockIdx.x; blk < tr * tk; blk += gridDim.x) {
-    const int64_t r0 = (blk / tk) * 32, k0 = (blk % tk) * 32;
-    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
-      // read: lanes along the contiguous index
-      int64_t r, k;
-      if (a.r_contig) { r = r0 + threadIdx.x; k = k0 + yy; }
-      else { r = r0 + yy; k = k0 + threadIdx.x; }
-      double v = 0.0;
-      if (r < a.R && k < a.K) v = a.src[a.ar.off(static_cast<uint32_t>(r)) + a.ak.off(static_cast<uint32_t>(k))];
-      if (a.r_contig) tile[threadIdx.x][yy] = v; else tile[yy][threadIdx.x] = v;
-    }
-    __syncthreads();
-    if (MODE == 0) {
-      // row maxima: threads (x = k lane, y = row) reduce over k with warp shuffles
-      for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
-        double m = fabs(tile[rr][threadIdx.x]);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-        const int64_t r = r0 + rr;
-        if (threadIdx.x == 0 && r < a.R && m > 0.0)
-          atomicMax(&a.rmax[r], static_cast<unsigned long long>(__double_as_longlong(m)));
-      }
+// Packing works on tiles of 64 rows x 64 k staged in shared memory.  The row and
+// k offsets of a tile are computed once per tile (two-level index maps need an
+// integer division each), every thread keeps 16 loads in flight, and the FP16
+// slices leave as 16-byte vector stores along k.
+constexpr int PR = 64, PKT = 64, PTHREADS = 256, PSTRIP = 16;  // strip: k tiles per row max
+
+struct PackTile {
+  double v[PR][PKT + 1];
+  int64_t roff[PR];
+  int64_t koff[PKT];
+};
+
+// Loads the tile (r0, k0) of the operand into t.v (zero outside R x K).
+__device__ __forceinline__ void pack_load_tile(const PackArgs& a, int64_t r0, int64_t k0,
+                                               PackTile& t) {
+  for (int q = threadIdx.x; q < PR + PKT; q += PTHREADS) {
+    if (q < PR) {
+      const int64_t r = r0 + q;
+      t.roff[q] = r < a.R ? a.ar.off(static_cast<uint32_t>(r)) : -1;
     } else {
-      for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
-        const int64_t r = r0 + rr, k = k0 + threadIdx.x;
-        if (r >= a.Rp || k >= a.Kp) continue;
-        double x = tile[rr][threadIdx.x];
-        int e = 0;
-        if (r < a.R) {
-          const double m = __longlong_as_double(static_cast<long long>(a.rmax[r]));
-          if (m > 0.0) frexp(m, &e);
-          if (k == 0) a.rexp[r] = e;
-        }
-        x = ldexp(x, -e) * 64.0;                 // |x| <= 64
+      const int64_t k = k0 + (q - PR);
+      t.koff[q - PR] = k < a.K ? a.ak.off(static_cast<uint32_t>(k)) : -1;
+    }
+  }
+  __syncthreads();
+  const int lo = threadIdx.x & 63, hi = threadIdx.x >> 6;  // lanes along the contiguous index
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int rr = a.r_contig ? lo : hi + 4 * j;
+    const int kk = a.r_contig ? hi + 4 * j : lo;
+    const int64_t ro = t.roff[rr], ko = t.koff[kk];
+    x[j] = (ro >= 0 && ko >= 0) ? a.src[ro + ko] : 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int rr = a.r_contig ? lo : hi + 4 * j;
+    const int kk = a.r_contig ? hi + 4 * j : lo;
+    t.v[rr][kk] = x[j];
+  }
+  __syncthreads();
+}
+
+// Row maxima |x| over all k, as IEEE bits of non-negative doubles: each block
+// walks PSTRIP k tiles of one row strip, one atomicMax per row and strip.
+__global__ void __launch_bounds__(PTHREADS) pack_max_kernel(PackArgs a) {
+  __shared__ PackTile t;
+  const int64_t nr = a.Rp / PR, nks = (a.Kp + PKT * PSTRIP - 1) / (PKT * PSTRIP);
+  const int row = threadIdx.x >> 2, part = threadIdx.x & 3;  // 4 threads per row, 16 k each
+  for (int64_t w = blockIdx.x; w < nr * nks; w += gridDim.x) {
+    const int64_t r0 = (w / nks) * PR, kbeg = (w % nks) * PKT * PSTRIP;
+    double m = 0.0;
+    for (int64_t k0 = kbeg; k0 < kbeg + PKT * PSTRIP && k0 < a.Kp; k0 += PKT) {
+      pack_load_tile(a, r0, k0, t);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) m = fmax(m, fabs(t.v[row][16 * part + j]));
+      __syncthreads();
+    }
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
+    const int64_t r = r0 + row;
+    if (part == 0 && r < a.R && m > 0.0)
+      atomicMax(&a.rmax[r], static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+// Three FP16 integer slices of every element (row-padded to Rp, k-padded to Kp)
+// and the per-row exponent.
+__global__ void __launch_bounds__(PTHREADS) pack_slices_kernel(PackArgs a) {
+  __shared__ PackTile t;
+  __shared__ int rexp_s[PR];
+  const int64_t nr = a.Rp / PR, nk = (a.Kp + PKT - 1) / PKT;
+  const int row = threadIdx.x >> 2, part = threadIdx.x & 3;
+  const int64_t pl = a.Rp * a.Kp;
+  for (int64_t w = blockIdx.x; w < nr * nk; w += gridDim.x) {
+    const int64_t r0 = (w / nk) * PR, k0 = (w % nk) * PKT;
+    if (threadIdx.x < PR) {
+      const int64_t r = r0 + threadIdx.x;
+      int e = 0;
+      if (r < a.R) {
+        const double m = __longlong_as_double(static_cast<long long>(a.rmax[r]));
+        if (m > 0.0) frexp(m, &e);
+        if (k0 == 0) a.rexp[r] = e;
+      }
+      rexp_s[threadIdx.x] = e;
+    }
+    pack_load_tile(a, r0, k0, t);   // its first barrier also publishes rexp_s
+    const int64_t r = r0 + row, kb = k0 + 16 * part;
+    if (kb < a.Kp) {
+      const int e = rexp_s[row];
+      __align__(16) __half h[3][16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        double x = ldexp(t.v[row][16 * part + j], -e) * 64.0;   // |x| <= 64
         const double s1 = rint(x);
-        double t = (x - s1) * 2048.0;            // |t| <= 1024
-        const double s2 = rint(t);
-        t = (t - s2) * 2048.0;
-        const double s3 = rint(t);
-        const int64_t o = r * a.Kp + k, pl = a.Rp * a.Kp;
+        double u = (x - s1) * 2048.0;                            // |u| <= 1024
+        const double s2 = rint(u);
+        u = (u - s2) * 2048.0;
+        const double s3 = rint(u);
         // integers of at most 11 bits: exact in FP32 and FP16
-        a.dst[o] = __float2half_rn(static_cast<float>(s1));
-        a.dst[o + pl] = __float2half_rn(static_cast<float>(s2));
-        a.dst[o + 2 * pl] = __float2half_rn(static_cast<float>(s3));
+        h[0][j] = __float2half_rn(static_cast<float>(s1));
+        h[1][j] = __float2half_rn(static_cast<float>(s2));
+        h[2][j] = __float2half_rn(static_cast<float>(s3));
+      }
+      const int64_t o = r * a.Kp + kb;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        uint4* d = reinterpret_cast<uint4*>(a.dst + q * pl + o);
+        const uint4* src = reinterpret_cast<const uint4*>(h[q]);
+        d[0] = src[0];
+        d[1] = src[1];
       }
     }
     __syncthreads();
@@ -762,12 +824,13 @@ void pack(const View& v, bool rows_are_m, const Contraction& g, int64_t R, int64
   }
   a.R = R; a.K = g.K; a.Rp = Rp; a.Kp = Kp;
   a.rmax = rmax; a.rexp = rexp; a.dst = dst;
+  if (Rp % PR || Kp % 16) throw Error(ERR_BAD_SHAPE, "gemm_split: packed extents not tiled");
   CC_CHECK(cudaMemsetAsync(rmax, 0, R * sizeof(unsigned long long), s));
-  const int64_t tiles = ((Rp + 31) / 32) * ((Kp + 31) / 32);
-  const unsigned grid = static_cast<unsigned>(std::min<int64_t>(tiles, 148 * 64));
-  pack_kernel<0><<<grid, dim3(32, 8), 0, s>>>(a);
+  const int64_t strips = (Rp / PR) * ((Kp + PKT * PSTRIP - 1) / (PKT * PSTRIP));
+  const int64_t tiles = (Rp / PR) * ((Kp + PKT - 1) / PKT);
+  pack_max_kernel<<<static_cast<unsigned>(std::min<int64_t>(strips, 148 * 8)), PTHREADS, 0, s>>>(a);
   CC_LAUNCH_CHECK();
-  pack_kernel<1><<<grid, dim3(32, 8), 0, s>>>(a);
+  pack_slices_kernel<<<static_cast<unsigned>(std::min<int64_t>(tiles, 148 * 8)), PTHREADS, 0, s>>>(a);
   CC_LAUNCH_CHECK();
 }
 
@@ -820,7 +883,8 @@ std::vector<Panel> panels_of(const Contraction& g, int64_t P) {
   return out;
 }
 
-void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws);
+void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws,
+                 const SplitPackedB* pb = nullptr);
 
 }  // namespace
 
@@ -831,6 +895,38 @@ size_t gemm_split_scratch_bytes(const Contraction& g) {
   h.K = std::min(g.K, panel_len(g));
   const Layout2 L = layout_of(h);
   return L.a_bytes + L.b_bytes + L.meta_bytes;
+}
+
+size_t split_packed_b_bytes(const Contraction& g) {
+  const Layout2 L = layout_of(g);
+  return L.b_bytes + rup(L.Np * 8, 1024) + rup(L.Np * 4, 1024);
+}
+
+size_t split_scratch_bytes_packed_b(const Contraction& g) {
+  const Layout2 L = layout_of(g);
+  return L.a_bytes + L.meta_bytes;
+}
+
+bool split_single_panel(const Contraction& g) { return g.K <= panel_len(g) && g.batch == 1; }
+
+SplitPackedB split_pack_b(const Contraction& g, void* dst, cudaStream_t s) {
+  if (!split_single_panel(g)) throw Error(ERR_UNSUPPORTED, "split_pack_b: K beyond one panel");
+  const Layout2 L = layout_of(g);
+  unsigned char* p = static_cast<unsigned char*>(dst);
+  SplitPackedB b;
+  b.slices = p;
+  auto* bmax = reinterpret_cast<unsigned long long*>(p + L.b_bytes);
+  b.exps = reinterpret_cast<int*>(p + L.b_bytes + rup(L.Np * 8, 1024));
+  b.N = g.N; b.K = g.K; b.Np = L.Np; b.Kp = L.Kp;
+  pack(g.B, false, g, g.N, L.Np, L.Kp, static_cast<__half*>(b.slices), bmax, b.exps, s);
+  return b;
+}
+
+void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream_t s,
+                         SplitScratch& ws) {
+  if (g.M <= 0 || g.N <= 0) return;
+  if (!split_single_panel(g)) throw Error(ERR_UNSUPPORTED, "gemm_split_packed_b: K beyond one panel");
+  split_panel(g, s, ws, &b);
 }
 
 void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
@@ -851,21 +947,30 @@ void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
 
 namespace {
 
-void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
+void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws, const SplitPackedB* pb) {
   const Layout2 L = layout_of(g);
-  if (L.a_bytes + L.b_bytes + L.meta_bytes > ws.bytes) throw Error(ERR_OUT_OF_MEMORY, "gemm_split: scratch too small");
+  // with a pre-packed B the scratch holds A and the metadata only
+  const size_t need = L.a_bytes + (pb ? 0 : L.b_bytes) + L.meta_bytes;
+  if (need > ws.bytes) throw Error(ERR_OUT_OF_MEMORY, "gemm_split: scratch too small");
   if (L.Mp * NSLICE >= (int64_t(1) << 31) || L.Np * NSLICE >= (int64_t(1) << 31) || L.Kp >= (int64_t(1) << 31))
     throw Error(ERR_BAD_SHAPE, "gemm_split: extent too large");
   unsigned char* p = static_cast<unsigned char*>(ws.p);
   __half* Apk = reinterpret_cast<__half*>(p);
   __half* Bpk = reinterpret_cast<__half*>(p + L.a_bytes);
-  unsigned char* meta = p + L.a_bytes + L.b_bytes;
+  unsigned char* meta = p + L.a_bytes + (pb ? 0 : L.b_bytes);
   auto* amax = reinterpret_cast<unsigned long long*>(meta);
   auto* bmax = amax + L.Mp;
   int* aexp = reinterpret_cast<int*>(bmax + L.Np);
   int* bexp = aexp + L.Mp;
   pack(g.A, true, g, g.M, L.Mp, L.Kp, Apk, amax, aexp, s);
-  pack(g.B, false, g, g.N, L.Np, L.Kp, Bpk, bmax, bexp, s);
+  if (pb) {   // B sliced before, by split_pack_b, for this N, K and padding
+    if (pb->N != g.N || pb->K != g.K || pb->Np != L.Np || pb->Kp != L.Kp)
+      throw Error(ERR_INVALID_ARGUMENT, "gemm_split: pre-packed B of another shape");
+    Bpk = static_cast<__half*>(pb->slices);
+    bexp = pb->exps;
+  } else {
+    pack(g.B, false, g, g.N, L.Np, L.Kp, Bpk, bmax, bexp, s);
+  }
   const CUtensorMap ta = make_map(Apk, NSLICE * L.Mp, L.Kp);
   const CUtensorMap tb = make_map(Bpk, NSLICE * L.Np, L.Kp);
   const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;

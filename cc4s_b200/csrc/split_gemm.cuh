@@ -31,6 +31,27 @@ void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws);
 // Bytes of scratch gemm_split needs for this contraction.
 size_t gemm_split_scratch_bytes(const Contraction& g);
 
+// Operand B of a one-panel split contraction, sliced once and reused by several
+// contractions that share B (same N, K and B view), e.g. the ladder's X panel
+// for every block pair of one c range.
+struct SplitPackedB {
+  void* slices = nullptr;  // [3][Np][Kp] FP16
+  int* exps = nullptr;     // [Np] power-of-two column scales
+  int64_t N = 0, K = 0, Np = 0, Kp = 0;
+};
+// Bytes split_pack_b writes (slices, row maxima, exponents).
+size_t split_packed_b_bytes(const Contraction& g);
+// Scratch bytes of gemm_split_packed_b for this contraction (packed A and metadata).
+size_t split_scratch_bytes_packed_b(const Contraction& g);
+// True if g runs as one K panel (the condition for a pre-packed B).
+bool split_single_panel(const Contraction& g);
+// Slices B of g into dst (device memory of split_packed_b_bytes(g) bytes, 1 KiB aligned).
+SplitPackedB split_pack_b(const Contraction& g, void* dst, cudaStream_t s);
+// gemm_split with B taken from split_pack_b (A is sliced into ws as usual; ws must
+// not overlap b).
+void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream_t s,
+                         SplitScratch& ws);
+
 uint64_t split_launch_count();
 
 }  // namespace cc4s_b200

@@ -131,6 +131,33 @@ void gemm_split(const Contraction& g, cudaStream_t, SplitScratch&) {
     }
 }
 
+// Pre-packed B: the emulation keeps a dense copy B[n][k] of the operand's values
+// and slices it again in gemm_split (same values, same slices).
+size_t split_packed_b_bytes(const Contraction& g) { return size_t(g.N) * g.K * 8 + 64; }
+size_t split_scratch_bytes_packed_b(const Contraction&) { return 64; }
+bool split_single_panel(const Contraction& g) { return g.batch == 1; }
+
+SplitPackedB split_pack_b(const Contraction& g, void* dst, cudaStream_t) {
+  const int64_t Ni = g.Ni > 0 ? g.Ni : g.N, Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);
+  Ax Bk = ax(Ki, g.B.s_ro, g.B.s_ri), Bn = ax(Ni, g.B.s_co, g.B.s_ci);
+  double* d = static_cast<double*>(dst);
+  for (int64_t n = 0; n < g.N; ++n)
+    for (int64_t k = 0; k < g.K; ++k) d[n * g.K + k] = g.B.p[Bk.off(k) + Bn.off(n)];
+  SplitPackedB b;
+  b.slices = dst; b.N = g.N; b.K = g.K; b.Np = g.N; b.Kp = g.K;
+  return b;
+}
+
+void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream_t s,
+                         SplitScratch& ws) {
+  if (b.N != g.N || b.K != g.K) throw Error(ERR_INVALID_ARGUMENT, "pre-packed B of another shape");
+  const int64_t Ni = g.Ni > 0 ? g.Ni : g.N, Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);
+  Contraction h = g;   // B(k, n) = copy[n * K + k] in the contraction's two-level k and n
+  h.B.p = static_cast<double*>(b.slices);
+  h.B.s_ro = Ki; h.B.s_ri = 1; h.B.s_co = Ni * g.K; h.B.s_ci = g.K;
+  gemm_split(h, s, ws);
+}
+
 // Plain-loop stand-in for the allocation-free energy entry (host pointers).
 int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t o, int64_t v,
                    int cplx, double* out, cudaStream_t, const char** err) {

@@ -116,3 +116,16 @@ def test_adjoint_line():
         assert f["lambda_converged"] and len(f["fd_directions"]) == 1
         assert f["fd_max_rel_err"] < 1e-5
     assert "max_abs_diff_vs_fp64_over_max" in line["forms"]["split3"]
+
+
+def test_converge_line():
+    """--converge: split form, FP64 from the split amplitudes, FP64 from T = 0."""
+    import build_emu
+    line = _line(build_emu.build(), ["--converge", "--shape", "2,32,40",
+                                      "--converge-energy", "1e-10"])
+    forms = line["forms"]
+    assert set(forms) == {"split3", "fp64_from_split", "fp64"}
+    assert line["value"] == forms["split3"]["abs_dE_vs_fp64"] < 1e-6
+    assert forms["fp64"]["abs_dE_vs_fp64_from_split"] < 1e-9
+    assert forms["fp64_from_split"]["iterations"] < forms["fp64"]["iterations"]
+    assert len(forms["split3"]["history_residuum_norm"]) == forms["split3"]["iterations"]

@@ -314,3 +314,27 @@ def test_relaxed_gradient_split_precision(emu_lib):
         d = rng.standard_normal(s.gamma.shape)
         fd = (solve(s.gamma + h * d)[1] - solve(s.gamma - h * d)[1]) / (2 * h)
         assert abs(fd - (gs * d).sum()) < 1e-6 * abs(fd)
+
+
+def test_split_ladder_prepacked_x_panel(emu_lib):
+    """Split form with several ladder blocks (integralsSliceSize 8 at Nv = 24): the
+    X panel is sliced once per c range and shared by the block pairs; the residual
+    equals the one-block split residual (no shared panel) and the oracle's to the
+    split precision."""
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(8, 24, 30, seed=3)
+    rng = np.random.default_rng(5)
+    T1 = rng.standard_normal((24, 8)) * 0.02
+    T2 = rng.standard_normal((24, 24, 8, 8)) * 0.02
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    out = {}
+    for sl in (8, 24):
+        sol = Solver({"precision": "split3", "integralsSliceSize": sl}, lib=emu_lib)
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, True)
+        out[sl] = sol.residual((T1, T2))
+        sol.close()
+    Q1, Q2 = ccsd.residuum((T1, T2), ccsd.CcsdInputs(s))
+    for R1, R2 in out.values():
+        assert np.abs(R2 - Q2).max() < 1e-6 * np.abs(Q2).max()
+        assert np.abs(R1 - Q1).max() < 1e-6 * np.abs(Q1).max()
+    assert np.abs(out[8][1] - out[24][1]).max() < 1e-12 * np.abs(Q2).max()
