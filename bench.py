@@ -269,7 +269,7 @@ FP64_OVER_SPLIT_BOUND = 4.5
 # generation, of one handle's set-up (vertex upload, integral build) and of the
 # CPU baseline leg.  projected_seconds() uses them to check that the driver's
 # command fits its time limit.
-MEASURED_C2 = {"split3": 20.96, "fp64": 69.68, "inputs": 60.0, "setup": 30.0, "cpu": 40.0,
+MEASURED_C2 = {"split3": 12.0, "fp64": 69.7, "inputs": 60.0, "setup": 30.0, "cpu": 40.0,
                "download": 15.0}
 
 

@@ -94,10 +94,9 @@ void Schedule::split_reserve(size_t regular, size_t extra) {
 
 void Schedule::split_exec(const Contraction& c) {
   const size_t need = gemm_split_scratch_bytes(c);
-  if (need > split_.bytes) {
-    split_extra_bytes_ = 0;   // reallocated without the extra region
-    split_reserve(need, 0);
-  }
+  // growing keeps the size of the extra region (not its contents: no pre-packed
+  // operand is live across a contraction that needs more than the reserved part)
+  if (need > split_.bytes) split_reserve(need, split_extra_bytes_);
   gemm_split(c, s_, split_);
 }
 

@@ -148,7 +148,7 @@ class Schedule {
   // Makes the split scratch hold `regular` bytes for per-contraction packing plus a
   // second region of `extra` bytes (split_extra_) that survives those calls; may
   // reallocate (synchronises).  A later split_exec that needs more than `regular`
-  // reallocates and drops the extra region.
+  // reallocates with an extra region of the same size (its contents are lost).
   void split_reserve(size_t regular, size_t extra);
   // One split contraction whose B was sliced by split_pack_b (recorded like tc_).
   void tc_packed_b_(const Contraction& c, const SplitPackedB& b);
