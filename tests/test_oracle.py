@@ -181,3 +181,23 @@ def test_c0_triples_golden():
     T1, T2 = r["amplitudes"]
     e = triples.triples_atrip(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
     assert abs(e - g["triples"]["correlation"]) < 1e-10
+
+
+def test_real_path_equals_pinned_complex_path():
+    """The real (half-grid) path pinned through the complex path: for a real
+    symmetric vertex the complex path's integrals V_pqsr = sum conj(G_sp) G_qr
+    (VertexCoulombIntegrals.cxx:143-190) equal the real path's sum G_ps G_qr, so a
+    converged CCSD run on the complex path (pinned to cc4s's expected UEG
+    energies by test_ueg_pinned_to_reference_expected_output) and on the real
+    path give the same energies and amplitudes."""
+    s = inputs.synthetic_system(5, 18, 40, seed=12)
+    sc = inputs.System(s.eps_h, s.eps_p, np.asarray(s.gamma, dtype=complex), half_grid=False)
+    opts = dict(maxIterations=60, energyConvergence=1e-12, amplitudesConvergence=1e-10,
+                mixer=dict(type="DiisMixer", maxResidua=5))
+    r = coupled_cluster.run(s, **opts)
+    c = coupled_cluster.run(sc, **opts)
+    assert r["iterations"] == c["iterations"]
+    for k in ("correlation", "direct", "exchange", "secondOrder"):
+        assert abs(r["energy"][k] - c["energy"][k]) < 1e-12 * abs(r["energy"][k])
+    assert np.abs(r["amplitudes"][1] - c["amplitudes"][1].real).max() < 1e-12
+    assert np.abs(c["amplitudes"][1].imag).max() < 1e-14
