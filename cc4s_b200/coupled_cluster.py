@@ -171,11 +171,13 @@ class Solver:
     def residual_vjp(self, T, Rbar, gradient=True):
         """Transposed-Jacobian product of the residual at amplitudes T = (T1, T2):
         returns (T1bar, T2bar) = Rbar^T dR/dT and, if asked, Rbar^T dR/dGamma in the
-        vertex layout (cc4s_cc_residual_vjp; real half-grid path)."""
-        t1 = _abi.as_f64(np.asarray(T[0], dtype=np.float64))
-        t2 = _abi.as_f64(np.asarray(T[1], dtype=np.float64))
-        r1 = _abi.as_f64(np.asarray(Rbar[0], dtype=np.float64))
-        r2 = _abi.as_f64(np.asarray(Rbar[1], dtype=np.float64))
+        vertex layout (cc4s_cc_residual_vjp).  On the complex path every adjoint is
+        d/dRe + i d/dIm of the real-valued <Rbar, R> pairing Re sum conj(Rbar) R."""
+        dt = self._dtype()
+        t1 = _abi.as_f64(np.asarray(T[0], dtype=dt))
+        t2 = _abi.as_f64(np.asarray(T[1], dtype=dt))
+        r1 = _abi.as_f64(np.asarray(Rbar[0], dtype=dt))
+        r2 = _abi.as_f64(np.asarray(Rbar[1], dtype=dt))
         b1, b2 = self._alloc_amps()
         g = self._vertex_grad_buffer() if gradient else None
         self._check(self.lib.cc4s_cc_residual_vjp(self.h, _abi.ptr(t1), _abi.ptr(t2), _abi.ptr(r1),

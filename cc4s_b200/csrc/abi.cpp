@@ -294,23 +294,25 @@ void Handle::backward(double* S_of_G, double* dE_dGamma) {
   ops::release(dG);
 }
 
-// Reverse-mode schedule (real path), built on first use: the fast schedule
-// reuses buffers, this one keeps every recorded value of a residual.
-CcsdReal* Handle::adjoint_schedule() {
-  if (complex_path || opt.method == CC4S_METHOD_DRCCD)
-    throw Error(ERR_UNSUPPORTED, "reverse mode is provided for Ccsd and Ccd on the real path");
+// Reverse-mode schedule, built on first use: the fast schedule reuses buffers,
+// this one keeps every recorded value of a residual.  Real half-grid path
+// (CcsdReal) or complex path (CcsdComplex, adjoints of both planes).
+Schedule* Handle::adjoint_schedule() {
+  if (opt.method == CC4S_METHOD_DRCCD)
+    throw Error(ERR_UNSUPPORTED, "reverse mode is provided for Ccsd and Ccd");
   if (!adj) {
     RealOptions ro;
     ro.ccd = opt.method == CC4S_METHOD_CCD;
     ro.ppl = opt.ppl != 0;
     ro.slab = opt.integrals_slice_size;
     ro.adjoint = true;
-    adj.reset(new CcsdReal(sys, ro, stream));
+    if (complex_path) adj.reset(new CcsdComplex(csys, ro, stream));
+    else adj.reset(new CcsdReal(sys, ro, stream));
   }
   // the handle's precision: the split form runs the recorded residual and the
   // large contractions of every reverse sweep on the tensor cores
   adj->set_precision(opt.precision != CC4S_PRECISION_FP64 ? 3 : 0);
-  return static_cast<CcsdReal*>(adj.get());
+  return adj.get();
 }
 
 // Device vertex-block adjoints -> caller layout Gamma[G, p, q] (column-major,
@@ -318,7 +320,10 @@ CcsdReal* Handle::adjoint_schedule() {
 // go to the two parts).  out is overwritten.
 void Handle::scatter_vertex_bar(const Schedule::VertexBar& vb, double* out) {
   const int64_t o = shape.o, v = shape.v, G = sys.G, NG = in_NG, Np = in_Np;
-  const int64_t es = in_complex ? 2 : 1, parts = in_stacked ? 2 : 1;
+  // planes of the device blocks: stacked Re/Im rows (real path) or the planar
+  // real and imaginary parts (complex path) go to the two parts of the output
+  const int64_t es = in_complex ? 2 : 1, parts = (in_stacked || complex_path) ? 2 : 1;
+  const int64_t planes = complex_path ? 2 : 1;
   std::memset(out, 0, sizeof(double) * NG * Np * Np * es);
   struct Block { const double* d; int64_t row0, nx, col0, ny; };
   const Block blocks[4] = {{vb.Gpp, o, v, o, v}, {vb.Gph, o, v, 0, o}, {vb.Ghh, 0, o, 0, o},
@@ -326,7 +331,7 @@ void Handle::scatter_vertex_bar(const Schedule::VertexBar& vb, double* out) {
   std::vector<double> h;
   for (const Block& b : blocks) {
     if (!b.d) continue;
-    h.resize(G * b.nx * b.ny);
+    h.resize(planes * G * b.nx * b.ny);
     ops::d2h(h.data(), b.d, h.size(), stream);
     ops::sync(stream);
     for (int64_t part = 0; part < parts; ++part)
@@ -342,7 +347,7 @@ void Handle::residual_vjp(const double* T1, const double* T2, const double* R1b,
                           const double* R2b, double* T1b, double* T2b, double* dGamma) {
   require_inputs();
   if (!T1 || !T2 || !R1b || !R2b) throw Error(ERR_INVALID_ARGUMENT, "null amplitudes or adjoint");
-  CcsdReal* adjs = adjoint_schedule();
+  Schedule* adjs = adjoint_schedule();
   const int64_t n = shape.total(), o = shape.o, v = shape.v, G = sys.G;
   std::vector<double*> tmp;
   auto dev = [&](int64_t k) { double* p = ops::alloc(k); tmp.push_back(p); return p; };
@@ -355,10 +360,11 @@ void Handle::residual_vjp(const double* T1, const double* T2, const double* R1b,
     adjs->prepare_vjp(Tin);
     Schedule::VertexBar vb;
     if (dGamma) {
-      vb.Gpp = dev(G * v * v); vb.Gph = dev(G * v * o); vb.Ghh = dev(G * o * o);
-      vb.Ghp = dev(G * o * v);
-      ops::zero(vb.Gpp, G * v * v, stream); ops::zero(vb.Gph, G * v * o, stream);
-      ops::zero(vb.Ghh, G * o * o, stream); ops::zero(vb.Ghp, G * o * v, stream);
+      const int64_t pl = complex_path ? 2 : 1;
+      vb.Gpp = dev(pl * G * v * v); vb.Gph = dev(pl * G * v * o); vb.Ghh = dev(pl * G * o * o);
+      vb.Ghp = dev(pl * G * o * v);
+      ops::zero(vb.Gpp, pl * G * v * v, stream); ops::zero(vb.Gph, pl * G * v * o, stream);
+      ops::zero(vb.Ghh, pl * G * o * o, stream); ops::zero(vb.Ghp, pl * G * o * v, stream);
     }
     adjs->vjp(Rb, Tb, dGamma ? &vb : nullptr, nullptr);
     download_amplitudes(Tb, T1b, T2b, Rbuf);
@@ -378,7 +384,7 @@ void Handle::relaxed_gradient(int max_iterations, double convergence, double* dE
   if (!have_T) throw Error(ERR_STATE, "no amplitudes: run first");
   if (max_iterations < 1) throw Error(ERR_INVALID_ARGUMENT, "maxIterations < 1");
   std::memset(out, 0, sizeof(*out));
-  CcsdReal* adjs = adjoint_schedule();
+  Schedule* adjs = adjoint_schedule();
   const int64_t n = shape.total(), o = shape.o, v = shape.v, G = sys.G, n1 = shape.n1();
   std::vector<double*> tmp;
   auto dev = [&](int64_t k) { double* p = ops::alloc(k); tmp.push_back(p); return p; };
@@ -386,7 +392,8 @@ void Handle::relaxed_gradient(int max_iterations, double convergence, double* dE
     double* lam = dev(n);
     double* g = dev(n);
     double* Jt = dev(n);
-    double* VdB = dev(n1 * n1);
+    const int64_t planes = complex_path ? 2 : 1;
+    double* VdB = dev(planes * n1 * n1);
     ops::event_record(ev0, stream);
     adjs->prepare_vjp(Tcur);
     adjs->energy_gradients(Tcur, g, VdB);
@@ -431,10 +438,10 @@ void Handle::relaxed_gradient(int max_iterations, double convergence, double* dE
     }
     out->iterations = it;
     Schedule::VertexBar vb;
-    vb.Gpp = dev(G * v * v); vb.Gph = dev(G * v * o); vb.Ghh = dev(G * o * o);
-    vb.Ghp = dev(G * o * v);
-    ops::zero(vb.Gpp, G * v * v, stream); ops::zero(vb.Gph, G * v * o, stream);
-    ops::zero(vb.Ghh, G * o * o, stream); ops::zero(vb.Ghp, G * o * v, stream);
+    vb.Gpp = dev(planes * G * v * v); vb.Gph = dev(planes * G * v * o);
+    vb.Ghh = dev(planes * G * o * o); vb.Ghp = dev(planes * G * o * v);
+    ops::zero(vb.Gpp, planes * G * v * v, stream); ops::zero(vb.Gph, planes * G * v * o, stream);
+    ops::zero(vb.Ghh, planes * G * o * o, stream); ops::zero(vb.Ghp, planes * G * o * v, stream);
     ops::event_record(ev0, stream);
     adjs->vjp(lam, Jt, &vb, VdB);
     ops::event_record(ev1, stream);

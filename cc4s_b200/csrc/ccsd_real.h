@@ -35,7 +35,7 @@ class CcsdReal : public Schedule {
   const double* Ve() const override { return nullptr; }
   // dE/dT (amplitude vector g) and dE/dV_abij (pair layout Vd_bar, may be null) of
   // E = sum X (2 V_abij - V_abji), X = T2 + T1 T1, at amplitudes T.
-  void energy_gradients(const double* T, double* g, double* Vd_bar);
+  void energy_gradients(const double* T, double* g, double* Vd_bar) override;
   void prepare_vjp(const double* T) override;
   void vjp(const double* Rbar, double* Tbar, const VertexBar* gbar,
            const double* extra_Vd_bar) override;

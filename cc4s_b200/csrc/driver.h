@@ -39,7 +39,7 @@ struct Handle {
   void mix(double* A_new, double* dT_new, double* norm2_dev, double* out);
   std::string diis_failure(int status, int iteration, double energy, double norm);
   // reverse mode (real path)
-  CcsdReal* adjoint_schedule();
+  Schedule* adjoint_schedule();
   void scatter_vertex_bar(const Schedule::VertexBar& vb, double* out);
   void residual_vjp(const double* T1, const double* T2, const double* R1b, const double* R2b,
                     double* T1b, double* T2b, double* dGamma);

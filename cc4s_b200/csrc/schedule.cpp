@@ -487,6 +487,7 @@ void Schedule::reverse(const std::vector<TapeOp>& tape) {
       case TapeOp::GEMM: {
         if (op.recompute) {
           exec_(op.pre);
+          for (const Contraction& q : op.pres) exec_(q);
           if (double* zb = bar_of(op.zero_p)) ops::zero(zb, op.zero_n, s_);
         }
         reverse_gemm(op.c);
@@ -558,12 +559,16 @@ void Schedule::reverse(const std::vector<TapeOp>& tape) {
   }
 }
 
+void Schedule::energy_gradients(const double*, double*, double*) {
+  throw Error(ERR_UNSUPPORTED, "energy gradients are provided by the CCSD/CCD schedules");
+}
+
 void Schedule::prepare_vjp(const double*) {
-  throw Error(ERR_UNSUPPORTED, "reverse mode is provided for the real-path CCSD/CCD schedule");
+  throw Error(ERR_UNSUPPORTED, "reverse mode is provided by the CCSD/CCD schedules");
 }
 
 void Schedule::vjp(const double*, double*, const VertexBar*, const double*) {
-  throw Error(ERR_UNSUPPORTED, "reverse mode is provided for the real-path CCSD/CCD schedule");
+  throw Error(ERR_UNSUPPORTED, "reverse mode is provided by the CCSD/CCD schedules");
 }
 
 }  // namespace cc4s_b200

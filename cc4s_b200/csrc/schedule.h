@@ -84,6 +84,9 @@ class Schedule {
     double* Ghp = nullptr;  // [G][o][v]
   };
   bool adjoint_mode() const { return adjoint_; }
+  // dE/dT (amplitude vector g, every plane) and dE/dV_abij (pair layout, every
+  // plane; may be null) of the correlation energy at amplitudes T.
+  virtual void energy_gradients(const double* T, double* g, double* Vd_bar);
   virtual void prepare_vjp(const double* T);
   virtual void vjp(const double* Rbar, double* Tbar, const VertexBar* gbar,
                    const double* extra_Vd_bar);
@@ -102,8 +105,9 @@ class Schedule {
   struct TapeOp {
     enum Kind { GEMM, PERM, AXPBY, RANK1, SYMM, COPY, ZERO } kind = GEMM;
     Contraction c;                      // GEMM
-    bool recompute = false;             // GEMM: rerun `pre` forward and clear the
-    Contraction pre;                    // adjoint of [zero_p, zero_p + zero_n) first
+    bool recompute = false;             // GEMM: rerun `pre` (and `pres`) forward and
+    Contraction pre;                    // clear the adjoint of [zero_p, zero_p + zero_n) first
+    std::vector<Contraction> pres;      // further contractions of the recomputation
     double* zero_p = nullptr;
     int64_t zero_n = 0;
     double* dst = nullptr;              // PERM / AXPBY / RANK1 / SYMM / COPY / ZERO output

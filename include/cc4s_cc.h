@@ -171,24 +171,28 @@ int cc4s_cc_residual(cc4s_cc_handle* h, const double* T1, const double* T2, doub
  * d/dRe + i d/dIm), nonzero in the particle-hole block.  Either output may be NULL. */
 int cc4s_cc_backward(cc4s_cc_handle* h, double* S_of_G, double* dE_dGamma);
 
-/* Transposed-Jacobian product of the residual (real half-grid path, Ccsd / Ccd):
- * at amplitudes T1 [Nv,No], T2 [Nv,Nv,No,No] (reference layout, as for
- * cc4s_cc_residual) and an adjoint R1bar, R2bar of the residual (same layout),
+/* Transposed-Jacobian product of the residual (Ccsd / Ccd, real half-grid and
+ * complex paths): at amplitudes T1 [Nv,No], T2 [Nv,Nv,No,No] (reference layout,
+ * as for cc4s_cc_residual) and an adjoint R1bar, R2bar of the residual (same layout),
  *   T1bar, T2bar = Rbar^T dR/dT   (T2bar projected on T_abij = T_baji),
  *   dGamma       = Rbar^T dR/dGamma in the caller's vertex layout (may be NULL).
- * The adjoint of Ccsd::getResiduum (Ccsd.cxx:77-378), built by replaying the
- * recorded residual backwards. */
+ * Complex path: the real pairing Re sum conj(Rbar) R is differentiated, every
+ * adjoint is d/dRe + i d/dIm.  The adjoint of Ccsd::getResiduum (Ccsd.cxx:77-378,
+ * complex :382-633), built by replaying the recorded residual backwards. */
 int cc4s_cc_residual_vjp(cc4s_cc_handle* h, const double* T1, const double* T2,
                          const double* R1bar, const double* R2bar, double* T1bar, double* T2bar,
                          double* dGamma);
 
-/* Relaxed gradient of the converged correlation energy (after cc4s_cc_run, real
- * half-grid path, Ccsd / Ccd): solves the Lambda equations
+/* Relaxed gradient of the converged correlation energy (after cc4s_cc_run, Ccsd /
+ * Ccd, real half-grid and complex paths): solves the Lambda equations
  *   (dR/dT + D)^T lambda = -dE/dT
  * with the amplitude iteration's Jacobi update, level shift and mixer, each
  * iteration one transposed-Jacobian product, and returns
  *   dE_dGamma = dE_c/dGamma|_T + lambda^T dR/dGamma
- * in the caller's vertex layout (complex input: d/dRe + i d/dIm).  Converged when
+ * in the caller's vertex layout (complex input: d/dRe + i d/dIm; on the complex
+ * path the amplitude iteration keeps T_abij = T_baji, exact for a vertex with
+ * Gamma_qp = conj(Gamma_pq), so directional derivatives are meaningful along
+ * directions that keep that symmetry).  Converged when
  * the norm of the change of lambda is below `convergence`; otherwise status 4.
  * Replaces finite differences of CoupledCluster::run (CoupledCluster.cxx:56-191)
  * around converged amplitudes. */

@@ -338,3 +338,75 @@ def test_split_ladder_prepacked_x_panel(emu_lib):
         assert np.abs(R2 - Q2).max() < 1e-6 * np.abs(Q2).max()
         assert np.abs(R1 - Q1).max() < 1e-6 * np.abs(Q1).max()
     assert np.abs(out[8][1] - out[24][1]).max() < 1e-12 * np.abs(Q2).max()
+
+
+@pytest.mark.parametrize("method,ppl", [("Ccsd", True), ("Ccd", True), ("Ccsd", False)])
+def test_complex_residual_vjp_matches_finite_differences(emu_lib, method, ppl):
+    """Complex path: the transposed-Jacobian product of the residual (reverse
+    replay of the recorded planar schedule) against central differences of
+    Re sum conj(Rbar) R(T) along complex directions in T and in the vertex; the
+    adjoints are d/dRe + i d/dIm."""
+    from cc4s_b200 import Solver
+    No, Nv, NG = 3, 8, 6
+    s = inputs.synthetic_system(No, Nv, NG, complex=True, seed=3)
+    rng = np.random.default_rng(1)
+
+    def c(shape):
+        return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+    def sym(x):
+        return x + x.transpose(1, 0, 3, 2)
+    T = (c((Nv, No)) * 0.1, sym(c((Nv, Nv, No, No))) * 0.05)
+    Rb = (c((Nv, No)), c((Nv, Nv, No, No)))
+    opts = {"method": method, "ppl": ppl}
+    sol = Solver(opts, lib=emu_lib)
+    sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=False)
+    (T1b, T2b), Gb = sol.residual_vjp(T, Rb)
+
+    def f(TT, gm=None):
+        so = sol
+        if gm is not None:
+            so = Solver(opts, lib=emu_lib)
+            so.set_inputs(s.eps_h, s.eps_p, gm, half_grid=False)
+        return sum(np.real(np.conj(a) * b).sum() for a, b in zip(Rb, so.residual(TT)))
+    d = (c((Nv, No)) * (method == "Ccsd"), sym(c((Nv, Nv, No, No))))
+    h = 1e-5
+    fd = (f((T[0] + h * d[0], T[1] + h * d[1])) - f((T[0] - h * d[0], T[1] - h * d[1]))) / (2 * h)
+    an = np.real(np.conj(T1b) * d[0]).sum() + np.real(np.conj(T2b) * d[1]).sum()
+    assert abs(fd - an) < 1e-7 * abs(fd)
+    dg = c(s.gamma.shape)
+    fdg = (f(T, s.gamma + h * dg) - f(T, s.gamma - h * dg)) / (2 * h)
+    assert abs(fdg - np.real(np.conj(Gb) * dg).sum()) < 1e-8 * abs(fdg)
+
+
+@pytest.mark.parametrize("method", ["Ccsd", "Ccd"])
+def test_complex_relaxed_gradient_matches_finite_differences(emu_lib, method):
+    """Complex path: Lambda equations by transposed-Jacobian products, relaxed
+    dE_c/dGamma (d/dRe + i d/dIm) against central differences of re-converged
+    energies, to 1e-6 relative.  The directions keep the vertex Hermitian
+    (Gamma_qp = conj(Gamma_pq)), the symmetry under which the integrals are pair
+    symmetric (V_abij = V_baji) and the amplitude iteration keeps T_abij = T_baji.
+    The differences are Richardson-extrapolated from steps 1e-5 and 5e-6 (these
+    Hermitian directions are long enough for an O(h^2) error of a few 1e-6)."""
+    from cc4s_b200 import Solver
+    s = inputs.synthetic_system(3, 10, 16, complex=True, seed=2)
+    opts = dict(method=method, maxIterations=80, energyConvergence=1e-14,
+                amplitudesConvergence=1e-12)
+
+    def energy(gm):
+        so = Solver(opts, lib=emu_lib)
+        so.set_inputs(s.eps_h, s.eps_p, gm, half_grid=False)
+        return so, so.run()["correlation"]
+    sol, _ = energy(s.gamma)
+    g, info = sol.relaxed_gradient(max_iterations=100, convergence=1e-12)
+    assert info["converged"]
+    rng = np.random.default_rng(5)
+    h = 1e-5
+    for _ in range(3):
+        d = rng.standard_normal(s.gamma.shape) + 1j * rng.standard_normal(s.gamma.shape)
+        d = d + np.conj(d.transpose(0, 2, 1))
+
+        def cd(step):
+            return (energy(s.gamma + step * d)[1] - energy(s.gamma - step * d)[1]) / (2 * step)
+        fd = (4.0 * cd(h / 2) - cd(h)) / 3.0
+        assert abs(fd - np.real(np.conj(g) * d).sum()) < 1e-6 * abs(fd)

@@ -458,3 +458,31 @@ def test_real_path_equals_complex_path_on_device(Solver):
     for k in ("correlation", "direct", "exchange", "secondOrder"):
         assert abs(rr[k] - rc[k]) < 1e-10 * abs(rr[k])
     assert _rel(Tc[1].real, Tr[1]) < 1e-10 and np.abs(Tc[1].imag).max() < 1e-12
+
+
+def test_complex_relaxed_gradient_on_device(Solver):
+    """Complex path on the B200: the relaxed dE_c/dGamma (Lambda equations, d/dRe +
+    i d/dIm) against central differences of re-converged energies along Hermitian
+    vertex directions (Richardson-extrapolated from steps 1e-5 and 5e-6), 1e-6
+    relative."""
+    s = inputs.synthetic_system(6, 36, 80, complex=True, seed=2)
+    opts = dict(maxIterations=100, energyConvergence=1e-14, amplitudesConvergence=1e-11)
+
+    def energy(gm):
+        so = Solver(opts)
+        so.set_inputs(s.eps_h, s.eps_p, gm, half_grid=False)
+        return so, so.run()["correlation"]
+    sol, _ = energy(s.gamma)
+    g, info = sol.relaxed_gradient(max_iterations=100, convergence=1e-11)
+    sol.close()
+    assert info["converged"]
+    rng = np.random.default_rng(5)
+    h = 1e-5
+    for _ in range(3):
+        d = rng.standard_normal(s.gamma.shape) + 1j * rng.standard_normal(s.gamma.shape)
+        d = d + np.conj(d.transpose(0, 2, 1))
+
+        def cd(step):
+            return (energy(s.gamma + step * d)[1] - energy(s.gamma - step * d)[1]) / (2 * step)
+        fd = (4.0 * cd(h / 2) - cd(h)) / 3.0
+        assert abs(fd - np.real(np.conj(g) * d).sum()) < 1e-6 * abs(fd)
