@@ -2,7 +2,7 @@
 
 A "step" is one CCSD iteration (residual, Jacobi update, DIIS, energy) on a
 seeded synthetic system.  Default workload: No=64, Nv=640, NG=2560, real
-(T2 13.4 GB), vertex scaled by 0.3 (CCSD diverges on the unscaled synthetic
+(T2 13.4 GB), vertex scaled by 0.2 (CCSD diverges on the unscaled synthetic
 vertex; the cost of an iteration does not depend on the scale).  T2 and the
 vertex are far larger than L2, so no flush is needed between iterations.
 
@@ -255,9 +255,10 @@ def timed_run(opts, inputs, W, K, world, local, keep_amplitudes=False):
 
 # Default vertex scale of the CCSD line: the synthetic systems of c1, c2 and c4
 # are strongly correlated and CCSD from T = 0 diverges on the unscaled vertex
-# (E_c of about -3200 Eh after four iterations at c2); at 0.3 it converges.  The
+# (E_c of about -3200 Eh after four iterations at c2; at scale 0.3 c1 and c4
+# converge but c2 still diverges after ~80 iterations); at 0.2 all converge.  The
 # cost of an iteration does not depend on the scale.
-DEFAULT_VERTEX_SCALE = 0.3
+DEFAULT_VERTEX_SCALE = 0.2
 # Upper bound of the FP64 form's time per iteration relative to the split form,
 # used only to decide whether the FP64 comparison still fits the time budget
 # (measured at c2: 3.3).
@@ -415,9 +416,10 @@ def run_adjoint(args, local):
     transposed-Jacobian products, relaxed dE_c/dGamma; the same with the split
     form's backward (forward and reverse contractions on the split kernel); the
     time of each against one forward iteration, and both gradients against
-    central differences (step 1e-5) of re-converged FP64 energies on
-    --fd-directions random vertex directions (each perturbed solve starts from
-    the converged amplitudes)."""
+    central differences of re-converged FP64 energies (steps 1e-5 and 5e-6,
+    Richardson-extrapolated) on --fd-directions random vertex directions (each
+    perturbed solve starts from the converged amplitudes and reaches the FP64
+    fixed point)."""
     import numpy as np
     import torch
     from cc4s_b200 import Solver
@@ -430,7 +432,7 @@ def run_adjoint(args, local):
         eh, ep, g, hg = synthetic(o, v, G, complex=False, seed=0)
     else:
         eh, ep, g, hg = config(cfg, seed=0)
-    scale = args.vertex_scale if args.vertex_scale is not None else 0.3
+    scale = args.vertex_scale if args.vertex_scale is not None else DEFAULT_VERTEX_SCALE
     g *= scale
     # energies converged far below the 1e-5 step times the 1e-6 bound on the
     # derivative; the split form's rounding (~1e-9 relative in the residual) sets
@@ -467,17 +469,34 @@ def run_adjoint(args, local):
     rng = np.random.default_rng(7)
     h = 1e-5
     checks = {p: [] for p in forms}
+
+    def fd_energy(gm):
+        # the FP64 fixed point from the converged amplitudes: split iterations until
+        # the residuum norm is below 1e-6, FP64 iterations to energyConvergence 1e-13
+        so = Solver(dict(base, precision="split3", precisionRefinement=1e-6, **tight))
+        so.set_inputs(eh, ep, gm, half_grid=hg)
+        so.set_initial_amplitudes(*T0)
+        r = so.run()
+        so.close()
+        return r
+
+    def central(d, step):
+        rp, rm_ = fd_energy(g + step * d), fd_energy(g - step * d)
+        return (rp["correlation"] - rm_["correlation"]) / (2 * step), [rp["iterations"],
+                                                                        rm_["iterations"]]
     for _ in range(args.fd_directions):
         d = rng.standard_normal(g.shape)
-        sp, rp = solve(g + h * d, start=T0)
-        sp.close()
-        sm, rm_ = solve(g - h * d, start=T0)
-        sm.close()
-        fd = (rp["correlation"] - rm_["correlation"]) / (2 * h)
+        # Richardson: the O(h^2) error of a central difference along these long
+        # directions (|d| ~ sqrt(#entries)) is ~1e-5 relative at h = 1e-5
+        c1, it1 = central(d, h)
+        c2, it2 = central(d, h / 2)
+        fd = (4.0 * c2 - c1) / 3.0
         for p, f in forms.items():
             an = float((f["grad"] * d).sum())
-            checks[p].append({"fd": fd, "adjoint": an, "rel_err": abs(fd - an) / abs(fd),
-                              "fd_iterations": [rp["iterations"], rm_["iterations"]]})
+            checks[p].append({"fd": fd, "fd_h": c1, "fd_h2": c2, "adjoint": an,
+                              "rel_err": abs(fd - an) / abs(fd),
+                              "rel_err_plain_central": abs(c1 - an) / abs(c1),
+                              "fd_iterations": it1 + it2})
     head = "fp64" if "fp64" in forms else args.precision
     out = {}
     for p, f in forms.items():
@@ -505,7 +524,9 @@ def run_adjoint(args, local):
             "unit": "x forward iteration", "higher_is_better": False, "n_gpus": 1, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "CCSD %s: No=%d Nv=%d NG=%d real, DIIS 5" % (cfg, o, v, G),
-                       "vertex_scale": scale, "fd_step": h, "fd_directions": args.fd_directions},
+                       "vertex_scale": scale, "fd_steps": [h, h / 2], "fd_directions": args.fd_directions,
+                       "fd": "central differences at h and h/2, Richardson-extrapolated "
+                             "(4 D(h/2) - D(h)) / 3"},
             "forms": out}
 
 
@@ -518,7 +539,7 @@ def run_converge(args, local):
       fp64            the FP64 form from T = 0 (skipped with --converge-skip-fp64).
     Reports |E_split - E_fp64|, the per-iteration energies and residuum norms,
     the final amplitudes' difference (max and norm, relative), iterations and
-    time to solution.  The synthetic vertex is scaled (default 0.3): unscaled,
+    time to solution.  The synthetic vertex is scaled (default 0.2): unscaled,
     CCSD diverges at these sizes."""
     import numpy as np
     import torch
@@ -532,7 +553,7 @@ def run_converge(args, local):
         eh, ep, g, hg = synthetic(o, v, G, complex=False, seed=0)
     else:
         eh, ep, g, hg = config(cfg, seed=0)
-    scale = args.vertex_scale if args.vertex_scale is not None else 0.3
+    scale = args.vertex_scale if args.vertex_scale is not None else DEFAULT_VERTEX_SCALE
     g *= scale
     base = dict(maxIterations=100, energyConvergence=args.converge_energy,
                 amplitudesConvergence=1e-7, mixer=dict(type="DiisMixer", maxResidua=5),
@@ -938,7 +959,7 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="--triples: device time of each phase of the block loop")
     ap.add_argument("--vertex-scale", type=float, default=None,
-                    help="scale of the synthetic vertex (default 0.3 for the CCSD line, the "
+                    help="scale of the synthetic vertex (default 0.2 for the CCSD line, the "
                          "reference arm, --converge and --adjoint: CCSD on the unscaled "
                          "synthetic vertex diverges at these sizes, strongly correlated; 1 for "
                          "--triples and --fsc)")
