@@ -82,7 +82,8 @@ class LambdaResult(ctypes.Structure):
 
 
 class TriplesOptions(ctypes.Structure):
-    _fields_ = [("block_size", ctypes.c_int64), ("formulation", ctypes.c_int)]
+    _fields_ = [("block_size", ctypes.c_int64), ("formulation", ctypes.c_int),
+                ("cT", ctypes.c_int)]
 
 
 class TriplesResult(ctypes.Structure):

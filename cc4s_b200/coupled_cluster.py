@@ -200,13 +200,15 @@ class Solver:
                     vjp_seconds=res.vjp_seconds, gradient_seconds=res.gradient_seconds)
         return self._vertex_grad(g), info
 
-    def perturbative_triples(self, block_size=0, reference_form=False):
+    def perturbative_triples(self, block_size=0, reference_form=False, cT=False):
         """(T) energy at the current amplitudes (cc4s_cc_perturbative_triples);
-        reference_form: the conjugation of PerturbativeTriplesReference (complex path)."""
+        reference_form: the conjugation of PerturbativeTriplesReference (complex path);
+        cT: its completely renormalised branch (PerturbativeTriplesReference.cxx:92-109)."""
         o = _abi.TriplesOptions()
         self.lib.cc4s_cc_triples_default_options(ctypes.byref(o))
         o.block_size = int(block_size)
         o.formulation = 1 if reference_form else 0
+        o.cT = 1 if cT else 0
         r = _abi.TriplesResult()
         self._check(self.lib.cc4s_cc_perturbative_triples(self.h, ctypes.byref(o),
                                                           ctypes.byref(r)))
@@ -313,7 +315,8 @@ class PerturbativeTriples:
     (the integral slices are formed on the device, so coulombIntegrals is not
     needed), halfGrid; plus precision ('fp64' or 'split3'), blockSize and
     referenceForm (the complex-path conjugation of PerturbativeTriplesReference;
-    the pipeline sets it for that step name), and optionally mp2PairEnergies
+    the pipeline sets it for that step name), cT (that step's completely
+    renormalised branch, PerturbativeTriplesReference.cxx:70-71; 0 or 1), and optionally mp2PairEnergies
     (the complete-basis-set estimates of the MP2 pair energies, any shape).
     Returns {'energy': {'correlation', 'unit'}} like the reference, with
     'starCorrection' = (sum of mp2PairEnergies) / E_MP2 * correlation when
@@ -334,7 +337,8 @@ class PerturbativeTriples:
             s.set_inputs(eps["h"], eps["p"], gamma, half_grid=half_grid)
             s.set_initial_amplitudes(amps["ph"], amps["pphh"])
             r = s.perturbative_triples(int(arguments.get("blockSize", 0) or 0),
-                                       reference_form=bool(arguments.get("referenceForm", False)))
+                                       reference_form=bool(arguments.get("referenceForm", False)),
+                                       cT=int(arguments.get("cT", 0) or 0) == 1)
         finally:
             s.close()
         energy = {"correlation": r["correlation"], "unit": 1.0}

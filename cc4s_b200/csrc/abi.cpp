@@ -472,9 +472,11 @@ void Handle::triples(const cc4s_cc_triples_options& o, cc4s_cc_triples_result* o
   if (o.block_size < 0) throw Error(ERR_INVALID_ARGUMENT, "block_size < 0");
   if (o.formulation != 0 && o.formulation != 1)
     throw Error(ERR_INVALID_ARGUMENT, "formulation must be 0 or 1");
+  if (o.cT != 0 && o.cT != 1) throw Error(ERR_INVALID_ARGUMENT, "cT must be 0 or 1");
   TriplesOptions to;
   to.block = o.block_size;
   to.reference_form = o.formulation == 1;
+  to.complete = o.cT == 1;
   Triples tr(sys, complex_path ? &csys : nullptr, to, stream);
   tr.set_precision(opt.precision == CC4S_PRECISION_SPLIT3 ? 3 : 0);
   tr.set_profile(opt.profile != 0);
@@ -706,6 +708,7 @@ void cc4s_cc_triples_default_options(cc4s_cc_triples_options* o) {
   if (!o) return;
   o->block_size = 0;
   o->formulation = 0;
+  o->cT = 0;
 }
 
 int cc4s_cc_perturbative_triples(cc4s_cc_handle* h, const cc4s_cc_triples_options* opt,

@@ -181,11 +181,14 @@ void triples_singles(double* S, double* S_im, const double* t1, const double* t1
 // Y(q) = sum_pi coef[pi] S(q o pi), where S(q o pi) takes the hole indices of the
 // three pairs in the order pi (pi over the six permutations 012, 021, 102, 120,
 // 201, 210):  out_dev[0] = sum_q Re W Re Y / D,  out_dev[1] = sum_q Im W Im Y / D.
-// ws holds the partial sums (>= 2 * 148 * 4 doubles).
+// ws holds the partial sums (>= 2 * 148 * 4 doubles).  M (planar, may be null):
+// a block array of the same layout taking the place of W (the cT branch, whose
+// energy is sum M Y / D).
 void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
                     const double* V, const double* V_im, const double* eps_h,
                     const double* eps_p, const TriplesBlock& b, const double coef[6],
-                    double* ws, double* out_dev, Stream s);
+                    double* ws, double* out_dev, Stream s, const double* M = nullptr,
+                    const double* M_im = nullptr);
 
 // Number of bandwidth-kernel launches issued so far.
 uint64_t launch_count();

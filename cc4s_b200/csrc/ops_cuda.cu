@@ -1076,6 +1076,8 @@ struct TriplesArgs {
   int64_t o, n1, P1, P2, P3, L2, L3, total;
   double coef[6];
   double* ws;
+  const double* M;   // cT branch: block array used in place of W = S - singles
+  const double* Mi;
 };
 
 struct Cplx { double re, im; };
@@ -1136,8 +1138,9 @@ __global__ void triples_energy_kernel(TriplesArgs a) {
       if (CPLX) yi += a.coef[k] * a.Si[idx[k]];
     }
     const double inv = 1.0 / d;
-    acc[0] += (a.S[e] - sg.re) * yr * inv;
-    if (CPLX) acc[1] += (a.Si[e] - sg.im) * yi * inv;
+    const double wr = a.M ? a.M[e] : a.S[e] - sg.re;
+    acc[0] += wr * yr * inv;
+    if (CPLX) acc[1] += (a.M ? a.Mi[e] : a.Si[e] - sg.im) * yi * inv;
   }
   block_sum<2>(acc);
   if (threadIdx.x == 0) {
@@ -1173,9 +1176,11 @@ void triples_singles(double* S, double* S_im, const double* t1, const double* t1
 void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
                     const double* V, const double* V_im, const double* eps_h,
                     const double* eps_p, const TriplesBlock& b, const double coef[6],
-                    double* ws, double* out_dev, Stream s) {
+                    double* ws, double* out_dev, Stream s, const double* M,
+                    const double* M_im) {
   TriplesArgs a = triples_args(t1, t1_im, V, V_im, b);
   a.S = S; a.Si = S_im; a.eh = eps_h; a.ep = eps_p; a.ws = ws;
+  a.M = M; a.Mi = M_im;
   for (int k = 0; k < 6; ++k) a.coef[k] = coef[k];
   if (S_im)
     triples_energy_kernel<true><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);

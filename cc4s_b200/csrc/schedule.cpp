@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <vector>
 
@@ -185,6 +186,167 @@ void Schedule::zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bo
     wrote = true;
   }
   if (!wrote) throw Error(ERR_STATE, "zgemm: complex result from real operands");
+}
+
+namespace {
+// One index of an ein() operand: label id, extent, element stride.
+struct EinAx {
+  int id;
+  int64_t n, s;
+};
+struct EinOps {
+  double* p[3];
+  std::vector<EinAx> ax[3];  // memory order, outer first
+};
+int ein_find(const std::vector<EinAx>& v, int id) {
+  for (size_t k = 0; k < v.size(); ++k)
+    if (v[k].id == id) return static_cast<int>(k);
+  return -1;
+}
+// Fuses index pairs (x, y) that are adjacent (y right after x, stride_x = n_y stride_y)
+// in every operand holding either of them.
+void ein_fuse(EinOps& e, int& next_id) {
+  for (bool again = true; again;) {
+    again = false;
+    for (int t = 0; t < 3 && !again; ++t)
+      for (size_t k = 0; k + 1 < e.ax[t].size() && !again; ++k) {
+        const int x = e.ax[t][k].id, y = e.ax[t][k + 1].id;
+        bool ok = true;
+        for (int u = 0; u < 3 && ok; ++u) {
+          const int px = ein_find(e.ax[u], x), py = ein_find(e.ax[u], y);
+          if ((px < 0) != (py < 0)) ok = false;
+          else if (px >= 0)
+            ok = py == px + 1 && e.ax[u][px].s == e.ax[u][py].n * e.ax[u][py].s;
+        }
+        if (!ok) continue;
+        const int id = next_id++;
+        for (int u = 0; u < 3; ++u) {
+          const int px = ein_find(e.ax[u], x);
+          if (px < 0) continue;
+          EinAx& a = e.ax[u][px];
+          const EinAx b = e.ax[u][px + 1];
+          a = EinAx{id, a.n * b.n, b.s};
+          e.ax[u].erase(e.ax[u].begin() + px + 1);
+        }
+        again = true;
+      }
+  }
+}
+// Groups the indices, loops on the host over one index of any group wider than
+// two levels (the smallest such index; a summed one accumulates), and hands one
+// contraction per launch to `launch`.
+void ein_run(EinOps e, int& next_id, double alpha, double beta,
+             const std::function<void(const Contraction&)>& launch) {
+  ein_fuse(e, next_id);
+  std::vector<int> g[4];  // M (A, C), N (B, C), K (A, B), batch (all three)
+  auto has = [&](int t, int id) { return ein_find(e.ax[t], id) >= 0; };
+  for (int t = 0; t < 3; ++t)
+    for (const auto& a : e.ax[t]) {
+      const bool inA = has(0, a.id), inB = has(1, a.id), inC = has(2, a.id);
+      const int grp = inA && inB && inC ? 3 : inA && inC ? 0 : inB && inC ? 1 : inA && inB ? 2 : -1;
+      if (grp < 0) throw Error(ERR_STATE, "ein: a label appears in one operand only");
+      if (std::find(g[grp].begin(), g[grp].end(), a.id) == g[grp].end()) g[grp].push_back(a.id);
+    }
+  for (int k = 0; k < 4; ++k) {
+    if (g[k].size() <= 2) continue;
+    int best = -1;
+    int64_t bn = 0;
+    for (int id : g[k]) {
+      for (int t = 0; t < 3; ++t) {
+        const int q = ein_find(e.ax[t], id);
+        if (q >= 0 && (best < 0 || e.ax[t][q].n < bn)) { best = id; bn = e.ax[t][q].n; }
+      }
+    }
+    for (int64_t x = 0; x < bn; ++x) {
+      EinOps f = e;
+      for (int t = 0; t < 3; ++t) {
+        const int q = ein_find(f.ax[t], best);
+        if (q < 0) continue;
+        f.p[t] += x * f.ax[t][q].s;
+        f.ax[t].erase(f.ax[t].begin() + q);
+      }
+      ein_run(f, next_id, alpha, k == 2 && x > 0 ? 1.0 : beta, launch);
+    }
+    return;
+  }
+  // extent, inner extent (0: one level) and the outer / inner strides in operand t
+  auto level = [&](const std::vector<int>& ids, int t, int64_t& so, int64_t& si) {
+    so = si = 0;
+    if (ids.empty()) return;
+    const EinAx& in = e.ax[t][ein_find(e.ax[t], ids.back())];
+    si = in.s;
+    if (ids.size() == 2) so = e.ax[t][ein_find(e.ax[t], ids.front())].s;
+  };
+  auto extent = [&](const std::vector<int>& ids, int64_t& n, int64_t& ni) {
+    n = 1; ni = 0;
+    for (int id : ids)
+      for (int t = 0; t < 3; ++t) {
+        const int q = ein_find(e.ax[t], id);
+        if (q >= 0) { n *= e.ax[t][q].n; if (ids.size() == 2 && id == ids.back()) ni = e.ax[t][q].n; break; }
+      }
+  };
+  // inner level of M and N: the index with the smaller stride in C
+  for (int k : {0, 1})
+    if (g[k].size() == 2 && e.ax[2][ein_find(e.ax[2], g[k][0])].s <
+                                e.ax[2][ein_find(e.ax[2], g[k][1])].s)
+      std::swap(g[k][0], g[k][1]);
+  Contraction c;
+  extent(g[0], c.M, c.Mi);
+  extent(g[1], c.N, c.Ni);
+  extent(g[2], c.K, c.Ki);
+  extent(g[3], c.batch, c.Bi);
+  c.A.p = e.p[0]; c.B.p = e.p[1]; c.C.p = e.p[2];
+  level(g[0], 0, c.A.s_ro, c.A.s_ri);
+  level(g[2], 0, c.A.s_co, c.A.s_ci);
+  level(g[2], 1, c.B.s_ro, c.B.s_ri);
+  level(g[1], 1, c.B.s_co, c.B.s_ci);
+  level(g[0], 2, c.C.s_ro, c.C.s_ri);
+  level(g[1], 2, c.C.s_co, c.C.s_ci);
+  for (int t = 0; t < 3; ++t) {
+    View& v = t == 0 ? c.A : t == 1 ? c.B : c.C;
+    level(g[3], t, v.s_bo, v.s_bi);
+  }
+  c.alpha = alpha;
+  c.beta = beta;
+  launch(c);
+}
+}  // namespace
+
+void Schedule::ein(double alpha, const Ten& A, const Ten& B, double beta, const Ten& C, bool big) {
+  EinOps e;
+  const Ten* T[3] = {&A, &B, &C};
+  std::map<char, int> ids;
+  std::map<int, int64_t> ext;
+  for (int t = 0; t < 3; ++t) {
+    const Ten& x = *T[t];
+    if (x.labels.size() != x.dims.size())
+      throw Error(ERR_STATE, "ein: labels and extents differ in number");
+    e.p[t] = x.p;
+    int64_t stride = 1;
+    std::vector<EinAx> v(x.labels.size());
+    for (size_t k = x.labels.size(); k-- > 0;) {
+      const char c = x.labels[k];
+      auto it = ids.find(c);
+      const int id = it == ids.end() ? (ids[c] = static_cast<int>(ids.size())) : it->second;
+      auto et = ext.find(id);
+      if (et != ext.end() && et->second != x.dims[k])
+        throw Error(ERR_STATE, std::string("ein: extents of label ") + c + " differ");
+      ext[id] = x.dims[k];
+      v[k] = EinAx{id, x.dims[k], stride};
+      stride *= x.dims[k];
+    }
+    e.ax[t] = v;
+  }
+  for (int t = 0; t < 3; ++t)
+    for (size_t k = 0; k < e.ax[t].size(); ++k)
+      if (ein_find(e.ax[t], e.ax[t][k].id) != static_cast<int>(k))
+        throw Error(ERR_STATE, "ein: repeated label in one operand");
+  if (C.conj || (C.im != 0) != (A.im != 0 || B.im != 0))
+    throw Error(ERR_STATE, "ein: output must be complex exactly when an operand is");
+  int next_id = static_cast<int>(ids.size());
+  ein_run(e, next_id, alpha, beta, [&](const Contraction& c) {
+    zgemm(c, A.im, B.im, C.im, A.conj, B.conj, big);
+  });
 }
 
 // W[G][(a,i)] = sum_{b,j} Gamma^hp_Gjb M[(b,j),(a,i)] with M = 2X - X^x, X = T2 + T1 T1

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <array>
+#include <string>
 #include <vector>
 
 #include "ops.h"
@@ -163,6 +164,23 @@ class Schedule {
   // contractions; `big` routes them through tc_.
   void zgemm(Contraction c, int64_t a_im, int64_t b_im, int64_t c_im, bool conjA = false,
              bool conjB = false, bool big = false);
+  // A labelled operand of ein(): a dense row-major tensor whose indices are named
+  // by one character each, in memory order (last fastest), with their extents;
+  // `im` the element offset of the imaginary plane (0: real), `conj` conjugates it.
+  struct Ten {
+    double* p = nullptr;
+    std::string labels;
+    std::vector<int64_t> dims;
+    int64_t im = 0;
+    bool conj = false;
+  };
+  // C = alpha * A B + beta * C over labelled operands, like numpy's einsum with the
+  // summed labels those of A and B absent from C (every label in exactly two of the
+  // operands, or in all three as a batch label).  Labels that stay adjacent in
+  // every operand are fused; groups still wider than the contraction's two levels
+  // are looped over on the host.  One zgemm per launch (FP64, or tc_ when big).
+  void ein(double alpha, const Ten& A, const Ten& B, double beta, const Ten& C,
+           bool big = false);
   void profile_finish();
   int precision_ = 0;
   SplitScratch split_;

@@ -60,11 +60,12 @@ void Triples::coefficients(int64_t A, int64_t B, int64_t C, double coef[6]) {
 
 Triples::Triples(const RealSystem& sys, const ComplexSystem* cs, const TriplesOptions& opt,
                  Stream s)
-    : Schedule(s), sys_(sys), cplx_(cs != nullptr), reference_form_(opt.reference_form) {
+    : Schedule(s), sys_(sys), cs_(cs), cplx_(cs != nullptr), reference_form_(opt.reference_form),
+      complete_(opt.complete) {
   o_ = sys.o; v_ = sys.v; n1_ = o_ * v_;
   const int64_t o = o_, v = v_, n1 = n1_, G = sys.G;
   const int pl = cplx_ ? 2 : 1;
-  nb_ = opt.block > 0 ? std::min(opt.block, v) : auto_block(o, v, pl);
+  nb_ = opt.block > 0 ? std::min(opt.block, v) : auto_block(o, v, pl * (complete_ ? 2 : 1));
   const int64_t nbk = (v + nb_ - 1) / nb_;
   ntri_ = nbk * (nbk + 1) * (nbk + 2) / 6;
   const int64_t L = nb_ * o;
@@ -78,6 +79,11 @@ Triples::Triples(const RealSystem& sys, const ComplexSystem* cs, const TriplesOp
     Vppph_ = take(pl * v * n1 * v);
     Vhhhp_ = take(pl * o * n1 * o);
     S_ = take(pl * L * L * L);
+    if (complete_) {
+      Ip_ = take(pl * v * n1 * v);
+      Ih_ = take(pl * o * n1 * o);
+      Mb_ = take(pl * L * L * L);
+    }
     ws_ = take(2048);
     slots_ = take(2 * ntri_ + 2);
   } catch (...) {
@@ -129,7 +135,8 @@ void Triples::residual(const double*, double*) {
 // are the virtual and hole index at position q, the pair (x3, y3) is position r.
 // particle = true: the six d sums; false: the six l sums.
 void Triples::connected(const double* T2, const ops::TriplesBlock& b, const int64_t X[3],
-                        const int64_t n[3], bool particle) {
+                        const int64_t n[3], bool particle, const double* Vp, const double* Vh,
+                        double* S) {
   static const int PQR[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}};
   const int64_t o = o_, v = v_, n1 = n1_;
   const int64_t sP[3] = {b.L[1] * b.L[2], b.L[2], 1};
@@ -143,13 +150,13 @@ void Triples::connected(const double* T2, const ops::TriplesBlock& b, const int6
       if (p == 2) {  // pair p is the output's contiguous index: make it the inner row level
         c.Mi = b.L[p];
         c.A = vw(T + b.P[p] * n1, 1, n1, 0, o);
-        c.C = vw(S_, sP[q], sP[p], o * sP[q], sP[r]);
+        c.C = vw(S, sP[q], sP[p], o * sP[q], sP[r]);
       } else {
         c.Mi = o;
         c.A = vw(T + b.P[p] * n1, n1, 1, 0, o);
-        c.C = vw(S_, sP[p], sP[q], o * sP[q], sP[r]);
+        c.C = vw(S, sP[p], sP[q], o * sP[q], sP[r]);
       }
-      c.B = vw(Vppph_ + X[q] * n1 * v + b.P[r] * v, 0, 1, n1 * v, v);
+      c.B = vw(cp(Vp) + X[q] * n1 * v + b.P[r] * v, 0, 1, n1 * v, v);
       c.alpha = 1.0; c.beta = 1.0;
       zgemm(c, ti, vi_ppph_, si_, false, false, true);
     } else {  // - sum_l T[(x1,y1),(x2,l)] V[y2][(x3,y3)][l]   (conj(V) on the complex path)
@@ -158,25 +165,171 @@ void Triples::connected(const double* T2, const ops::TriplesBlock& b, const int6
       if (p == 2) {  // rows (virtual q, pair p) with pair p inner
         c.Mi = b.L[p];
         c.A = vw(T + b.P[p] * n1 + X[q] * o, o, n1, 0, 1);
-        c.C = vw(S_, o * sP[q], sP[p], 0, 0);
+        c.C = vw(S, o * sP[q], sP[p], 0, 0);
       } else {
         c.Mi = n[q];
         c.A = vw(T + b.P[p] * n1 + X[q] * o, n1, o, 0, 1);
-        c.C = vw(S_, sP[p], o * sP[q], 0, 0);
+        c.C = vw(S, sP[p], o * sP[q], 0, 0);
       }
       if (q == 2) {  // hole q is the output's contiguous index: columns (pair r, hole q)
         c.Ni = o;
-        c.B = vw(Vhhhp_ + b.P[r] * o, 0, 1, o, n1 * o);
+        c.B = vw(cp(Vh) + b.P[r] * o, 0, 1, o, n1 * o);
         c.C.s_co = sP[r]; c.C.s_ci = sP[q];
       } else {
         c.Ni = b.L[r];
-        c.B = vw(Vhhhp_ + b.P[r] * o, 0, 1, n1 * o, o);
+        c.B = vw(cp(Vh) + b.P[r] * o, 0, 1, n1 * o, o);
         c.C.s_co = sP[q]; c.C.s_ci = sP[r];
       }
       c.alpha = -1.0; c.beta = 1.0;
       zgemm(c, ti, vi_hhhp_, si_, false, cplx_, true);
     }
   }
+}
+
+void Triples::vslice(const char* name, const char* lab, double alpha, double beta, const Ten& C) {
+  // V_pqsr = sum_G L_Gps R_Gqr with L = Gamma^{LO LI} (real half-grid rows) or
+  // conj(Gamma^{LI LO})^T (complex), R = Gamma^{RO RI}: VertexCoulombIntegrals.cxx:55-197.
+  const int64_t o = o_, v = v_, G = sys_.G;
+  auto gam = [&](char X, char Y, char x, char y, bool conj) {
+    Ten t;
+    const bool px = X == 'p', py = Y == 'p';
+    const RealSystem& r = sys_;
+    double* base = px ? (py ? (cplx_ ? cs_->Gpp : r.Gpp) : (cplx_ ? cs_->Gph : r.Gph))
+                      : (py ? (cplx_ ? cs_->Ghp : r.Ghp) : (cplx_ ? cs_->Ghh : r.Ghh));
+    t.p = base;
+    t.labels = std::string("#") + x + y;
+    t.dims = {G, px ? v : o, py ? v : o};
+    t.im = cplx_ ? G * t.dims[1] * t.dims[2] : 0;
+    t.conj = conj;
+    return t;
+  };
+  const char LO = name[0], RO = name[1], LI = name[2], RI = name[3];
+  const Ten L = cplx_ ? gam(LI, LO, lab[2], lab[0], true) : gam(LO, LI, lab[0], lab[2], false);
+  const Ten R = gam(RO, RI, lab[1], lab[3], false);
+  ein(alpha, L, R, beta, C);
+}
+
+// ct::getCompleteTriples (CompleteTriples.cxx:11-118) on the device: every statement
+// of :51-114 as one labelled contraction (ein), the integral slices from the vertex.
+// Pair-layout amplitudes T_abij sit in memory as [a][i][b][j]; I_bcek is stored in
+// the layout of Vppph_ ([b][c][k][e]) and I_mcjk in that of Vhhhp_ ([j][c][k][m]),
+// so that the block contractions of V take them unchanged.
+void Triples::complete_intermediates(const double* T) {
+  const int64_t o = o_, v = v_, n1 = n1_;
+  const int64_t plane = n1 + n1 * n1;
+  const int pl = cplx_ ? 2 : 1;
+  auto ext = [&](char c) { return c == 'p' ? v : o; };
+  // A tensor named by the reference's labels `lab` of its type (e.g. "hhhp"), held in
+  // memory in the order `perm` of the reference positions.
+  struct Buf {
+    double* p;
+    std::string type, perm;
+    int64_t size;
+  };
+  auto buf = [&](const char* type, const char* perm = nullptr) {
+    Buf b;
+    b.type = type;
+    b.perm = perm ? perm : std::string("0123").substr(0, b.type.size());
+    b.size = 1;
+    for (char c : b.type) b.size *= ext(c);
+    b.p = nullptr;
+    return b;
+  };
+  auto R = [&](const Buf& b, const char* lab) {
+    Ten t;
+    t.p = b.p;
+    for (char k : b.perm) {
+      const int q = k - '0';
+      t.labels += lab[q];
+      t.dims.push_back(ext(b.type[q]));
+    }
+    t.im = cplx_ ? b.size : 0;
+    return t;
+  };
+  Buf t1 = buf("ph"), t2 = buf("pphh", "0213");
+  t1.p = cp(T);
+  t2.p = cp(T) + n1;
+  auto T1 = [&](const char* l) { Ten x = R(t1, l); x.im = cplx_ ? plane : 0; return x; };
+  auto T2 = [&](const char* l) { Ten x = R(t2, l); x.im = cplx_ ? plane : 0; return x; };
+  Buf Ip = buf("ppph", "0132"), Ih = buf("hphh", "2130");
+  Ip.p = Ip_;
+  Ih.p = Ih_;
+  Buf Vhhhp = buf("hhhp", "0312");  // Vhhhp_: V_jklc as [j][c][k][l]
+  Vhhhp.p = Vhhhp_;
+  Buf Vhp = buf("hhpp"), Xk = buf("hhhp"), Xa = buf("phpp"), I = buf("hp"), P1 = buf("hphp"),
+      P2 = buf("hpph"), Vhhph = buf("hhph"), Vhhhh = buf("hhhh"), Y = buf("ph");
+  Y.type = "#ph";  // Y_Gck = sum_f Gamma^pp_Gcf t_fk
+  Y.perm = "012";
+  Y.size = sys_.G * v * o;
+  for (Buf* b : {&Vhp, &Xk, &Xa, &I, &P1, &P2, &Vhhph, &Vhhhh, &Y}) b->p = take(pl * b->size);
+  auto RY = [&](const char* lab) {
+    Ten t;
+    t.p = Y.p; t.labels = lab; t.dims = {sys_.G, v, o}; t.im = cplx_ ? Y.size : 0;
+    return t;
+  };
+  vslice("hhpp", "ijab", 1.0, 0.0, R(Vhp, "ijab"));
+  // :53-55  Xijka = Vhhhp + T_fk Vhhpp_ijfa
+  vslice("hhhp", "ijka", 1.0, 0.0, R(Xk, "ijka"));
+  ein(1.0, T1("fk"), R(Vhp, "ijfa"), 1.0, R(Xk, "ijka"));
+  // :57-59  pXaibc = Vphpp - 1/2 T_al Vhhpp_libc
+  vslice("phpp", "aibc", 1.0, 0.0, R(Xa, "aibc"));
+  ein(-0.5, T1("al"), R(Vhp, "libc"), 1.0, R(Xa, "aibc"));
+  // :61-63  Iia = 2 Vhhpp_ilaf T_fl - Vhhpp_ilfa T_fl
+  ein(2.0, R(Vhp, "ilaf"), T1("fl"), 0.0, R(I, "ia"));
+  ein(-1.0, R(Vhp, "ilfa"), T1("fl"), 1.0, R(I, "ia"));
+  // :66-69  pXiajb = Vhphp - 1/2 Vhhhp_iljb T_al + T_fj pXaibc_aibf
+  vslice("hphp", "iajb", 1.0, 0.0, R(P1, "iajb"));
+  ein(-0.5, R(Vhhhp, "iljb"), T1("al"), 1.0, R(P1, "iajb"));
+  ein(1.0, T1("fj"), R(Xa, "aibf"), 1.0, R(P1, "iajb"));
+  // :71-74  pXiabj = Vhpph - 1/2 Vhhph_ilbj T_al + pXaibc_aifb T_fj
+  vslice("hhph", "ilbj", 1.0, 0.0, R(Vhhph, "ilbj"));
+  vslice("hpph", "iabj", 1.0, 0.0, R(P2, "iabj"));
+  ein(-0.5, R(Vhhph, "ilbj"), T1("al"), 1.0, R(P2, "iabj"));
+  ein(1.0, R(Xa, "aifb"), T1("fj"), 1.0, R(P2, "iabj"));
+  // :76-78  Xaibc = pXaibc - 1/2 T_al Vhhpp_libc
+  ein(-0.5, T1("al"), R(Vhp, "libc"), 1.0, R(Xa, "aibc"));
+  // :90-101  dpIbcek
+  copy_(Ip_, Vppph_, pl * v * n1 * v);
+  {  // V_bcef T_fk = sum_G L_Gbe Y_Gck without forming V_pppp
+    auto gpp = [&](const char* lab, bool conj) {
+      Ten g;
+      g.p = cplx_ ? cs_->Gpp : sys_.Gpp;
+      g.labels = lab;
+      g.dims = {sys_.G, v, v};
+      g.im = cplx_ ? sys_.G * v * v : 0;
+      g.conj = conj;
+      return g;
+    };
+    ein(1.0, gpp("#cf", false), T1("fk"), 0.0, RY("#ck"));
+    ein(1.0, cplx_ ? gpp("#eb", true) : gpp("#be", false), RY("#ck"), 1.0, R(Ip, "bcek"));
+  }
+  ein(-1.0, R(P1, "lbke"), T1("cl"), 1.0, R(Ip, "bcek"));
+  ein(-1.0, T1("bl"), R(P2, "lcek"), 1.0, R(Ip, "bcek"));
+  ein(-1.0, T2("bclk"), R(I, "le"), 1.0, R(Ip, "bcek"));
+  ein(2.0, R(Xa, "blef"), T2("cfkl"), 1.0, R(Ip, "bcek"));
+  ein(-1.0, R(Xa, "blef"), T2("fckl"), 1.0, R(Ip, "bcek"));
+  ein(-1.0, R(Xa, "blfe"), T2("fclk"), 1.0, R(Ip, "bcek"));
+  ein(-1.0, T2("fbkl"), R(Xa, "clfe"), 1.0, R(Ip, "bcek"));
+  ein(1.0, T2("cbln"), R(Xk, "lnke"), 1.0, R(Ip, "bcek"));
+  // :80-83  dpXiajb = Vhphp - Vhhhp_iljb T_al + 1/2 T_fj Xaibc_aibf
+  vslice("hphp", "iajb", 1.0, 0.0, R(P1, "iajb"));
+  ein(-1.0, R(Vhhhp, "iljb"), T1("al"), 1.0, R(P1, "iajb"));
+  ein(0.5, T1("fj"), R(Xa, "aibf"), 1.0, R(P1, "iajb"));
+  // :85-88  dpXiabj = Vhpph - Vhhph_ilbj T_al + 1/2 Xaibc_aifb T_fj
+  vslice("hpph", "iabj", 1.0, 0.0, R(P2, "iabj"));
+  ein(-1.0, R(Vhhph, "ilbj"), T1("al"), 1.0, R(P2, "iabj"));
+  ein(0.5, R(Xa, "aifb"), T1("fj"), 1.0, R(P2, "iabj"));
+  // :103-113  dpImcjk
+  vslice("hhhh", "mljk", 1.0, 0.0, R(Vhhhh, "mljk"));
+  vslice("hphh", "mcjk", 1.0, 0.0, R(Ih, "mcjk"));
+  ein(-1.0, R(Vhhhh, "mljk"), T1("cl"), 1.0, R(Ih, "mcjk"));
+  ein(1.0, R(P1, "mcjf"), T1("fk"), 1.0, R(Ih, "mcjk"));
+  ein(1.0, T1("fj"), R(P2, "mcfk"), 1.0, R(Ih, "mcjk"));
+  ein(2.0, R(Xk, "mljf"), T2("cfkl"), 1.0, R(Ih, "mcjk"));
+  ein(-1.0, R(Xk, "mljf"), T2("fckl"), 1.0, R(Ih, "mcjk"));
+  ein(-1.0, R(Xk, "lmjf"), T2("fclk"), 1.0, R(Ih, "mcjk"));
+  ein(-1.0, T2("cflj"), R(Xk, "lmkf"), 1.0, R(Ih, "mcjk"));
+  ein(1.0, T2("dfkj"), R(Xa, "cmdf"), 1.0, R(Ih, "mcjk"));
 }
 
 TriplesOutcome Triples::run(const double* T) {
@@ -195,6 +348,14 @@ TriplesOutcome Triples::run(const double* T) {
   out.flops = 2.0 * double(o) * o * o * double(v) * v * v * double(o + v);
   void* e0 = ops::event_create();
   void* e1 = ops::event_create();
+  if (complete_) {
+    ops::event_record(e0, s_);
+    complete_intermediates(T);
+    ops::event_record(e1, s_);
+    out.setup_seconds += ops::event_ms(e0, e1) * 1e-3;
+  }
+  const int64_t Lm = nb * o;
+  double* Mi = complete_ && cplx_ ? Mb_ + si_ : nullptr;
   // profile: events around the four phases of every block triple
   std::vector<void*> pev;
   if (profile_) {
@@ -214,18 +375,21 @@ TriplesOutcome Triples::run(const double* T) {
         for (int m = 0; m < 3; ++m) { b.P[m] = X[m] * o; b.L[m] = n[m] * o; }
         if (profile_) ops::event_record(pev[5 * t], s_);
         ops::triples_singles(S_, Si, t1, t1i, Vpphh_, Vi, b, s_);
+        if (complete_) zero_(Mb_, (cplx_ ? 2 : 1) * Lm * Lm * Lm);
         if (profile_) ops::event_record(pev[5 * t + 1], s_);
-        connected(T2, b, X, n, true);
+        connected(T2, b, X, n, true, Vppph_, Vhhhp_, S_);
+        if (complete_) connected(T2, b, X, n, true, Ip_, Ih_, Mb_);
         if (profile_) ops::event_record(pev[5 * t + 2], s_);
-        connected(T2, b, X, n, false);
+        connected(T2, b, X, n, false, Vppph_, Vhhhp_, S_);
+        if (complete_) connected(T2, b, X, n, false, Ip_, Ih_, Mb_);
         if (profile_) ops::event_record(pev[5 * t + 3], s_);
         double coef[6];
         coefficients(A, B, C, coef);
         ops::triples_energy(S_, Si, t1, t1i, Vpphh_, Vi, sys_.eh, sys_.ep, b, coef, ws_,
-                            slots_ + 2 * t, s_);
+                            slots_ + 2 * t, s_, complete_ ? Mb_ : nullptr, Mi);
         if (profile_) ops::event_record(pev[5 * t + 4], s_);
-        out.executed_flops += (cplx_ ? 4.0 : 1.0) * 12.0 * double(n[0] * n[1] * n[2]) * o * o * o *
-                              double(v + o);
+        out.executed_flops += (complete_ ? 2.0 : 1.0) * (cplx_ ? 4.0 : 1.0) * 12.0 *
+                              double(n[0] * n[1] * n[2]) * o * o * o * double(v + o);
       }
   ops::sum_partials_to(slots_ + 2 * ntri_, slots_, static_cast<int>(ntri_), 2, s_);
   ops::event_record(e1, s_);
@@ -240,8 +404,9 @@ TriplesOutcome Triples::run(const double* T) {
   ops::d2h(sums, slots_ + 2 * ntri_, 2, s_);
   ops::sync(s_);
   if (device_error()) throw Error(ERR_TIMEOUT, "tensor-core kernel wait expired in (T)");
-  // Re conj(W) Z = ReW ReZ + ImW ImZ;  Re conj(W) conj(Z) = ReW ReZ - ImW ImZ
-  out.energy = reference_form_ ? sums[0] - sums[1] : sums[0] + sums[1];
+  // Re conj(W) Z = ReW ReZ + ImW ImZ;  Re conj(W) conj(Z) = ReW ReZ - ImW ImZ;
+  // cT: Re M conj(Z) = ReM ReZ + ImM ImZ
+  out.energy = reference_form_ && !complete_ ? sums[0] - sums[1] : sums[0] + sums[1];
   return out;
 }
 

@@ -38,6 +38,11 @@ namespace cc4s_b200 {
 struct TriplesOptions {
   int64_t block = 0;            // virtual indices per block (0: automatic)
   bool reference_form = false;  // complex path: PerturbativeTriplesReference's conjugation
+  // The cT branch of PerturbativeTriplesReference (:92-109, :178-179): the
+  // completely renormalised intermediates I_bcek, I_mcjk of ct::getCompleteTriples
+  // (CompleteTriples.cxx:11-118) in place of V_bcek and V_jkmc in a second block
+  // array M, and E = sum M (4/3 S - 2 S_acb + 2/3 S_bca)^* / D.
+  bool complete = false;
 };
 
 struct TriplesOutcome {
@@ -65,7 +70,7 @@ class Triples : public Schedule {
   const double* Vd() const override { return Vpphh_; }
   const double* Ve() const override { return nullptr; }
 
-  // Block length whose block array planes * (block * o)^3 fits the L2-sized budget.
+  // Block length whose block arrays (arrays * planes * (block * o)^3) fit the L2-sized budget.
   static int64_t auto_block(int64_t o, int64_t v, int planes);
   // Weights of the six hole permutations (012, 021, 102, 120, 201, 210) for the
   // block triple (A, B, C), A <= B <= C: every distinct ordering sigma of the
@@ -74,16 +79,28 @@ class Triples : public Schedule {
   static void coefficients(int64_t A, int64_t B, int64_t C, double coef[6]);
 
  private:
+  // S += the six permutations of X = sum_d T V^p - sum_l T V^h (particle or hole
+  // half), V^p in the layout of Vppph_, V^h in the layout of Vhhhp_.
   void connected(const double* T2, const ops::TriplesBlock& b, const int64_t X[3],
-                 const int64_t n[3], bool particle);
+                 const int64_t n[3], bool particle, const double* Vp, const double* Vh,
+                 double* S);
+  // I_bcek into Ip_ and I_mcjk into Ih_ at amplitudes T (cT branch).
+  void complete_intermediates(const double* T);
+  // beta C + alpha V_pqsr for the integral slice `name` (LO RO LI RI), C labelled
+  // by lab = the characters of p, q, s, r.
+  void vslice(const char* name, const char* lab, double alpha, double beta, const Ten& C);
   RealSystem sys_;
-  bool cplx_ = false, reference_form_ = false;
+  const ComplexSystem* cs_ = nullptr;
+  bool cplx_ = false, reference_form_ = false, complete_ = false;
   int64_t o_ = 0, v_ = 0, n1_ = 0, nb_ = 0;
   int64_t vi_pphh_ = 0, vi_ppph_ = 0, vi_hhhp_ = 0, si_ = 0;  // imaginary-plane offsets
   double* Vpphh_ = nullptr;  // V_abij, pair layout [(a,i)][(b,j)]
   double* Vppph_ = nullptr;  // V_bcdk as [b][(c,k)][d]
   double* Vhhhp_ = nullptr;  // V_jklc as [j][(c,k)][l]
   double* S_ = nullptr;      // block array (imaginary plane at S_ + si_)
+  double* Ip_ = nullptr;     // cT: I_bcdk in the layout of Vppph_
+  double* Ih_ = nullptr;     // cT: I_lcjk as [j][(c,k)][l], the layout of Vhhhp_
+  double* Mb_ = nullptr;     // cT: block array of M (layout of S_)
   double* ws_ = nullptr;     // reduction partials
   double* slots_ = nullptr;  // two energy sums of every block triple, then their totals
   int64_t ntri_ = 0;

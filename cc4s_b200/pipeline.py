@@ -142,6 +142,7 @@ def run_steps(steps, workdir=".", lib=None, symbols=None):
                 "precision": a.get("precision", "fp64"),
                 "blockSize": a.get("blockSize", 0),
                 "referenceForm": name == "PerturbativeTriplesReference",
+                "cT": int(a.get("cT", 0) or 0) if name == "PerturbativeTriplesReference" else 0,
                 "mp2PairEnergies": getattr(pairs, "values", pairs)})
             sym[out.get("energy", name + "Energy")] = res["energy"]
         elif name == "FiniteSizeCorrection":

@@ -206,12 +206,17 @@ typedef struct {
   int formulation;      /* complex path: 0 = PerturbativeTriples (atrip, Equations.hpp
                            getEnergyDistinct: Re conj(W) Z), 1 = PerturbativeTriplesReference
                            (PerturbativeTriplesReference.cxx:136-173: Re conj(W) conj(Z));
-                           the same on the real path */
+                           the same on the real path; ignored when cT = 1 */
+  int cT;               /* "cT" of PerturbativeTriplesReference (:70-71, :92-109, :178-179):
+                           1 = completely renormalised triples, E = sum M Z with M built
+                           from the intermediates of ct::getCompleteTriples
+                           (CompleteTriples.cxx:11-118) in place of V_bcdk, V_jklc */
 } cc4s_cc_triples_options;
 typedef struct {
   double correlation;     /* energy.correlation of the step */
   double seconds;         /* device time of the block loop */
-  double setup_seconds;   /* device time of the integral slices pphh, ppph, hhhp */
+  double setup_seconds;   /* device time of the integral slices pphh, ppph, hhhp (and of
+                             the cT intermediates) */
   double flops;           /* 2 No^3 Nv^3 (No + Nv), the reference's count
                              (PerturbativeTriples.cxx, atripDryRun) */
   double executed_flops;  /* flops of the contractions launched (whole block triples) */
@@ -231,7 +236,7 @@ void cc4s_cc_triples_default_options(cc4s_cc_triples_options* opt);
  *   - name: PerturbativeTriples           (src/main/algorithms/PerturbativeTriples.cxx:27-255,
  *                                           the atrip tuple loop)
  *   - name: PerturbativeTriplesReference  (src/main/algorithms/PerturbativeTriplesReference.cxx:56-222,
- *                                           cT = 0)
+ *                                           cT = 0 or 1)
  *     in:  {amplitudes, coulombIntegrals, slicedEigenEnergies}
  *     out: {energy: {correlation, unit}}
  * The integral slices pphh, ppph and hhhp are formed on the device from the

@@ -5,8 +5,9 @@ Test infrastructure (see ``oracle/__init__.py``): the checker of the device
 
 Two restatements of the same energy, used against each other:
 
-* ``triples_reference`` follows ``PerturbativeTriplesReference::run`` (the
-  non-cT branch, src/main/algorithms/PerturbativeTriplesReference.cxx:107-175)
+* ``triples_reference`` follows ``PerturbativeTriplesReference::run``
+  (src/main/algorithms/PerturbativeTriplesReference.cxx:92-179, both branches;
+  the cT branch with ``complete_triples_intermediates``, CompleteTriples.cxx:11-118)
   statement by statement on full [a,b,c,i,j,k] arrays (small systems only);
 * ``triples_atrip`` follows the tuple loop of the distributed implementation
   that ``PerturbativeTriples`` runs (perturbative-triples/src/atrip/Atrip.cxx:
@@ -36,8 +37,57 @@ def triples_integrals(sys: System):
     return coulomb_integrals(sys, ["pphh", "ppph", "hhhp"])
 
 
-def triples_reference(T1, T2, V, eps_h, eps_p):
-    """PerturbativeTriplesReference.cxx:107-175 (cT = 0); returns the real part of E."""
+COMPLETE_TRIPLES_SLICES = ["pppp", "phph", "hhhh", "hhhp", "ppph", "hhpp", "pphp", "phhh",
+                           "hphp", "phhp", "phpp", "hhph", "hppp", "hpph", "hphh"]
+
+
+def complete_triples_intermediates(sys: System, T1, T2):
+    """ct::getCompleteTriples (src/main/algorithms/CompleteTriples.cxx:11-118): the
+    doubly primed intermediates I_bcek ("ppph") and I_mcjk ("hphh") of the cT
+    branch, statement by statement on full arrays (small systems only)."""
+    V = coulomb_integrals(sys, COMPLETE_TRIPLES_SLICES)
+    t, T = T1, T2
+    # :53-55  Xijka = Vhhhp + T_fk Vhhpp_ijfa
+    Xijka = V["hhhp"] + es("fk,ijfa->ijka", t, V["hhpp"])
+    # :57-59  pXaibc = Vphpp - 1/2 T_al Vhhpp_libc
+    pXaibc = V["phpp"] - 0.5 * es("al,libc->aibc", t, V["hhpp"])
+    # :61-63  Iia = 2 Vhhpp_ilaf T_fl - Vhhpp_ilfa T_fl
+    Iia = 2.0 * es("ilaf,fl->ia", V["hhpp"], t) - es("ilfa,fl->ia", V["hhpp"], t)
+    # :66-69  pXiajb = Vhphp - 1/2 Vhhhp_iljb T_al + T_fj pXaibc_aibf
+    pXiajb = (V["hphp"] - 0.5 * es("iljb,al->iajb", V["hhhp"], t)
+              + es("fj,aibf->iajb", t, pXaibc))
+    # :71-74  pXiabj = Vhpph - 1/2 Vhhph_ilbj T_al + pXaibc_aifb T_fj
+    pXiabj = (V["hpph"] - 0.5 * es("ilbj,al->iabj", V["hhph"], t)
+              + es("aifb,fj->iabj", pXaibc, t))
+    # :76-78  Xaibc = pXaibc - 1/2 T_al Vhhpp_libc
+    Xaibc = pXaibc - 0.5 * es("al,libc->aibc", t, V["hhpp"])
+    # :80-83  dpXiajb = Vhphp - Vhhhp_iljb T_al + 1/2 T_fj Xaibc_aibf
+    dpXiajb = (V["hphp"] - es("iljb,al->iajb", V["hhhp"], t)
+               + 0.5 * es("fj,aibf->iajb", t, Xaibc))
+    # :85-88  dpXiabj = Vhpph - Vhhph_ilbj T_al + 1/2 Xaibc_aifb T_fj
+    dpXiabj = (V["hpph"] - es("ilbj,al->iabj", V["hhph"], t)
+               + 0.5 * es("aifb,fj->iabj", Xaibc, t))
+    # :90-101  dpIbcek
+    dpI = (V["ppph"] + es("bcef,fk->bcek", V["pppp"], t)
+           - es("lbke,cl->bcek", pXiajb, t) - es("bl,lcek->bcek", t, pXiabj)
+           - es("le,bclk->bcek", Iia, T)
+           + 2.0 * es("blef,cfkl->bcek", Xaibc, T) - es("blef,fckl->bcek", Xaibc, T)
+           - es("blfe,fclk->bcek", Xaibc, T) - es("fbkl,clfe->bcek", T, Xaibc)
+           + es("cbln,lnke->bcek", T, Xijka))
+    # :103-113  dpImcjk
+    dpM = (V["hphh"] - es("mljk,cl->mcjk", V["hhhh"], t)
+           + es("mcjf,fk->mcjk", dpXiajb, t) + es("fj,mcfk->mcjk", t, dpXiabj)
+           + 2.0 * es("mljf,cfkl->mcjk", Xijka, T) - es("mljf,fckl->mcjk", Xijka, T)
+           - es("lmjf,fclk->mcjk", Xijka, T) - es("cflj,lmkf->mcjk", T, Xijka)
+           + es("dfkj,cmdf->mcjk", T, Xaibc))
+    return {"ppph": dpI, "hphh": dpM}
+
+
+def triples_reference(T1, T2, V, eps_h, eps_p, complete=None):
+    """PerturbativeTriplesReference.cxx:107-175; returns the real part of E.
+    complete: the intermediates of complete_triples_intermediates for the cT branch
+    (:92-109, :178-179): M = I_bcdk T_adij - conj(I_lcjk) T_abil summed over the six
+    simultaneous permutations, and E = sum M Z instead of sum T Z D."""
     Vpphh, Vppph, Vhhhp = V["pphh"], V["ppph"], V["hhhp"]
     cplx = np.iscomplexobj(T2) or np.iscomplexobj(Vppph)
     cj = np.conj if cplx else (lambda x: x)
@@ -60,8 +110,15 @@ def triples_reference(T1, T2, V, eps_h, eps_p):
          + eh[None, None, None, None, None, :] - ep[:, None, None, None, None, None]
          - ep[None, :, None, None, None, None] - ep[None, None, :, None, None, None])
     # :136-140  Z <- conj(Z) / D, T <- conj(T) / D;  :173  E = T Z D
-    E = np.sum(cj(W) / D * cj(Zs) / D * D)
-    return float(np.real(E))
+    if complete is None:
+        E = np.sum(cj(W) / D * cj(Zs) / D * D)
+        return float(np.real(E))
+    # cT (:94-109): M from the intermediates, symmetrised like W;  :178-179  E = M Z
+    M = es("bcdk,adij->abcijk", complete["ppph"], T2)
+    M = M - es("lcjk,abil->abcijk", cj(complete["hphh"]), T2)
+    M = (M + es("bacjik->abcijk", M) + es("acbikj->abcijk", M) + es("cbakji->abcijk", M)
+         + es("cabkij->abcijk", M) + es("bcajki->abcijk", M))
+    return float(np.real(np.sum(M * cj(Zs) / D)))
 
 
 def _atrip_doubles(a, b, c, T2, Vppph, Vhhhp, cplx):

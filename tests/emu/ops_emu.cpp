@@ -660,7 +660,8 @@ void triples_singles(double* S, double* S_im, const double* t1, const double* t1
 
 void triples_energy(const double* S, const double* S_im, const double* t1, const double* t1_im,
                     const double* V, const double* V_im, const double* eh, const double* ep,
-                    const TriplesBlock& b, const double coef[6], double*, double* out, Stream) {
+                    const TriplesBlock& b, const double coef[6], double*, double* out, Stream,
+                    const double* M, const double* M_im) {
   ++g_ops;
   static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
   const int64_t o = b.o;
@@ -684,8 +685,9 @@ void triples_energy(const double* S, const double* S_im, const double* t1, const
           yr += coef[k] * at(S, r1, r2, r3);
           if (S_im) yi += coef[k] * at(S_im, r1, r2, r3);
         }
-        acc[0] += (at(S, q1, q2, q3) - sg.re) * yr / d;
-        if (S_im) acc[1] += (at(S_im, q1, q2, q3) - sg.im) * yi / d;
+        const double wr = M ? at(M, q1, q2, q3) : at(S, q1, q2, q3) - sg.re;
+        acc[0] += wr * yr / d;
+        if (S_im) acc[1] += (M ? at(M_im, q1, q2, q3) : at(S_im, q1, q2, q3) - sg.im) * yi / d;
       }
   out[0] = acc[0];
   out[1] = acc[1];

@@ -189,3 +189,71 @@ def test_triples_star_correction(emu_lib, cplx):
     assert abs(r["energy"]["starCorrection"] - star) < 1e-12 * abs(star)
     from oracle import properties
     assert abs(e_mp2 - properties.mp2(s)[0]) < 1e-12 * abs(e_mp2)
+
+
+def _amplitudes(rng, Nv, No, cplx):
+    T1, T2 = _rand_T(rng, Nv, No)
+    if cplx:
+        U1, U2 = _rand_T(rng, Nv, No)
+        T1, T2 = T1 + 1j * U1, T2 + 1j * U2
+    return T1, T2
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("shape,block", [((3, 8, 14), 0), ((2, 7, 9), 3), ((3, 10, 16), 4),
+                                         ((1, 5, 7), 2)])
+def test_triples_complete_matches_oracle(emu_lib, cplx, shape, block):
+    """cT = 1 (PerturbativeTriplesReference.cxx:92-109, :178-179): the intermediates of
+    ct::getCompleteTriples formed on the device from the vertex (every statement of
+    CompleteTriples.cxx:51-114 as a labelled contraction) and E = sum M Z, against the
+    oracle's statement-by-statement restatement on full arrays."""
+    from cc4s_b200.coupled_cluster import Solver
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, complex=cplx, seed=No + Nv)
+    T1, T2 = _amplitudes(np.random.default_rng(NG), Nv, No, cplx)
+    J = triples.complete_triples_intermediates(s, T1, T2)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p,
+                                    complete=J)
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+        sol.set_initial_amplitudes(T1, T2)
+        r = sol.perturbative_triples(block, reference_form=True, cT=True)
+        plain = sol.perturbative_triples(block, reference_form=True)["correlation"]
+    finally:
+        sol.close()
+    assert abs(r["correlation"] - ref) < 1e-12 * max(1.0, abs(ref)), (r["correlation"], ref)
+    assert abs(r["correlation"] - plain) > 1e-8 * abs(plain)  # the branches differ here
+    # the M contractions double the executed flops of the block loop
+    assert r["executed_flops"] >= 2 * r["flops"] * (1 - 1e-12)
+
+
+def test_triples_complete_rejects_invalid_flag(emu_lib):
+    import ctypes
+    from cc4s_b200 import _abi
+    from cc4s_b200.coupled_cluster import Solver
+    s = inputs.synthetic_system(2, 5, 8, seed=1)
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+        sol.set_initial_amplitudes(*_rand_T(np.random.default_rng(0), 5, 2))
+        o = _abi.TriplesOptions()
+        sol.lib.cc4s_cc_triples_default_options(ctypes.byref(o))
+        assert o.cT == 0
+        o.cT = 2
+        r = _abi.TriplesResult()
+        st = sol.lib.cc4s_cc_perturbative_triples(sol.h, ctypes.byref(o), ctypes.byref(r))
+        assert st == _abi.ERR_INVALID_ARGUMENT
+    finally:
+        sol.close()
+
+
+def test_complete_intermediates_reduce_to_integrals_at_zero_amplitudes():
+    """Oracle check: at T = 0 every correction term of CompleteTriples.cxx:90-113
+    vanishes, I_bcek = V_bcek and I_mcjk = V_mcjk; and the cT energy then equals
+    the plain energy with W in place of M (both vanish with T)."""
+    s = inputs.synthetic_system(2, 5, 8, seed=3)
+    z1, z2 = np.zeros((5, 2)), np.zeros((5, 5, 2, 2))
+    J = triples.complete_triples_intermediates(s, z1, z2)
+    V = inputs.coulomb_integrals(s, ["ppph", "hphh"])
+    assert np.array_equal(J["ppph"], V["ppph"]) and np.array_equal(J["hphh"], V["hphh"])

@@ -169,3 +169,31 @@ def test_triples_star_correction_on_device(cplx):
     star, e_mp2 = triples.triples_star(V, s.eps_h, s.eps_p, pairs, r["energy"]["correlation"])
     assert abs(r["stats"]["mp2_energy"] - e_mp2) < TOL_FP64 * abs(e_mp2)
     assert abs(r["energy"]["starCorrection"] - star) < TOL_FP64 * abs(star)
+
+
+@pytest.mark.parametrize("cplx,block,precision", [(False, 0, "fp64"), (False, 4, "fp64"),
+                                                  (True, 3, "fp64"), (False, 4, "split3")])
+def test_triples_complete_matches_oracle(cplx, block, precision):
+    """cT = 1 on the B200: the ct::getCompleteTriples intermediates (CompleteTriples.cxx:
+    11-118) formed on the device, the second block array M and E = sum M Z
+    (PerturbativeTriplesReference.cxx:92-109, :178-179), against the oracle."""
+    from cc4s_b200 import Solver
+    No, Nv = 4, 20
+    s = inputs.synthetic_system(No, Nv, 40, complex=cplx, seed=6)
+    rng = np.random.default_rng(3)
+    T1, T2 = _rand_T(rng, Nv, No)
+    if cplx:
+        U1, U2 = _rand_T(rng, Nv, No)
+        T1, T2 = T1 + 1j * U1, T2 + 1j * U2
+    J = triples.complete_triples_intermediates(s, T1, T2)
+    ref = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p,
+                                    complete=J)
+    sol = Solver({"precision": precision})
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+        sol.set_initial_amplitudes(T1, T2)
+        e = sol.perturbative_triples(block, reference_form=True, cT=True)["correlation"]
+    finally:
+        sol.close()
+    tol = TOL_FP64 if precision == "fp64" else TOL_SPLIT
+    assert abs(e - ref) < tol * abs(ref), (e, ref)

@@ -245,3 +245,29 @@ def test_input_chain_complex_triples_step_names(tmp_path, emu_lib, step):
     f = triples.triples_reference if step.endswith("Reference") else triples.triples_atrip
     e = f(T1, T2, V, s.eps_h, s.eps_p)
     assert abs(sym["TriplesEnergy"]["correlation"] - e) < 1e-11 * max(1.0, abs(e))
+
+
+@pytest.mark.parametrize("half_grid", [True, False])
+def test_input_chain_triples_reference_with_cT(tmp_path, emu_lib, half_grid):
+    """The (T) step of test/tests/hf/cc4s.in:49-56: PerturbativeTriplesReference with
+    cT: 1 after the CCSD step; the energy is the completely renormalised one
+    (CompleteTriples.cxx:11-118), against the oracle on the chain's amplitudes."""
+    import yaml
+    from cc4s_b200 import pipeline
+    from oracle import triples
+    s = inputs.synthetic_system(2, 6, 12, complex=not half_grid, seed=5)
+    _write_system(tmp_path, s, half_grid, True)
+    steps = STEPS[:-1] + [
+        {"name": "PerturbativeTriplesReference",
+         "in": {"coulombIntegrals": "CoulombIntegrals", "cT": 1, "amplitudes": "Amplitudes",
+                "slicedEigenEnergies": "EigenEnergies"},
+         "out": {"energy": "TriplesEnergy"}}]
+    with open(tmp_path / "cc4s.in", "w") as f:
+        yaml.safe_dump(steps, f, sort_keys=False)
+    sym = pipeline.run_file(str(tmp_path / "cc4s.in"), lib=emu_lib)
+    T1 = sym["Amplitudes"]["ph"].values
+    T2 = sym["Amplitudes"]["pphh"].values
+    J = triples.complete_triples_intermediates(s, T1, T2)
+    e = triples.triples_reference(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p,
+                                  complete=J)
+    assert abs(sym["TriplesEnergy"]["correlation"] - e) < 1e-11 * max(1.0, abs(e))
