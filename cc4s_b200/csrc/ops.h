@@ -33,6 +33,10 @@ void event_destroy(void* e);
 // destination axis k is source axis perm[k].
 void permute4(double* dst, const double* src, const int64_t d[4], const int perm[4],
               double alpha, double beta, Stream s);
+// Strided 4-index copy: dst[i] = alpha * src[i] + beta * dst[i] over the extents e,
+// element i at sum_k i_k ss[k] in src and sum_k i_k ds[k] in dst (ds[3] == 1).
+void copy4(double* dst, const int64_t ds[4], const double* src, const int64_t ss[4],
+           const int64_t e[4], double alpha, double beta, Stream s);
 // out = a*x + b*y + c*out   (y may be null; c == 0 does not read out)
 void axpby(double* out, double a, const double* x, double b, const double* y, double c,
            int64_t n, Stream s);

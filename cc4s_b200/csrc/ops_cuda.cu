@@ -63,7 +63,7 @@ __global__ void permute_rows_kernel(double* dst, const double* src, Perm4 p, dou
     const int64_t i1 = (r / p.e[2]) % p.e[1];
     const int64_t i0 = r / (p.e[2] * p.e[1]);
     const double* s = src + i0 * p.ss[0] + i1 * p.ss[1] + i2 * p.ss[2];
-    double* d = dst + r * p.e[3];
+    double* d = dst + i0 * p.ds[0] + i1 * p.ds[1] + i2 * p.ds[2];
     for (int64_t x = threadIdx.x; x < p.e[3]; x += blockDim.x) {
       const double v = alpha * s[x];
       d[x] = (beta != 0.0) ? v + beta * d[x] : v;
@@ -683,6 +683,32 @@ void permute4(double* dst, const double* src, const int64_t d[4], const int perm
     for (int k = 0; k < 3; ++k)
       if (k != q) b[nb++] = k;
     const int64_t tiles = ((p.e[3] + 31) / 32) * ((p.e[q] + 31) / 32) * p.e[b[0]] * p.e[b[1]];
+    permute_tiled_kernel<<<grid_for(tiles, 1, 148 * 64), dim3(32, 8), 0, s>>>(
+        dst, src, p, q, b[0], b[1], alpha, beta);
+  }
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void copy4(double* dst, const int64_t ds[4], const double* src, const int64_t ss[4],
+           const int64_t e[4], double alpha, double beta, Stream s) {
+  if (ds[3] != 1) throw Error(ERR_STATE, "copy4: the destination's inner stride must be 1");
+  Perm4 p;
+  for (int k = 0; k < 4; ++k) { p.e[k] = e[k]; p.ss[k] = ss[k]; p.ds[k] = ds[k]; }
+  const int64_t total = e[0] * e[1] * e[2] * e[3];
+  if (total == 0) return;
+  if (ss[3] == 1) {
+    const int64_t rows = e[0] * e[1] * e[2];
+    int threads = e[3] >= 256 ? 256 : (e[3] >= 128 ? 128 : (e[3] >= 64 ? 64 : 32));
+    permute_rows_kernel<<<grid_for(rows, 1, 148 * 64), threads, 0, s>>>(dst, src, p, alpha, beta);
+  } else {
+    int q = 0;  // the destination axis with the smallest source stride
+    for (int k = 1; k < 3; ++k)
+      if (ss[k] < ss[q]) q = k;
+    int b[2], nb = 0;
+    for (int k = 0; k < 3; ++k)
+      if (k != q) b[nb++] = k;
+    const int64_t tiles = ((e[3] + 31) / 32) * ((e[q] + 31) / 32) * e[b[0]] * e[b[1]];
     permute_tiled_kernel<<<grid_for(tiles, 1, 148 * 64), dim3(32, 8), 0, s>>>(
         dst, src, p, q, b[0], b[1], alpha, beta);
   }

@@ -79,10 +79,17 @@ Triples::Triples(const RealSystem& sys, const ComplexSystem* cs, const TriplesOp
     Vppph_ = take(pl * v * n1 * v);
     Vhhhp_ = take(pl * o * n1 * o);
     S_ = take(pl * L * L * L);
+    kc_ = v + o;
+    ai_ = cplx_ ? n1 * o * kc_ : 0;
+    bi_ = cplx_ ? v * n1 * kc_ : 0;
+    Ac_ = take(pl * n1 * o * kc_);
+    Bc_ = take(pl * v * n1 * kc_);
     if (complete_) {
       Ip_ = take(pl * v * n1 * v);
       Ih_ = take(pl * o * n1 * o);
       Mb_ = take(pl * L * L * L);
+      AcM_ = take(pl * n1 * o * kc_);
+      BcM_ = take(pl * v * n1 * kc_);
     }
     ws_ = take(2048);
     slots_ = take(2 * ntri_ + 2);
@@ -130,58 +137,64 @@ void Triples::residual(const double*, double*) {
   throw Error(ERR_STATE, "the triples schedule has no residual");
 }
 
-// S += the six permutations of the base term X for one block triple.  Term
-// (p, q, r): the pair (x1, y1) of X is the pair at block position p, x2 and y2
-// are the virtual and hole index at position q, the pair (x3, y3) is position r.
-// particle = true: the six d sums; false: the six l sums.
-void Triples::connected(const double* T2, const ops::TriplesBlock& b, const int64_t X[3],
-                        const int64_t n[3], bool particle, const double* Vp, const double* Vh,
-                        double* S) {
+// S += the six permutations of the base term X for one block triple, the particle
+// and the hole half of each in one contraction over K = v + o.  Term (p, q, r): the
+// pair (x1, y1) of X is the pair at block position p, x2 and y2 are the virtual and
+// hole index at position q, the pair (x3, y3) is position r.  Its particle half
+//   + sum_d T[(x1,y1),(d,y2)] V^p[x2][(x3,y3)][d]
+// has rows (pair p, hole q) and columns (virtual q, pair r); the hole half of the
+// term (r, q, p),
+//   - sum_l T[(x3,y3),(x2,l)] V^h[y2][(x1,y1)][l]   (conj(V^h) on the complex path),
+// writes the same elements of S with the same rows and columns (its transpose), so
+// rows of Ac hold [T | -V^h] and columns of Bc hold [V^p | T] along K.
+void Triples::connected(const ops::TriplesBlock& b, const int64_t X[3], const int64_t n[3],
+                        const double* Ac, const double* Bc, double* S) {
   static const int PQR[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}};
-  const int64_t o = o_, v = v_, n1 = n1_;
+  const int64_t o = o_, n1 = n1_, kc = kc_;
   const int64_t sP[3] = {b.L[1] * b.L[2], b.L[2], 1};
-  const int64_t ti = cplx_ ? n1 + n1 * n1 : 0;  // imaginary plane of the amplitude vector
-  double* T = cp(T2);
   for (const auto& t : PQR) {
     const int p = t[0], q = t[1], r = t[2];
-    if (particle) {  // + sum_d T[(x1,y1),(d,y2)] V[x2][(x3,y3)][d]
-      Contraction c;
-      c.M = b.L[p] * o; c.N = n[q] * b.L[r]; c.Ni = b.L[r]; c.K = v;
-      if (p == 2) {  // pair p is the output's contiguous index: make it the inner row level
-        c.Mi = b.L[p];
-        c.A = vw(T + b.P[p] * n1, 1, n1, 0, o);
-        c.C = vw(S, sP[q], sP[p], o * sP[q], sP[r]);
-      } else {
-        c.Mi = o;
-        c.A = vw(T + b.P[p] * n1, n1, 1, 0, o);
-        c.C = vw(S, sP[p], sP[q], o * sP[q], sP[r]);
-      }
-      c.B = vw(cp(Vp) + X[q] * n1 * v + b.P[r] * v, 0, 1, n1 * v, v);
-      c.alpha = 1.0; c.beta = 1.0;
-      zgemm(c, ti, vi_ppph_, si_, false, false, true);
-    } else {  // - sum_l T[(x1,y1),(x2,l)] V[y2][(x3,y3)][l]   (conj(V) on the complex path)
-      Contraction c;
-      c.M = b.L[p] * n[q]; c.N = o * b.L[r]; c.K = o;
-      if (p == 2) {  // rows (virtual q, pair p) with pair p inner
-        c.Mi = b.L[p];
-        c.A = vw(T + b.P[p] * n1 + X[q] * o, o, n1, 0, 1);
-        c.C = vw(S, o * sP[q], sP[p], 0, 0);
-      } else {
-        c.Mi = n[q];
-        c.A = vw(T + b.P[p] * n1 + X[q] * o, n1, o, 0, 1);
-        c.C = vw(S, sP[p], o * sP[q], 0, 0);
-      }
-      if (q == 2) {  // hole q is the output's contiguous index: columns (pair r, hole q)
-        c.Ni = o;
-        c.B = vw(cp(Vh) + b.P[r] * o, 0, 1, o, n1 * o);
-        c.C.s_co = sP[r]; c.C.s_ci = sP[q];
-      } else {
-        c.Ni = b.L[r];
-        c.B = vw(cp(Vh) + b.P[r] * o, 0, 1, n1 * o, o);
-        c.C.s_co = sP[q]; c.C.s_ci = sP[r];
-      }
-      c.alpha = -1.0; c.beta = 1.0;
-      zgemm(c, ti, vi_hhhp_, si_, false, cplx_, true);
+    Contraction c;
+    c.M = b.L[p] * o; c.N = n[q] * b.L[r]; c.Ni = b.L[r]; c.K = kc;
+    double* A0 = cp(Ac) + b.P[p] * o * kc;
+    if (p == 2) {  // pair p is the output's contiguous index: make it the inner row level
+      c.Mi = b.L[p];
+      c.A = vw(A0, kc, o * kc, 0, 1);
+      c.C = vw(S, sP[q], sP[p], o * sP[q], sP[r]);
+    } else {
+      c.Mi = o;
+      c.A = vw(A0, o * kc, kc, 0, 1);
+      c.C = vw(S, sP[p], sP[q], o * sP[q], sP[r]);
+    }
+    c.B = vw(cp(Bc) + (X[q] * n1 + b.P[r]) * kc, 0, 1, n1 * kc, kc);
+    c.alpha = 1.0; c.beta = 1.0;
+    zgemm(c, ai_, bi_, si_, false, false, true);
+  }
+}
+
+void Triples::concat_operands(const double* T, const double* Vp, const double* Vh, double* Ac,
+                              double* Bc) {
+  const int64_t o = o_, v = v_, n1 = n1_, kc = kc_;
+  const int64_t plane = n1 + n1 * n1;
+  for (int pl = 0; pl < (cplx_ ? 2 : 1); ++pl) {
+    const double* T2 = T + pl * plane + n1;
+    double* A = Ac + pl * ai_;
+    double* B = Bc + pl * bi_;
+    {  // Ac[P][y][d] = T2[P][(d, y)]
+      const int64_t e[4] = {1, n1, o, v}, ds[4] = {0, o * kc, kc, 1}, ss[4] = {0, n1, 1, o};
+      ops::copy4(A, ds, T2, ss, e, 1.0, 0.0, s_);
+    }
+    {  // Ac[P][y][v + l] = -conj(V^h[y][P][l])
+      const int64_t e[4] = {1, n1, o, o}, ds[4] = {0, o * kc, kc, 1}, ss[4] = {0, o, n1 * o, 1};
+      ops::copy4(A + v, ds, Vh + pl * vi_hhhp_, ss, e, pl == 0 ? -1.0 : 1.0, 0.0, s_);
+    }
+    {  // Bc[x][P][d] = V^p[x][P][d]
+      const int64_t e[4] = {1, v, n1, v}, ds[4] = {0, n1 * kc, kc, 1}, ss[4] = {0, n1 * v, v, 1};
+      ops::copy4(B, ds, Vp + pl * vi_ppph_, ss, e, 1.0, 0.0, s_);
+    }
+    {  // Bc[x][P][v + l] = T2[P][(x, l)]
+      const int64_t e[4] = {1, v, n1, o}, ds[4] = {0, n1 * kc, kc, 1}, ss[4] = {0, o, n1, 1};
+      ops::copy4(B + v, ds, T2, ss, e, 1.0, 0.0, s_);
     }
   }
 }
@@ -338,7 +351,6 @@ TriplesOutcome Triples::run(const double* T) {
   const int64_t plane = n1 + n1 * n1;
   const double* t1 = T;
   const double* t1i = cplx_ ? T + plane : nullptr;
-  const double* T2 = T + n1;
   const double* Vi = cplx_ ? Vpphh_ + vi_pphh_ : nullptr;
   double* Si = cplx_ ? S_ + si_ : nullptr;
   TriplesOutcome out;
@@ -348,12 +360,12 @@ TriplesOutcome Triples::run(const double* T) {
   out.flops = 2.0 * double(o) * o * o * double(v) * v * v * double(o + v);
   void* e0 = ops::event_create();
   void* e1 = ops::event_create();
-  if (complete_) {
-    ops::event_record(e0, s_);
-    complete_intermediates(T);
-    ops::event_record(e1, s_);
-    out.setup_seconds += ops::event_ms(e0, e1) * 1e-3;
-  }
+  ops::event_record(e0, s_);
+  if (complete_) complete_intermediates(T);
+  concat_operands(T, Vppph_, Vhhhp_, Ac_, Bc_);
+  if (complete_) concat_operands(T, Ip_, Ih_, AcM_, BcM_);
+  ops::event_record(e1, s_);
+  out.setup_seconds += ops::event_ms(e0, e1) * 1e-3;
   const int64_t Lm = nb * o;
   double* Mi = complete_ && cplx_ ? Mb_ + si_ : nullptr;
   // profile: events around the four phases of every block triple
@@ -377,11 +389,10 @@ TriplesOutcome Triples::run(const double* T) {
         ops::triples_singles(S_, Si, t1, t1i, Vpphh_, Vi, b, s_);
         if (complete_) zero_(Mb_, (cplx_ ? 2 : 1) * Lm * Lm * Lm);
         if (profile_) ops::event_record(pev[5 * t + 1], s_);
-        connected(T2, b, X, n, true, Vppph_, Vhhhp_, S_);
-        if (complete_) connected(T2, b, X, n, true, Ip_, Ih_, Mb_);
+        connected(b, X, n, Ac_, Bc_, S_);
+        if (complete_) connected(b, X, n, AcM_, BcM_, Mb_);
         if (profile_) ops::event_record(pev[5 * t + 2], s_);
-        connected(T2, b, X, n, false, Vppph_, Vhhhp_, S_);
-        if (complete_) connected(T2, b, X, n, false, Ip_, Ih_, Mb_);
+        // (the hole terms ride in the contractions above: the hole phase stays empty)
         if (profile_) ops::event_record(pev[5 * t + 3], s_);
         double coef[6];
         coefficients(A, B, C, coef);

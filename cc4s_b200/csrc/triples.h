@@ -79,11 +79,15 @@ class Triples : public Schedule {
   static void coefficients(int64_t A, int64_t B, int64_t C, double coef[6]);
 
  private:
-  // S += the six permutations of X = sum_d T V^p - sum_l T V^h (particle or hole
-  // half), V^p in the layout of Vppph_, V^h in the layout of Vhhhp_.
-  void connected(const double* T2, const ops::TriplesBlock& b, const int64_t X[3],
-                 const int64_t n[3], bool particle, const double* Vp, const double* Vh,
-                 double* S);
+  // S += the six permutations of X = sum_d T V^p - sum_l T V^h through the
+  // K-concatenated operands Ac (rows (pair, hole)) and Bc (columns (virtual, pair)).
+  void connected(const ops::TriplesBlock& b, const int64_t X[3], const int64_t n[3],
+                 const double* Ac, const double* Bc, double* S);
+  // Ac[(a,i)][j][k] = T_adij (k = d < v), -V^h_jail^* (k = v + l);
+  // Bc[b][(c,k)][k'] = V^p_bcdk (k' = d < v), T_cbkl (k' = v + l); V^p in the layout of
+  // Vppph_, V^h in that of Vhhhp_.
+  void concat_operands(const double* T, const double* Vp, const double* Vh, double* Ac,
+                       double* Bc);
   // I_bcek into Ip_ and I_mcjk into Ih_ at amplitudes T (cT branch).
   void complete_intermediates(const double* T);
   // beta C + alpha V_pqsr for the integral slice `name` (LO RO LI RI), C labelled
@@ -101,6 +105,12 @@ class Triples : public Schedule {
   double* Ip_ = nullptr;     // cT: I_bcdk in the layout of Vppph_
   double* Ih_ = nullptr;     // cT: I_lcjk as [j][(c,k)][l], the layout of Vhhhp_
   double* Mb_ = nullptr;     // cT: block array of M (layout of S_)
+  // K-concatenated operands of the block contractions (K = v + o; second pair for M)
+  double* Ac_ = nullptr;
+  double* Bc_ = nullptr;
+  double* AcM_ = nullptr;
+  double* BcM_ = nullptr;
+  int64_t kc_ = 0, ai_ = 0, bi_ = 0;  // v + o; imaginary-plane offsets of Ac, Bc
   double* ws_ = nullptr;     // reduction partials
   double* slots_ = nullptr;  // two energy sums of every block triple, then their totals
   int64_t ntri_ = 0;

@@ -227,6 +227,20 @@ void permute4(double* dst, const double* src, const int64_t d[4], const int perm
         }
 }
 
+void copy4(double* dst, const int64_t ds[4], const double* src, const int64_t ss[4],
+           const int64_t e[4], double alpha, double beta, Stream) {
+  ++g_ops;
+  if (ds[3] != 1) throw Error(ERR_STATE, "copy4: the destination's inner stride must be 1");
+  for (int64_t i0 = 0; i0 < e[0]; ++i0)
+    for (int64_t i1 = 0; i1 < e[1]; ++i1)
+      for (int64_t i2 = 0; i2 < e[2]; ++i2)
+        for (int64_t i3 = 0; i3 < e[3]; ++i3) {
+          const double v = alpha * src[i0 * ss[0] + i1 * ss[1] + i2 * ss[2] + i3 * ss[3]];
+          double* d = dst + i0 * ds[0] + i1 * ds[1] + i2 * ds[2] + i3;
+          *d = beta != 0.0 ? v + beta * *d : v;
+        }
+}
+
 void axpby(double* out, double a, const double* x, double b, const double* y, double c,
            int64_t n, Stream) {
   ++g_ops;
