@@ -709,7 +709,8 @@ def run_triples(args, local):
         st0 = so.stats()
         for k in range(args.warmup + args.steps):
             with ClockSampler(local) as clk:
-                r = so.perturbative_triples(args.triples_block)
+                r = so.perturbative_triples(args.triples_block, reference_form=args.cT,
+                                            cT=args.cT)
             runs.append((r, clk.summary()))
         st1 = so.stats()
         so.close()
@@ -731,6 +732,7 @@ def run_triples(args, local):
     e = PerturbativeTriples().run({"slicedEigenEnergies": {"h": eh, "p": ep}, "coulombVertex": g,
                                    "halfGrid": hg, "amplitudes": {"ph": T[0], "pphh": T[1]},
                                    "precision": head, "blockSize": args.triples_block,
+                                   "referenceForm": args.cT, "cT": int(args.cT),
                                    "device": local})
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
@@ -741,9 +743,9 @@ def run_triples(args, local):
         peak = pk.get("bf16_tflops", 1686.1)
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": "whole (T) block loop: split_kernel particle contractions, FP64 hole "
-                          "contractions, singles and energy kernels (six FP16 slice products per "
-                          "executed FP64 multiply-add)",
+                "kernel": "whole (T) block loop: split_kernel contractions (particle and hole "
+                          "halves over K = v + o), singles and energy kernels (six FP16 slice "
+                          "products per executed FP64 multiply-add)",
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)"}
     else:
         achieved = hr["executed_flops"] / hr["seconds"] / 1e12
@@ -756,7 +758,8 @@ def run_triples(args, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * hr["seconds"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; amplitudes after two CCSD iterations)",
-            "config": {"workload": "(T) %s: No=%d Nv=%d NG=%d real, %s" % (cfg, o, v, G, head),
+            "config": {"workload": "(T)%s %s: No=%d Nv=%d NG=%d real, %s" % (
+                           " cT=1" if args.cT else "", cfg, o, v, G, head),
                        "flops_reference": F, "forms": out, "fp64_dgemm_peak_tflops": dpeak,
                        "abs_dE_split_vs_fp64": abs(out["split3"]["energy"] - out["fp64"]["energy"])
                        if len(out) == 2 else None,
@@ -953,6 +956,9 @@ def main():
     ap.add_argument("--fsc-n", type=int, default=20, help="--fsc: interpolationGridSize")
     ap.add_argument("--triples-block", type=int, default=0,
                     help="virtual indices per (T) block (0: automatic)")
+    ap.add_argument("--cT", action="store_true",
+                    help="--triples: the completely renormalised branch (cT = 1) of "
+                         "PerturbativeTriplesReference")
     ap.add_argument("--shape", default=None,
                     help="No,Nv,NG of a real synthetic system instead of --config (profiling of "
                          "small cases)")

@@ -60,6 +60,17 @@ def test_triples_line():
     assert line["e2e"]["h2d_bytes_per_step"] > 0
 
 
+def test_triples_cT_line():
+    """--cT: the completely renormalised branch; device and operator energies agree."""
+    import build_emu
+    line = _line(build_emu.build(), ["--triples", "--cT", "--shape", "2,6,10", "--warmup", "0",
+                                      "--steps", "1", "--precision", "fp64",
+                                      "--no-cpu-baseline"])
+    assert "cT=1" in line["config"]["workload"]
+    e = line["config"]["forms"]["fp64"]["energy"]
+    assert abs(line["e2e"]["energy"] - e) < 1e-12 * max(1.0, abs(e))
+
+
 def test_fsc_line():
     import build_emu
     line = _line(build_emu.build(), ["--fsc", "--shape", "2,6,10", "--fsc-grid", "4",
