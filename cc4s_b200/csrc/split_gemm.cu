@@ -673,7 +673,48 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
       const double sa = m < p.M ? ldexp(p.alpha, p.ea[m]) : 0.0;
       const int64_t rowoff = m < p.M ? p.Cm.off(static_cast<uint32_t>(m)) : -1;
       const int64_t rowoff2 = (m < p.M && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : -1;
-      if (m_major) {
+      if (m_major && !p.C2 && p.beta != 0.0) {
+        // Accumulating store, lanes on consecutive rows, software-pipelined: the old
+        // values of the next group of four columns are loaded before the current group
+        // is written (the elements of one output tile are distinct, so the loads may
+        // pass the stores), keeping two groups of loads in flight per lane.
+        int64_t colL[2];
+        double scL[2];
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int64_t nl = n0 + 64 * half + 32 * h2 + lane;
+          colL[h2] = nl < p.N ? p.Cn.off(static_cast<uint32_t>(nl)) : -1;
+          scL[h2] = nl < p.N ? pow2i(p.eb[nl]) : 0.0;
+        }
+        auto fetch = [&](int g, double* (&ptr)[4], double (&val)[4], double (&old)[4]) {
+          const int h2 = g >> 3, j0 = (g & 7) * 4;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int64_t col = __shfl_sync(0xffffffffu, colL[h2], j0 + j);
+            const double sc = __shfl_sync(0xffffffffu, scL[h2], j0 + j);
+            val[j] = acc[32 * h2 + j0 + j] * sa * sc;
+            ptr[j] = (rowoff >= 0 && col >= 0) ? p.C + rowoff + col : nullptr;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) old[j] = ptr[j] ? *ptr[j] : 0.0;
+        };
+        double* pc[4];
+        double vc[4], oc[4];
+        fetch(0, pc, vc, oc);
+#pragma unroll
+        for (int g = 0; g < 16; ++g) {
+          double* pn[4];
+          double vn[4], on[4];
+          if (g + 1 < 16) fetch(g + 1, pn, vn, on);
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (pc[j]) *pc[j] = vc[j] + p.beta * oc[j];
+          if (g + 1 < 16) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) { pc[j] = pn[j]; vc[j] = vn[j]; oc[j] = on[j]; }
+          }
+        }
+      } else if (m_major) {
         // lanes are consecutive rows: store column by column straight from registers
 #pragma unroll
         for (int h2 = 0; h2 < 2; ++h2) {
@@ -702,6 +743,51 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
               rmw_store<4>(ptr, val, p.beta);
             }
           }
+        }
+      } else if (!p.C2 && p.beta != 0.0) {
+        // Accumulating store, lanes along columns (16-column pieces through the warp's
+        // buffer), pipelined like the row-major case: the old values of the next four
+        // rows are loaded before the current four are written.
+#pragma unroll
+        for (int piece = 0; piece < 4; ++piece) {
+          const int cc = lane & 15;
+          const int64_t nn = n0 + 64 * half + 16 * piece + cc;
+          const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
+          const double scL = nn < p.N ? pow2i(p.eb[nn]) : 0.0;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const double sc = __shfl_sync(0xffffffffu, scL, j);
+            wb[lane * 16 + (j ^ (lane & 15))] = acc[16 * piece + j] * sa * sc;
+          }
+          __syncwarp();
+          auto fetch = [&](int k0, double* (&ptr)[4], double (&val)[4], double (&old)[4]) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int r = 2 * (k0 + k) + (lane >> 4);
+              const int64_t ro = __shfl_sync(0xffffffffu, rowoff, r);
+              val[k] = wb[r * 16 + (cc ^ (r & 15))];
+              ptr[k] = (ro >= 0 && cn >= 0) ? p.C + ro + cn : nullptr;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) old[k] = ptr[k] ? *ptr[k] : 0.0;
+          };
+          double* pc[4];
+          double vc[4], oc[4];
+          fetch(0, pc, vc, oc);
+#pragma unroll
+          for (int k0 = 0; k0 < 16; k0 += 4) {
+            double* pn[4];
+            double vn[4], on[4];
+            if (k0 + 4 < 16) fetch(k0 + 4, pn, vn, on);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              if (pc[k]) *pc[k] = vc[k] + p.beta * oc[k];
+            if (k0 + 4 < 16) {
+#pragma unroll
+              for (int k = 0; k < 4; ++k) { pc[k] = pn[k]; vc[k] = vn[k]; oc[k] = on[k]; }
+            }
+          }
+          __syncwarp();
         }
       } else {
         // 16-column pieces through the warp's buffer; lanes then run along columns
