@@ -472,8 +472,8 @@ def run_adjoint(args, local):
 
     def fd_energy(gm):
         # the FP64 fixed point from the converged amplitudes: split iterations until
-        # the residuum norm is below 1e-6, FP64 iterations to energyConvergence 1e-13
-        so = Solver(dict(base, precision="split3", precisionRefinement=1e-6, **tight))
+        # the residuum norm is below 1e-7, FP64 iterations to energyConvergence 1e-13
+        so = Solver(dict(base, precision="split3", precisionRefinement=1e-7, **tight))
         so.set_inputs(eh, ep, gm, half_grid=hg)
         so.set_initial_amplitudes(*T0)
         r = so.run()
