@@ -119,6 +119,26 @@ void Schedule::tc_packed_b_(const Contraction& c, const SplitPackedB& b) {
   gemm_split_packed_b(c, b, s_, split_);
 }
 
+void Schedule::tc_prepacked_(const Contraction& c, const SplitOperand& A, const SplitRuns& ar,
+                             const SplitOperand& B, const SplitRuns& br) {
+  if (taping_) throw Error(ERR_STATE, "pre-packed split operands are not recorded");
+  if (!split_.error) split_reserve(size_t(1) << 16, split_extra_bytes_);  // the error word
+  const double f = 2.0 * double(c.M) * double(c.N) * double(c.K);
+  if (count_flops_) flops_ += f;
+  if (profile_ && count_flops_) {
+    const size_t k = ev_flops_.size();
+    while (ev_.size() < 2 * (k + 1)) ev_.push_back(ops::event_create());
+    ev_flops_.push_back(f);
+    ev_split_.push_back(1);
+    ev_shape_.push_back({c.M, c.N, c.K, c.batch});
+    ops::event_record(ev_[2 * k], s_);
+    gemm_split_prepacked(c, A, ar, B, br, s_, split_);
+    ops::event_record(ev_[2 * k + 1], s_);
+    return;
+  }
+  gemm_split_prepacked(c, A, ar, B, br, s_, split_);
+}
+
 // A contraction of the reverse sweep (or a recomputed forward one): split
 // precision under the same rule as tc_, else FP64; neither recorded nor counted.
 void Schedule::exec_(const Contraction& c) {

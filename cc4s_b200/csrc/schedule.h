@@ -157,6 +157,10 @@ class Schedule {
   void split_reserve(size_t regular, size_t extra);
   // One split contraction whose B was sliced by split_pack_b (recorded like tc_).
   void tc_packed_b_(const Contraction& c, const SplitPackedB& b);
+  // One split contraction with both operands sliced beforehand (split_pack_operand);
+  // counted and profiled like tc_, not recorded.
+  void tc_prepacked_(const Contraction& c, const SplitOperand& A, const SplitRuns& ar,
+                     const SplitOperand& B, const SplitRuns& br);
   void exec_(const Contraction& c);
   // C = alpha * op(A) op(B) + beta * C on planar complex operands: the
   // imaginary plane of each operand sits at the given element offset (0: the

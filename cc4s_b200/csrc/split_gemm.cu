@@ -303,13 +303,19 @@ __device__ __forceinline__ void rmw_store(double* const (&ptr)[NB], const double
 
 struct SplitParams {
   int64_t M, N, K;                 // logical extents
-  int64_t Mp, Np;                  // padded row counts of the packed operands
+  int64_t Mp, Np;                  // padded row counts of the packed operands (slice strides)
   int nkb;                         // k-blocks of TK
   Ax Cm, Cn, C2m, C2n;
   double* C; double* C2;
   double alpha, beta;
-  const int* ea; const int* eb;    // row exponents of A (m) and of B (n)
+  const int* ea; const int* eb;    // exponents of the packed rows of A and of B
   int* error;
+  // Packed rows (persistent kernel): logical row m of A is packed row
+  //   a_base + (m / a_run) * a_stride + m % a_run,
+  // and tiles never straddle a run (a_tiles tiles per run, nMt tile rows in all);
+  // likewise n for B.  One run over the whole extent is the plain case.
+  int64_t a_run, a_stride, a_base, a_tiles, nMt;
+  int64_t b_run, b_stride, b_base, b_tiles, nNt;
 };
 
 __global__ void __launch_bounds__(320)
@@ -512,15 +518,30 @@ split_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
 constexpr int WBUF_DOUBLES = 32 * 16;
 constexpr int SMEM_BYTES_P = NST * STAGE_BYTES + 8 * WBUF_DOUBLES * 8 + 1024 + 256;
 
-__device__ __forceinline__ void tile_origin(const SplitParams& p, int64_t t, int64_t& m0,
-                                            int64_t& n0) {
-  const int64_t nM = p.Mp / TM, nN = p.Np / TN;
+// Tile t in the grouped raster order: logical origins (m0, n0), packed-row origins
+// (pa, pb) and the valid extents (mlim, nlim) of the tile.
+struct TileAt {
+  int64_t m0, n0, pa, pb;
+  int mlim, nlim;
+};
+__device__ __forceinline__ TileAt tile_at(const SplitParams& p, int64_t t) {
+  const int64_t nM = p.nMt, nN = p.nNt;
   const int64_t per_group = RASTER_M * nN, group = t / per_group;
   const int64_t first = group * RASTER_M;
   const int64_t rows = nM - first < RASTER_M ? nM - first : RASTER_M;
   const int64_t in = t - group * per_group;
-  m0 = (first + in % rows) * TM;
-  n0 = (in / rows) * TN;
+  const int64_t tm = first + in % rows, tn = in / rows;
+  TileAt a;
+  const int64_t rm = tm / p.a_tiles, om = (tm - rm * p.a_tiles) * TM;
+  const int64_t rn = tn / p.b_tiles, on = (tn - rn * p.b_tiles) * TN;
+  a.m0 = rm * p.a_run + om;
+  a.n0 = rn * p.b_run + on;
+  a.pa = p.a_base + rm * p.a_stride + om;
+  a.pb = p.b_base + rn * p.b_stride + on;
+  const int64_t ml = min(p.a_run - om, p.M - a.m0), nl = min(p.b_run - on, p.N - a.n0);
+  a.mlim = static_cast<int>(ml < 0 ? 0 : (ml > TM ? TM : ml));
+  a.nlim = static_cast<int>(nl < 0 ? 0 : (nl > TN ? TN : nl));
+  return a;
 }
 
 __global__ void __launch_bounds__(320)
@@ -536,7 +557,7 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
   volatile int* abort_v = &abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t ntiles = (p.Mp / TM) * (p.Np / TN);
+  const int64_t ntiles = p.nMt * p.nNt;
   const int nchunks = (p.nkb * TK + KCHUNK - 1) / KCHUNK;
   constexpr int KB_PER_CHUNK = KCHUNK / TK;
 
@@ -564,8 +585,7 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
     // ---- TMA producer: every k-block of every tile of this CTA ----
     uint32_t it = 0;
     for (int64_t t = blockIdx.x; t < ntiles && !*abort_v; t += gridDim.x) {
-      int64_t m0, n0;
-      tile_origin(p, t, m0, n0);
+      const TileAt ta = tile_at(p, t);
       for (int kb = 0; kb < p.nkb; ++kb, ++it) {
         const int s = it % NST;
         if (it >= NST && !mbar_wait(smem_u32(&bars[NST + s]), ((it / NST) - 1) & 1)) {
@@ -578,9 +598,9 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
         unsigned char* st = base + s * STAGE_BYTES;
         for (int q = 0; q < NSLICE; ++q) {
           tma_load_2d(smem_u32(st + q * TILE_BYTES), &tmA, full, kb * TK,
-                      static_cast<int>(q * p.Mp + m0));
+                      static_cast<int>(q * p.Mp + ta.pa));
           tma_load_2d(smem_u32(st + (NSLICE + q) * TILE_BYTES), &tmB, full, kb * TK,
-                      static_cast<int>(q * p.Np + n0));
+                      static_cast<int>(q * p.Np + ta.pb));
         }
       }
     }
@@ -632,8 +652,8 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
     uint32_t q = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
       if (__any_sync(0xffffffffu, *abort_v != 0)) break;
-      int64_t m0, n0;
-      tile_origin(p, t, m0, n0);
+      const TileAt ta = tile_at(p, t);
+      const int64_t m0 = ta.m0, n0 = ta.n0;
       double acc[64];
 #pragma unroll
       for (int j = 0; j < 64; ++j) acc[j] = 0.0;
@@ -670,9 +690,10 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
       // columns; both reach the lanes that store an element through warp shuffles
       // (offset -1: outside the output).
       const int64_t m = m0 + row;
-      const double sa = m < p.M ? ldexp(p.alpha, p.ea[m]) : 0.0;
-      const int64_t rowoff = m < p.M ? p.Cm.off(static_cast<uint32_t>(m)) : -1;
-      const int64_t rowoff2 = (m < p.M && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : -1;
+      const bool mv = row < ta.mlim;
+      const double sa = mv ? ldexp(p.alpha, p.ea[ta.pa + row]) : 0.0;
+      const int64_t rowoff = mv ? p.Cm.off(static_cast<uint32_t>(m)) : -1;
+      const int64_t rowoff2 = (mv && p.C2) ? p.C2m.off(static_cast<uint32_t>(m)) : -1;
       if (m_major && !p.C2 && p.beta != 0.0) {
         // Accumulating store, lanes on consecutive rows, software-pipelined: the old
         // values of the next group of four columns are loaded before the current group
@@ -682,9 +703,9 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
         double scL[2];
 #pragma unroll
         for (int h2 = 0; h2 < 2; ++h2) {
-          const int64_t nl = n0 + 64 * half + 32 * h2 + lane;
-          colL[h2] = nl < p.N ? p.Cn.off(static_cast<uint32_t>(nl)) : -1;
-          scL[h2] = nl < p.N ? pow2i(p.eb[nl]) : 0.0;
+          const int jl = 64 * half + 32 * h2 + lane;
+          colL[h2] = jl < ta.nlim ? p.Cn.off(static_cast<uint32_t>(n0 + jl)) : -1;
+          scL[h2] = jl < ta.nlim ? pow2i(p.eb[ta.pb + jl]) : 0.0;
         }
         auto fetch = [&](int g, double* (&ptr)[4], double (&val)[4], double (&old)[4]) {
           const int h2 = g >> 3, j0 = (g & 7) * 4;
@@ -718,9 +739,9 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
         // lanes are consecutive rows: store column by column straight from registers
 #pragma unroll
         for (int h2 = 0; h2 < 2; ++h2) {
-          const int64_t nl = n0 + 64 * half + 32 * h2 + lane;  // this lane's column of the group
-          const int64_t colL = nl < p.N ? p.Cn.off(static_cast<uint32_t>(nl)) : -1;
-          const double scL = nl < p.N ? pow2i(p.eb[nl]) : 0.0;
+          const int jl = 64 * half + 32 * h2 + lane;  // this lane's column of the group
+          const int64_t colL = jl < ta.nlim ? p.Cn.off(static_cast<uint32_t>(n0 + jl)) : -1;
+          const double scL = jl < ta.nlim ? pow2i(p.eb[ta.pb + jl]) : 0.0;
 #pragma unroll
           for (int j0 = 0; j0 < 32; j0 += 4) {
             double* ptr[4];
@@ -736,9 +757,9 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
             if (p.C2) {
 #pragma unroll
               for (int j = 0; j < 4; ++j) {
-                const int64_t n = n0 + 64 * half + 32 * h2 + j0 + j;
-                ptr[j] = (rowoff2 >= 0 && n < p.N)
-                             ? p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n)) : nullptr;
+                const int jc = 64 * half + 32 * h2 + j0 + j;
+                ptr[j] = (rowoff2 >= 0 && jc < ta.nlim)
+                             ? p.C2 + rowoff2 + p.C2n.off(static_cast<uint32_t>(n0 + jc)) : nullptr;
               }
               rmw_store<4>(ptr, val, p.beta);
             }
@@ -751,9 +772,10 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
 #pragma unroll
         for (int piece = 0; piece < 4; ++piece) {
           const int cc = lane & 15;
-          const int64_t nn = n0 + 64 * half + 16 * piece + cc;
-          const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
-          const double scL = nn < p.N ? pow2i(p.eb[nn]) : 0.0;
+          const int jn = 64 * half + 16 * piece + cc;
+          const int64_t nn = n0 + jn;
+          const int64_t cn = jn < ta.nlim ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
+          const double scL = jn < ta.nlim ? pow2i(p.eb[ta.pb + jn]) : 0.0;
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const double sc = __shfl_sync(0xffffffffu, scL, j);
@@ -794,9 +816,10 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
 #pragma unroll
         for (int piece = 0; piece < 4; ++piece) {
           const int cc = lane & 15;  // this lane's column within the piece
-          const int64_t nn = n0 + 64 * half + 16 * piece + cc;
-          const int64_t cn = nn < p.N ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
-          const double scL = nn < p.N ? pow2i(p.eb[nn]) : 0.0;
+          const int jn = 64 * half + 16 * piece + cc;
+          const int64_t nn = n0 + jn;
+          const int64_t cn = jn < ta.nlim ? p.Cn.off(static_cast<uint32_t>(nn)) : -1;
+          const double scL = jn < ta.nlim ? pow2i(p.eb[ta.pb + jn]) : 0.0;
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const double sc = __shfl_sync(0xffffffffu, scL, j);
@@ -816,7 +839,7 @@ split_kernel_persistent(const __grid_constant__ CUtensorMap tmA,
             }
             rmw_store<4>(ptr, val, p.beta);
             if (p.C2) {
-              const int64_t cn2 = nn < p.N ? p.C2n.off(static_cast<uint32_t>(nn)) : -1;
+              const int64_t cn2 = jn < ta.nlim ? p.C2n.off(static_cast<uint32_t>(nn)) : -1;
 #pragma unroll
               for (int k = 0; k < 4; ++k) {
                 const int r = 2 * (k0 + k) + (lane >> 4);
@@ -1033,6 +1056,29 @@ void gemm_split(const Contraction& g, cudaStream_t s, SplitScratch& ws) {
 
 namespace {
 
+// Persistent tile loop by default; CC4S_SPLIT_PERSISTENT=0 selects one tile per CTA.
+bool persistent_mode() {
+  static const bool persistent = [] {
+    const char* e = std::getenv("CC4S_SPLIT_PERSISTENT");
+    return !(e && e[0] == '0');
+  }();
+  return persistent;
+}
+
+void launch_persistent(const CUtensorMap& ta, const CUtensorMap& tb, const SplitParams& sp,
+                       int64_t tiles, cudaStream_t s) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    CC_CHECK(cudaGetDevice(&dev));
+    CC_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CC_CHECK(cudaFuncSetAttribute(split_kernel_persistent,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES_P));
+  }
+  dim3 grid(static_cast<unsigned>(std::min<int64_t>(tiles, sms)));
+  split_kernel_persistent<<<grid, 320, SMEM_BYTES_P, s>>>(ta, tb, sp);
+}
+
 void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws, const SplitPackedB* pb) {
   const Layout2 L = layout_of(g);
   // with a pre-packed B the scratch holds A and the metadata only
@@ -1071,24 +1117,12 @@ void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws, const S
   sp.alpha = g.alpha; sp.beta = g.beta;
   sp.ea = aexp; sp.eb = bexp;
   sp.error = ws.error;
+  sp.a_run = g.M; sp.a_stride = 0; sp.a_base = 0; sp.a_tiles = L.Mp / TM; sp.nMt = L.Mp / TM;
+  sp.b_run = g.N; sp.b_stride = 0; sp.b_base = 0; sp.b_tiles = L.Np / TN; sp.nNt = L.Np / TN;
   const int64_t tiles = (L.Np / TN) * (L.Mp / TM);
   if (tiles >= (int64_t(1) << 31)) throw Error(ERR_BAD_SHAPE, "gemm_split: too many tiles");
-  // Persistent tile loop by default; CC4S_SPLIT_PERSISTENT=0 selects one tile per CTA.
-  static const bool persistent = [] {
-    const char* e = std::getenv("CC4S_SPLIT_PERSISTENT");
-    return !(e && e[0] == '0');
-  }();
-  if (persistent) {
-    static int sms = 0;
-    if (!sms) {
-      int dev = 0;
-      CC_CHECK(cudaGetDevice(&dev));
-      CC_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      CC_CHECK(cudaFuncSetAttribute(split_kernel_persistent,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES_P));
-    }
-    dim3 grid(static_cast<unsigned>(std::min<int64_t>(tiles, sms)));
-    split_kernel_persistent<<<grid, 320, SMEM_BYTES_P, s>>>(ta, tb, sp);
+  if (persistent_mode()) {
+    launch_persistent(ta, tb, sp, tiles, s);
   } else {
     static bool configured = false;
     if (!configured) {
@@ -1103,4 +1137,78 @@ void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws, const S
 }
 
 }  // namespace
+size_t split_operand_bytes(int64_t R, int64_t K) {
+  const int64_t Rp = rup(std::max<int64_t>(R, 1), TM), Kp = rup(std::max<int64_t>(K, 1), TK);
+  return static_cast<size_t>(rup(NSLICE * Rp * Kp * 2, 1024) + rup(Rp * 8, 1024) +
+                             rup(Rp * 4, 1024));
+}
+
+SplitOperand split_pack_operand(const double* src, int64_t R, int64_t Ri, int64_t s_ro,
+                                int64_t s_ri, int64_t K, int64_t s_k, void* dst, cudaStream_t s) {
+  if (R <= 0 || K <= 0) throw Error(ERR_BAD_SHAPE, "split_pack_operand: empty operand");
+  SplitOperand o;
+  o.R = R; o.K = K;
+  o.Rp = rup(R, TM);
+  o.Kp = rup(K, TK);
+  if (o.Rp * NSLICE >= (int64_t(1) << 31) || o.Kp >= (int64_t(1) << 31))
+    throw Error(ERR_BAD_SHAPE, "split_pack_operand: extent too large");
+  unsigned char* p = static_cast<unsigned char*>(dst);
+  const int64_t sb = rup(NSLICE * o.Rp * o.Kp * 2, 1024);
+  o.slices = p;
+  auto* rmax = reinterpret_cast<unsigned long long*>(p + sb);
+  o.exps = reinterpret_cast<int*>(p + sb + rup(o.Rp * 8, 1024));
+  Contraction g;
+  g.M = R; g.Mi = Ri; g.K = K;
+  g.A.p = const_cast<double*>(src);
+  g.A.s_ro = s_ro; g.A.s_ri = s_ri; g.A.s_co = 0; g.A.s_ci = s_k;
+  pack(g.A, true, g, R, o.Rp, o.Kp, static_cast<__half*>(o.slices), rmax, o.exps, s);
+  return o;
+}
+
+void gemm_split_prepacked(const Contraction& g, const SplitOperand& A, const SplitRuns& ar,
+                          const SplitOperand& B, const SplitRuns& br, cudaStream_t s,
+                          SplitScratch& ws) {
+  if (g.M <= 0 || g.N <= 0) return;
+  if (!persistent_mode())
+    throw Error(ERR_UNSUPPORTED, "gemm_split_prepacked: needs the persistent kernel");
+  if (A.K != g.K || B.K != g.K || A.Kp != B.Kp)
+    throw Error(ERR_INVALID_ARGUMENT, "gemm_split_prepacked: operands of another K");
+  // every packed row that a valid logical row reads lies inside the operand
+  auto check = [](const SplitRuns& r, int64_t X, int64_t R, const char* what) {
+    if (r.run <= 0 || r.base < 0 || r.stride < 0)
+      throw Error(ERR_INVALID_ARGUMENT, std::string("gemm_split_prepacked: bad runs of ") + what);
+    const int64_t nr = (X + r.run - 1) / r.run;
+    const int64_t last = r.base + (nr - 1) * r.stride + std::min(r.run, X - (nr - 1) * r.run) - 1;
+    const int64_t full_last = nr > 1 ? r.base + (nr - 2) * r.stride + r.run - 1 : -1;
+    if (last >= R || full_last >= R)
+      throw Error(ERR_INVALID_ARGUMENT, std::string("gemm_split_prepacked: runs of ") + what +
+                                            " leave the operand");
+    return nr;
+  };
+  const int64_t nra = check(ar, g.M, A.R, "A"), nrb = check(br, g.N, B.R, "B");
+  const CUtensorMap ta = make_map(A.slices, NSLICE * A.Rp, A.Kp);
+  const CUtensorMap tb = make_map(B.slices, NSLICE * B.Rp, B.Kp);
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  SplitParams sp;
+  sp.M = g.M; sp.N = g.N; sp.K = g.K; sp.Mp = A.Rp; sp.Np = B.Rp;
+  sp.nkb = static_cast<int>(A.Kp / TK);
+  sp.Cm = mkax(Mi, g.C.s_ro, g.C.s_ri);
+  sp.Cn = mkax(Ni, g.C.s_co, g.C.s_ci);
+  sp.C2m = mkax(Mi, g.C2.s_ro, g.C2.s_ri);
+  sp.C2n = mkax(Ni, g.C2.s_co, g.C2.s_ci);
+  sp.C = g.C.p; sp.C2 = g.C2.p;
+  sp.alpha = g.alpha; sp.beta = g.beta;
+  sp.ea = A.exps; sp.eb = B.exps;
+  sp.error = ws.error;
+  sp.a_run = ar.run; sp.a_stride = ar.stride; sp.a_base = ar.base;
+  sp.a_tiles = (ar.run + TM - 1) / TM; sp.nMt = nra * sp.a_tiles;
+  sp.b_run = br.run; sp.b_stride = br.stride; sp.b_base = br.base;
+  sp.b_tiles = (br.run + TN - 1) / TN; sp.nNt = nrb * sp.b_tiles;
+  const int64_t tiles = sp.nMt * sp.nNt;
+  if (tiles >= (int64_t(1) << 31)) throw Error(ERR_BAD_SHAPE, "gemm_split_prepacked: too many tiles");
+  launch_persistent(ta, tb, sp, tiles, s);
+  CC_LAUNCH_CHECK();
+  g_split_launches.fetch_add(1);
+}
+
 }  // namespace cc4s_b200

@@ -52,6 +52,33 @@ SplitPackedB split_pack_b(const Contraction& g, void* dst, cudaStream_t s);
 void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream_t s,
                          SplitScratch& ws);
 
+// An operand sliced once for many contractions: R rows of K elements as three FP16
+// planes [3][Rp][Kp] with one power-of-two exponent per row (the scaling of every
+// row over its whole K, as gemm_split slices its operands).
+struct SplitOperand {
+  void* slices = nullptr;
+  int* exps = nullptr;   // [Rp]
+  int64_t R = 0, K = 0, Rp = 0, Kp = 0;
+};
+// Device bytes of a sliced operand of R rows and K columns.
+size_t split_operand_bytes(int64_t R, int64_t K);
+// Slices the rows of src into dst (device memory of split_operand_bytes bytes):
+// element (r, k) at src[(r / Ri) * s_ro + (r % Ri) * s_ri + k * s_k] (Ri = 0: one level).
+SplitOperand split_pack_operand(const double* src, int64_t R, int64_t Ri, int64_t s_ro,
+                                int64_t s_ri, int64_t K, int64_t s_k, void* dst, cudaStream_t s);
+// The rows of a contraction inside a sliced operand: logical index x is packed row
+//   base + (x / run) * stride + x % run.
+struct SplitRuns {
+  int64_t base = 0, run = 0, stride = 0;
+};
+// C = alpha A B + beta C (g gives M, N, K, the output views, alpha, beta) with the rows
+// m of A and the columns n of B taken from sliced operands (B sliced by its columns,
+// i.e. its rows are n).  Tiles never straddle a run, so a run shorter than a tile
+// costs a partial tile.  Persistent kernel only.
+void gemm_split_prepacked(const Contraction& g, const SplitOperand& A, const SplitRuns& ar,
+                          const SplitOperand& B, const SplitRuns& br, cudaStream_t s,
+                          SplitScratch& ws);
+
 uint64_t split_launch_count();
 
 }  // namespace cc4s_b200

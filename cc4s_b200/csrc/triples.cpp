@@ -172,6 +172,70 @@ void Triples::connected(const ops::TriplesBlock& b, const int64_t X[3], const in
   }
 }
 
+void Triples::pack_operands(int w, const double* Ac, const double* Bc) {
+  const int64_t o = o_, v = v_, n1 = n1_, kc = kc_;
+  const int planes = cplx_ ? 2 : 1;
+  const size_t ba = split_operand_bytes(n1 * o, kc), bb = split_operand_bytes(v * n1, kc);
+  const size_t per = 2 * ba + bb;
+  if (!sl_mem_[w]) sl_mem_[w] = take((planes * per + 7) / 8);
+  unsigned char* p = reinterpret_cast<unsigned char*>(sl_mem_[w]);
+  for (int pl = 0; pl < planes; ++pl, p += per) {
+    const double* A = Ac + pl * ai_;
+    const double* B = Bc + pl * bi_;
+    Sliced& s = sl_[w][pl];
+    s.A = split_pack_operand(A, n1 * o, 0, 0, kc, kc, 1, p, s_);
+    s.A2 = split_pack_operand(A, o * n1, n1, kc, o * kc, kc, 1, p + ba, s_);
+    s.B = split_pack_operand(B, v * n1, 0, 0, kc, kc, 1, p + 2 * ba, s_);
+  }
+}
+
+void Triples::connected_packed(const ops::TriplesBlock& b, const int64_t X[3], const int64_t n[3],
+                               int w, double* S) {
+  static const int PQR[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}};
+  const int64_t o = o_, n1 = n1_;
+  const int64_t sP[3] = {b.L[1] * b.L[2], b.L[2], 1};
+  for (const auto& t : PQR) {
+    const int p = t[0], q = t[1], r = t[2];
+    Contraction c;
+    c.M = b.L[p] * o; c.N = n[q] * b.L[r]; c.Ni = b.L[r]; c.K = kc_;
+    SplitRuns ar, br;
+    const bool inner_pair = p == 2;  // rows (hole q, pair p): pair p contiguous in S
+    if (inner_pair) {
+      c.Mi = b.L[p];
+      c.C = vw(S, sP[q], sP[p], o * sP[q], sP[r]);
+      ar.base = b.P[p]; ar.run = b.L[p]; ar.stride = n1;
+    } else {
+      c.Mi = o;
+      c.C = vw(S, sP[p], sP[q], o * sP[q], sP[r]);
+      ar.base = b.P[p] * o; ar.run = c.M; ar.stride = 0;
+    }
+    br.base = X[q] * n1 + b.P[r]; br.run = b.L[r]; br.stride = n1;
+    c.alpha = 1.0; c.beta = 1.0;
+    if (c.M < 64 || c.N < 64) {  // too small for the split form (a ragged last block): FP64
+      const double* Ac = w ? AcM_ : Ac_;
+      const double* Bc = w ? BcM_ : Bc_;
+      c.A = inner_pair ? vw(cp(Ac) + b.P[p] * o * kc_, kc_, o * kc_, 0, 1)
+                       : vw(cp(Ac) + b.P[p] * o * kc_, o * kc_, kc_, 0, 1);
+      c.B = vw(cp(Bc) + (X[q] * n1 + b.P[r]) * kc_, 0, 1, n1 * kc_, kc_);
+      zgemm(c, ai_, bi_, si_, false, false, false);
+      continue;
+    }
+    const Sliced& re = sl_[w][0];
+    auto A = [&](const Sliced& s) -> const SplitOperand& { return inner_pair ? s.A2 : s.A; };
+    tc_prepacked_(c, A(re), ar, re.B, br);
+    if (cplx_) {  // Re C -= Im A Im B; Im C += Re A Im B + Im A Re B
+      const Sliced& im = sl_[w][1];
+      Contraction d = c;
+      d.alpha = -1.0;
+      tc_prepacked_(d, A(im), ar, im.B, br);
+      d = c;
+      d.C.p = S + si_;
+      tc_prepacked_(d, A(re), ar, im.B, br);
+      tc_prepacked_(d, A(im), ar, re.B, br);
+    }
+  }
+}
+
 void Triples::concat_operands(const double* T, const double* Vp, const double* Vh, double* Ac,
                               double* Bc) {
   const int64_t o = o_, v = v_, n1 = n1_, kc = kc_;
@@ -364,6 +428,12 @@ TriplesOutcome Triples::run(const double* T) {
   if (complete_) complete_intermediates(T);
   concat_operands(T, Vppph_, Vhhhp_, Ac_, Bc_);
   if (complete_) concat_operands(T, Ip_, Ih_, AcM_, BcM_);
+  // split form (the contractions' K = v + o long enough for it): both operands sliced once here
+  const bool packed = precision_ == 3 && kc_ >= 64;
+  if (packed) {
+    pack_operands(0, Ac_, Bc_);
+    if (complete_) pack_operands(1, AcM_, BcM_);
+  }
   ops::event_record(e1, s_);
   out.setup_seconds += ops::event_ms(e0, e1) * 1e-3;
   const int64_t Lm = nb * o;
@@ -389,8 +459,13 @@ TriplesOutcome Triples::run(const double* T) {
         ops::triples_singles(S_, Si, t1, t1i, Vpphh_, Vi, b, s_);
         if (complete_) zero_(Mb_, (cplx_ ? 2 : 1) * Lm * Lm * Lm);
         if (profile_) ops::event_record(pev[5 * t + 1], s_);
-        connected(b, X, n, Ac_, Bc_, S_);
-        if (complete_) connected(b, X, n, AcM_, BcM_, Mb_);
+        if (packed) {
+          connected_packed(b, X, n, 0, S_);
+          if (complete_) connected_packed(b, X, n, 1, Mb_);
+        } else {
+          connected(b, X, n, Ac_, Bc_, S_);
+          if (complete_) connected(b, X, n, AcM_, BcM_, Mb_);
+        }
         if (profile_) ops::event_record(pev[5 * t + 2], s_);
         // (the hole terms ride in the contractions above: the hole phase stays empty)
         if (profile_) ops::event_record(pev[5 * t + 3], s_);

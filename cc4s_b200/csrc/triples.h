@@ -83,6 +83,13 @@ class Triples : public Schedule {
   // K-concatenated operands Ac (rows (pair, hole)) and Bc (columns (virtual, pair)).
   void connected(const ops::TriplesBlock& b, const int64_t X[3], const int64_t n[3],
                  const double* Ac, const double* Bc, double* S);
+  // The same six contractions in the split form from operands sliced once per
+  // evaluation (w = 0: S from Ac_/Bc_, w = 1: M from AcM_/BcM_).
+  void connected_packed(const ops::TriplesBlock& b, const int64_t X[3], const int64_t n[3],
+                        int w, double* S);
+  // Slices Ac (rows (pair, hole) and (hole, pair)) and Bc (rows (virtual, pair)) of
+  // every plane for connected_packed.
+  void pack_operands(int w, const double* Ac, const double* Bc);
   // Ac[(a,i)][j][k] = T_adij (k = d < v), -V^h_jail^* (k = v + l);
   // Bc[b][(c,k)][k'] = V^p_bcdk (k' = d < v), T_cbkl (k' = v + l); V^p in the layout of
   // Vppph_, V^h in that of Vhhhp_.
@@ -111,6 +118,11 @@ class Triples : public Schedule {
   double* AcM_ = nullptr;
   double* BcM_ = nullptr;
   int64_t kc_ = 0, ai_ = 0, bi_ = 0;  // v + o; imaginary-plane offsets of Ac, Bc
+  struct Sliced {
+    SplitOperand A, A2, B;  // Ac rows (pair, hole), Ac rows (hole, pair), Bc rows (virtual, pair)
+  };
+  Sliced sl_[2][2];         // [S or M][plane]
+  double* sl_mem_[2] = {nullptr, nullptr};
   double* ws_ = nullptr;     // reduction partials
   double* slots_ = nullptr;  // two energy sums of every block triple, then their totals
   int64_t ntri_ = 0;

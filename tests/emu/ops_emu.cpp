@@ -158,6 +158,50 @@ void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream
   gemm_split(h, s, ws);
 }
 
+// Sliced operands: the emulation keeps the rows as a dense copy [R][K] and slices the
+// rows a contraction reads again in gemm_split (same rows, same slices).
+size_t split_operand_bytes(int64_t R, int64_t K) { return size_t(R) * K * 8 + 64; }
+
+SplitOperand split_pack_operand(const double* src, int64_t R, int64_t Ri, int64_t s_ro,
+                                int64_t s_ri, int64_t K, int64_t s_k, void* dst, cudaStream_t) {
+  if (R <= 0 || K <= 0) throw Error(ERR_BAD_SHAPE, "split_pack_operand: empty operand");
+  Ax r = ax(Ri > 0 ? Ri : R, s_ro, s_ri);
+  double* d = static_cast<double*>(dst);
+  for (int64_t i = 0; i < R; ++i)
+    for (int64_t k = 0; k < K; ++k) d[i * K + k] = src[r.off(i) + k * s_k];
+  SplitOperand o;
+  o.slices = dst; o.R = R; o.K = K; o.Rp = R; o.Kp = K;
+  return o;
+}
+
+void gemm_split_prepacked(const Contraction& g, const SplitOperand& A, const SplitRuns& ar,
+                          const SplitOperand& B, const SplitRuns& br, cudaStream_t s,
+                          SplitScratch& ws) {
+  if (g.M <= 0 || g.N <= 0) return;
+  if (A.K != g.K || B.K != g.K)
+    throw Error(ERR_INVALID_ARGUMENT, "gemm_split_prepacked: operands of another K");
+  const int64_t K = g.K;
+  auto rows = [&](const SplitOperand& o, const SplitRuns& r, int64_t X) {
+    if (r.run <= 0) throw Error(ERR_INVALID_ARGUMENT, "gemm_split_prepacked: bad runs");
+    std::vector<double> d(size_t(X) * K);
+    const double* src = static_cast<const double*>(o.slices);
+    for (int64_t x = 0; x < X; ++x) {
+      const int64_t pr = r.base + (x / r.run) * r.stride + x % r.run;
+      if (pr < 0 || pr >= o.R)
+        throw Error(ERR_INVALID_ARGUMENT, "gemm_split_prepacked: runs leave the operand");
+      for (int64_t k = 0; k < K; ++k) d[x * K + k] = src[pr * K + k];
+    }
+    return d;
+  };
+  std::vector<double> Ad = rows(A, ar, g.M), Bd = rows(B, br, g.N);
+  const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
+  Contraction h = g;
+  h.Ki = 0;
+  h.A.p = Ad.data(); h.A.s_ro = Mi * K; h.A.s_ri = K; h.A.s_co = 0; h.A.s_ci = 1;
+  h.B.p = Bd.data(); h.B.s_ro = 0; h.B.s_ri = 1; h.B.s_co = Ni * K; h.B.s_ci = K;
+  gemm_split(h, s, ws);
+}
+
 // Plain-loop stand-in for the allocation-free energy entry (host pointers).
 int energy_noalloc(const double* T1, const double* T2, const double* V, int64_t o, int64_t v,
                    int cplx, double* out, cudaStream_t, const char** err) {

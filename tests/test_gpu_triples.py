@@ -197,3 +197,29 @@ def test_triples_complete_matches_oracle(cplx, block, precision):
         sol.close()
     tol = TOL_FP64 if precision == "fp64" else TOL_SPLIT
     assert abs(e - ref) < tol * abs(ref), (e, ref)
+
+
+@pytest.mark.parametrize("cplx,cT", [(True, False), (False, True)])
+def test_triples_split_sliced_operands_match_fp64(cplx, cT):
+    """The split form with both operands of the block contractions sliced once per
+    evaluation (K = v + o = 66, blocks of 11 with a ragged last block) against the
+    device FP64 energy, on the complex path (atrip's conjugation) and for cT = 1."""
+    from cc4s_b200 import Solver
+    No, Nv = 6, 60
+    s = inputs.synthetic_system(No, Nv, 80, complex=cplx, seed=5)
+    rng = np.random.default_rng(6)
+    T1, T2 = _rand_T(rng, Nv, No, scale=0.01)
+    if cplx:
+        U1, U2 = _rand_T(rng, Nv, No, scale=0.01)
+        T1, T2 = T1 + 1j * U1, T2 + 1j * U2
+    e = {}
+    for p in ("fp64", "split3"):
+        sol = Solver({"precision": p})
+        try:
+            sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+            sol.set_initial_amplitudes(T1, T2)
+            e[p] = sol.perturbative_triples(11, reference_form=cT, cT=cT)["correlation"]
+        finally:
+            sol.close()
+    assert abs(e["split3"] - e["fp64"]) < TOL_SPLIT * abs(e["fp64"]), e
+    assert e["split3"] != e["fp64"]  # the split form ran
