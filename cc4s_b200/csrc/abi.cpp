@@ -742,7 +742,8 @@ int cc4s_cc_finite_size_correction(cc4s_cc_handle* h, const double* singular_vec
 int cc4s_cc_get_stats(const cc4s_cc_handle* h, cc4s_cc_stats* out) {
   if (!h || !h->impl || !out) return CC4S_ERR_INVALID_ARGUMENT;
   // each split-precision contraction is two slicing launches plus the tensor-core kernel
-  out->gemm_launches = cc4s_b200::gemm_launch_count() + 3 * cc4s_b200::split_launch_count();
+  out->gemm_launches = cc4s_b200::gemm_launch_count() + cc4s_b200::split_launch_count() +
+                       cc4s_b200::split_pack_launch_count();
   out->other_launches = cc4s_b200::ops::launch_count();
   size_t bytes = 0;
   if (h->impl->solver) bytes += h->impl->solver->device_bytes();

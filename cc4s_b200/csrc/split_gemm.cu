@@ -53,6 +53,7 @@ constexpr uint32_t WAIT_LIMIT = 1u << 28;         // bounded mbarrier waits
 constexpr int64_t RASTER_M = 8;                  // tile rows per raster group
 
 std::atomic<uint64_t> g_split_launches{0};
+std::atomic<uint64_t> g_pack_launches{0};
 
 struct Ax {
   uint32_t inner;
@@ -941,6 +942,7 @@ void pack(const View& v, bool rows_are_m, const Contraction& g, int64_t R, int64
   CC_LAUNCH_CHECK();
   pack_slices_kernel<<<static_cast<unsigned>(std::min<int64_t>(tiles, 148 * 8)), PTHREADS, 0, s>>>(a);
   CC_LAUNCH_CHECK();
+  g_pack_launches.fetch_add(2);
 }
 
 // Packed slices of both operands are limited to this many bytes: a longer K is
@@ -998,6 +1000,7 @@ void split_panel(const Contraction& g, cudaStream_t s, SplitScratch& ws,
 }  // namespace
 
 uint64_t split_launch_count() { return g_split_launches.load(); }
+uint64_t split_pack_launch_count() { return g_pack_launches.load(); }
 
 size_t gemm_split_scratch_bytes(const Contraction& g) {
   Contraction h = g;

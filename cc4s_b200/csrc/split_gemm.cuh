@@ -80,5 +80,7 @@ void gemm_split_prepacked(const Contraction& g, const SplitOperand& A, const Spl
                           SplitScratch& ws);
 
 uint64_t split_launch_count();
+// Number of operand-slicing kernel launches issued so far (two per sliced operand).
+uint64_t split_pack_launch_count();
 
 }  // namespace cc4s_b200

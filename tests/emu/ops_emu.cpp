@@ -65,12 +65,14 @@ void gemm(const Contraction& g, cudaStream_t, const GemmScratch&) {
 // integer slices (6, 11, 11 bits) and the six slice products p + q <= 2
 // (0-based), summed exactly in FP64 (the device sums the leading group exactly
 // in FP32 per 4096-wide chunk; the lower groups differ only below 2^-50 relative).
-static uint64_t g_split = 0;
+static uint64_t g_split = 0, g_pack = 0;
 uint64_t split_launch_count() { return g_split; }
+uint64_t split_pack_launch_count() { return g_pack; }
 size_t gemm_split_scratch_bytes(const Contraction&) { return 64; }
 
 void gemm_split(const Contraction& g, cudaStream_t, SplitScratch&) {
   ++g_split;
+  g_pack += 4;  // the device slices both operands (two launches each)
   const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
   const int64_t Ki = g.Ki > 0 ? g.Ki : std::max<int64_t>(g.K, 1);
   Ax Am = ax(Mi, g.A.s_ro, g.A.s_ri), Ak = ax(Ki, g.A.s_co, g.A.s_ci);
@@ -145,6 +147,7 @@ SplitPackedB split_pack_b(const Contraction& g, void* dst, cudaStream_t) {
     for (int64_t k = 0; k < g.K; ++k) d[n * g.K + k] = g.B.p[Bk.off(k) + Bn.off(n)];
   SplitPackedB b;
   b.slices = dst; b.N = g.N; b.K = g.K; b.Np = g.N; b.Kp = g.K;
+  g_pack += 2;
   return b;
 }
 
@@ -156,6 +159,7 @@ void gemm_split_packed_b(const Contraction& g, const SplitPackedB& b, cudaStream
   h.B.p = static_cast<double*>(b.slices);
   h.B.s_ro = Ki; h.B.s_ri = 1; h.B.s_co = Ni * g.K; h.B.s_ci = g.K;
   gemm_split(h, s, ws);
+  g_pack -= 2;  // B was sliced before
 }
 
 // Sliced operands: the emulation keeps the rows as a dense copy [R][K] and slices the
@@ -171,6 +175,7 @@ SplitOperand split_pack_operand(const double* src, int64_t R, int64_t Ri, int64_
     for (int64_t k = 0; k < K; ++k) d[i * K + k] = src[r.off(i) + k * s_k];
   SplitOperand o;
   o.slices = dst; o.R = R; o.K = K; o.Rp = R; o.Kp = K;
+  g_pack += 2;
   return o;
 }
 
@@ -194,6 +199,7 @@ void gemm_split_prepacked(const Contraction& g, const SplitOperand& A, const Spl
     return d;
   };
   std::vector<double> Ad = rows(A, ar, g.M), Bd = rows(B, br, g.N);
+  g_pack -= 4;  // nothing is sliced here on the device (gemm_split below counts four)
   const int64_t Mi = g.Mi > 0 ? g.Mi : g.M, Ni = g.Ni > 0 ? g.Ni : g.N;
   Contraction h = g;
   h.Ki = 0;
