@@ -270,6 +270,13 @@ FP64_OVER_SPLIT_BOUND = 4.5
 # generation, of one handle's set-up (vertex upload, integral build) and of the
 # CPU baseline leg.  projected_seconds() uses them to check that the driver's
 # command fits its time limit.
+# DRAM traffic of the split contraction kernel at c2, from one ncu capture of the 851
+# split launches of one iteration (dram__bytes_read.sum + dram__bytes_write.sum; the
+# capture's command and the per-class figures are in profiles/launches_ccsd_c2_split.md):
+# 15.09 TB in all, 17.73 GB per launch, 3.6x the algorithmic bytes (packed slices of
+# both operands read once, the output read and written once).
+SPLIT_TRAFFIC_C2 = {"bytes_per_launch": 17.73e9, "algorithmic_bytes_per_launch": 4.9e9,
+                    "launches": 851}
 MEASURED_C2 = {"split3": 12.0, "fp64": 69.7, "inputs": 60.0, "setup": 30.0, "cpu": 40.0,
                "download": 15.0}
 
@@ -364,6 +371,12 @@ def run_ours(args, world, rank, local):
                           "library stream" % ps["split_launches"],
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
                 "fp64_equivalent_tflops": ps["split_flops"] / ps["split_seconds"] / 1e12}
+        if cfg == "c2":
+            roof["traffic"] = SPLIT_TRAFFIC_C2["bytes_per_launch"]
+            roof["traffic_note"] = (
+                "bytes per launch, mean over the %d split launches of one iteration (one ncu "
+                "capture); algorithmic %.2g bytes per launch" %
+                (SPLIT_TRAFFIC_C2["launches"], SPLIT_TRAFFIC_C2["algorithmic_bytes_per_launch"]))
     else:
         achieved = ps["gemm_flops"] / ps["gemm_seconds"] / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
