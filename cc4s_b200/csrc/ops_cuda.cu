@@ -1135,71 +1135,38 @@ __global__ void triples_singles_kernel(TriplesArgs a) {
   }
 }
 
-// The energy of one block triple.  Work items are (virtual triple (x1, x2, x3) of the
-// block, tile of 8 x 8 x 8 hole indices); for an item the six hole-permuted tiles of
-// the block array that Y = sum_k coef_k S(perm_k) reads are staged in shared memory
-// (rows of 8 consecutive doubles along the contiguous index), then every element of
-// the item is evaluated from them.  A fixed grid walks the items in a fixed order, so
-// the partial sums are deterministic.
-constexpr int TE = 8, TE3 = TE * TE * TE;
-
 template <bool CPLX>
-__global__ void __launch_bounds__(RED_THREADS) triples_energy_kernel(TriplesArgs a) {
-  extern __shared__ double tiles[];  // [6][TE3], then the imaginary planes [6][TE3]
-  const int o = static_cast<int>(a.o);
-  const int64_t L23 = a.L2 * a.L3, L3 = a.L3;
-  const int64_t n2 = a.L2 / o, n3 = a.L3 / o, n1 = a.total / (L23 * o);
-  const int nt = (o + TE - 1) / TE;
-  const int64_t nt3 = static_cast<int64_t>(nt) * nt * nt;
-  const int64_t items = n1 * n2 * n3 * nt3;
+__global__ void triples_energy_kernel(TriplesArgs a) {
+  const int64_t L23 = a.L2 * a.L3, o = a.o;
   const int64_t X1 = a.P1 / o, X2 = a.P2 / o, X3 = a.P3 / o;
-  // the hole positions (first, second, third) read by permutation k, as indices into
-  // (y0, y1, y2): 012, 021, 102, 120, 201, 210
-  const int PK[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
   double acc[2] = {0.0, 0.0};
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int64_t cube = it / nt3;
-    const int tt = static_cast<int>(it - cube * nt3);
-    const int64_t x1 = cube / (n2 * n3), x2 = (cube / n3) % n2, x3 = cube % n3;
-    const int T[3] = {tt / (nt * nt), (tt / nt) % nt, tt % nt};
-    const int64_t base = x1 * o * L23 + x2 * o * L3 + x3 * o;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q1 = e / L23, r = e - q1 * L23, q2 = r / a.L3, q3 = r - q2 * a.L3;
+    const int64_t x1 = q1 / o, x2 = q2 / o, x3 = q3 / o;
+    const int64_t y0 = q1 - x1 * o, y1 = q2 - x2 * o, y2 = q3 - x3 * o;
+    const Cplx sg = triples_singles_at<CPLX>(a, a.P1 + q1, a.P2 + q2, a.P3 + q3);
+    const double d = a.eh[y0] + a.eh[y1] + a.eh[y2] - a.ep[X1 + x1] - a.ep[X2 + x2] -
+                     a.ep[X3 + x3];
+    const int64_t b1 = x1 * o * L23, b2 = x2 * o * a.L3, b3 = x3 * o;
+    // the hole permutations 012, 021, 102, 120, 201, 210 of the pair (a, b, c)
+    const int64_t idx[6] = {e,
+                            b1 + y0 * L23 + b2 + y2 * a.L3 + b3 + y1,
+                            b1 + y1 * L23 + b2 + y0 * a.L3 + b3 + y2,
+                            b1 + y1 * L23 + b2 + y2 * a.L3 + b3 + y0,
+                            b1 + y2 * L23 + b2 + y0 * a.L3 + b3 + y1,
+                            b1 + y2 * L23 + b2 + y1 * a.L3 + b3 + y0};
+    double yr = 0.0, yi = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      if (k > 0 && a.coef[k] == 0.0) continue;
-      const int Ta = T[PK[k][0]], Tb = T[PK[k][1]], Tc = T[PK[k][2]];
-      for (int j = threadIdx.x; j < TE3; j += blockDim.x) {
-        const int u = j / (TE * TE), v = (j / TE) % TE, w = j % TE;
-        const int ya = Ta * TE + u, yb = Tb * TE + v, yc = Tc * TE + w;
-        const bool in = ya < o && yb < o && yc < o;
-        const int64_t e = base + ya * L23 + yb * L3 + yc;
-        tiles[k * TE3 + j] = in ? a.S[e] : 0.0;
-        if (CPLX) tiles[(6 + k) * TE3 + j] = in ? a.Si[e] : 0.0;
-      }
+      if (a.coef[k] == 0.0) continue;
+      yr += a.coef[k] * a.S[idx[k]];
+      if (CPLX) yi += a.coef[k] * a.Si[idx[k]];
     }
-    __syncthreads();
-    for (int j = threadIdx.x; j < TE3; j += blockDim.x) {
-      const int i[3] = {j / (TE * TE), (j / TE) % TE, j % TE};
-      const int y0 = T[0] * TE + i[0], y1 = T[1] * TE + i[1], y2 = T[2] * TE + i[2];
-      if (y0 >= o || y1 >= o || y2 >= o) continue;
-      double yr = 0.0, yi = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        if (a.coef[k] == 0.0) continue;
-        const int q = (i[PK[k][0]] * TE + i[PK[k][1]]) * TE + i[PK[k][2]];
-        yr += a.coef[k] * tiles[k * TE3 + q];
-        if (CPLX) yi += a.coef[k] * tiles[(6 + k) * TE3 + q];
-      }
-      const int64_t q1 = x1 * o + y0, q2 = x2 * o + y1, q3 = x3 * o + y2;
-      const int64_t e = q1 * L23 + q2 * L3 + q3;
-      const Cplx sg = triples_singles_at<CPLX>(a, a.P1 + q1, a.P2 + q2, a.P3 + q3);
-      const double d = a.eh[y0] + a.eh[y1] + a.eh[y2] - a.ep[X1 + x1] - a.ep[X2 + x2] -
-                       a.ep[X3 + x3];
-      const double inv = 1.0 / d;
-      const double wr = a.M ? a.M[e] : tiles[j] - sg.re;
-      acc[0] += wr * yr * inv;
-      if (CPLX) acc[1] += (a.M ? a.Mi[e] : tiles[6 * TE3 + j] - sg.im) * yi * inv;
-    }
-    __syncthreads();
+    const double inv = 1.0 / d;
+    const double wr = a.M ? a.M[e] : a.S[e] - sg.re;
+    acc[0] += wr * yr * inv;
+    if (CPLX) acc[1] += (a.M ? a.Mi[e] : a.Si[e] - sg.im) * yi * inv;
   }
   block_sum<2>(acc);
   if (threadIdx.x == 0) {
@@ -1241,21 +1208,10 @@ void triples_energy(const double* S, const double* S_im, const double* t1, const
   a.S = S; a.Si = S_im; a.eh = eps_h; a.ep = eps_p; a.ws = ws;
   a.M = M; a.Mi = M_im;
   for (int k = 0; k < 6; ++k) a.coef[k] = coef[k];
-  if (b.o <= 0 || b.L[0] % b.o || b.L[1] % b.o || b.L[2] % b.o)
-    throw Error(ERR_STATE, "triples_energy: block extents are not whole virtual indices");
-  // the six staged tiles (and their imaginary planes): 24 KB real, 48 KB complex
-  static const bool configured = [] {
-    CC_CHECK(cudaFuncSetAttribute(triples_energy_kernel<true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * TE3 * 8));
-    CC_CHECK(cudaFuncSetAttribute(triples_energy_kernel<false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, 6 * TE3 * 8));
-    return true;
-  }();
-  (void)configured;
   if (S_im)
-    triples_energy_kernel<true><<<RED_BLOCKS, RED_THREADS, 12 * TE3 * 8, s>>>(a);
+    triples_energy_kernel<true><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
   else
-    triples_energy_kernel<false><<<RED_BLOCKS, RED_THREADS, 6 * TE3 * 8, s>>>(a);
+    triples_energy_kernel<false><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
   CC_LAUNCH_CHECK();
   count();
   finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 1.0, 1.0, 1.0, 1.0);
