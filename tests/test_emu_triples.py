@@ -257,3 +257,31 @@ def test_complete_intermediates_reduce_to_integrals_at_zero_amplitudes():
     J = triples.complete_triples_intermediates(s, z1, z2)
     V = inputs.coulomb_integrals(s, ["ppph", "hphh"])
     assert np.array_equal(J["ppph"], V["ppph"]) and np.array_equal(J["hphh"], V["hphh"])
+
+
+def test_triples_split_sliced_operands(emu_lib):
+    """The split form once K = v + o >= 64: both concatenated operands sliced once per
+    evaluation, every block contraction reading its rows through runs (the p = 2 terms
+    from the (hole, pair) slicing, the columns from runs of one block of pairs), against
+    the FP64 form of the same schedule; the slicing happens outside the block loop."""
+    from cc4s_b200.coupled_cluster import Solver
+    No, Nv = 4, 64
+    s = inputs.synthetic_system(No, Nv, 60, seed=4)
+    T1, T2 = _rand_T(np.random.default_rng(8), Nv, No)
+    e, st = {}, {}
+    for p in ("fp64", "split3"):
+        sol = Solver({"precision": p}, lib=emu_lib)
+        try:
+            sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+            sol.set_initial_amplitudes(T1, T2)
+            s0 = sol.stats()
+            e[p] = sol.perturbative_triples(8)["correlation"]
+            s1 = sol.stats()
+            st[p] = s1["gemm_launches"] - s0["gemm_launches"]
+        finally:
+            sol.close()
+    assert abs(e["split3"] - e["fp64"]) < 1e-7 * abs(e["fp64"]), e
+    assert e["split3"] != e["fp64"]
+    # 120 block triples x 6 contractions, plus 3 x 2 slicing launches for the operands
+    # and the integral builds (FP64): far fewer than 5 launches per split contraction
+    assert st["split3"] < 2 * 120 * 6, st
