@@ -19,14 +19,15 @@
 //
 // For every block triple A <= B <= C the block array S[(a,i)][(b,j)][(c,k)]
 // (a in A, b in B, c in C, pair layout) is formed on the device: the singles
-// first, then the twelve contractions (six particle terms over d, six hole
-// terms over l), each writing its permutation of X straight into the pair
-// layout through the strided output view.  The energy kernel then sums over
+// first, then six contractions over K = v + o, each the particle term of one
+// output arrangement and the (transposed) hole term that writes the same
+// elements, each writing its permutation of X straight into the pair layout
+// through the strided output view.  The energy kernel then sums over
 // the block; the other orderings of the three blocks are folded in through the
 // symmetry of W and S under simultaneous permutations, which turns each
 // ordering into a permutation of the hole indices inside the same block
 // (coefficients()).  Blocks sized so that the block array stays in L2 keep the
-// twelve read-modify-write passes of the contractions on chip.
+// six read-modify-write passes of the contractions on chip.
 #pragma once
 
 #include "ccsd_complex.h"
