@@ -265,18 +265,19 @@ DEFAULT_VERTEX_SCALE = 0.2
 FP64_OVER_SPLIT_BOUND = 4.5
 
 
+# DRAM traffic of the split contraction kernel at c2, from one ncu capture of the 851
+# split launches of one iteration (dram__bytes_read.sum + dram__bytes_write.sum with
+# -k regex:split_kernel -c 851 around `bench.py --config c2 --precision split3 --steps 1
+# --warmup 1 --no-cpu-baseline`): 15.09 TB in all, 17.73 GB per launch, 3.6x the
+# algorithmic bytes (packed slices of both operands read once, the output read and
+# written once).
+SPLIT_TRAFFIC_C2 = {"bytes_per_launch": 17.73e9, "algorithmic_bytes_per_launch": 4.9e9,
+                    "launches": 851}
 # Measured on one B200 at c2 (No=64, Nv=640, NG=2560, real): seconds per full
 # iteration of each form (CUDA events), and wall seconds of the host-side input
 # generation, of one handle's set-up (vertex upload, integral build) and of the
-# CPU baseline leg.  projected_seconds() uses them to check that the driver's
-# command fits its time limit.
-# DRAM traffic of the split contraction kernel at c2, from one ncu capture of the 851
-# split launches of one iteration (dram__bytes_read.sum + dram__bytes_write.sum; the
-# capture's command and the per-class figures are in profiles/launches_ccsd_c2_split.md):
-# 15.09 TB in all, 17.73 GB per launch, 3.6x the algorithmic bytes (packed slices of
-# both operands read once, the output read and written once).
-SPLIT_TRAFFIC_C2 = {"bytes_per_launch": 17.73e9, "algorithmic_bytes_per_launch": 4.9e9,
-                    "launches": 851}
+# CPU baseline leg.  projected_seconds() uses them to check that the default
+# benchmark command (--steps 20 --warmup 5) fits a 1800 s limit.
 MEASURED_C2 = {"split3": 12.0, "fp64": 69.7, "inputs": 60.0, "setup": 30.0, "cpu": 40.0,
                "download": 15.0}
 

@@ -104,7 +104,7 @@ def test_ccsd_line():
     assert line["warmup"] == 3 and line["steps"] == 1
 
 
-def test_driver_command_fits_its_limit():
+def test_default_benchmark_command_fits_its_limit():
     """`bench.py --gpus 1 --steps 20 --warmup 5` at c2 (the measured seconds per
     iteration of both forms) projects well inside the 1800 s limit of a bench
     step, and the FP64 comparison is not skipped by the default 1500 s budget."""
