@@ -92,7 +92,7 @@ class TriplesResult(ctypes.Structure):
         ("setup_seconds", ctypes.c_double), ("flops", ctypes.c_double),
         ("executed_flops", ctypes.c_double), ("block_size", ctypes.c_int64),
         ("block_triples", ctypes.c_int64), ("phase_seconds", ctypes.c_double * 4),
-        ("mp2_energy", ctypes.c_double),
+        ("mp2_energy", ctypes.c_double), ("cr_denominator", ctypes.c_double),
     ]
 
 

@@ -216,6 +216,9 @@ class Solver:
                     setup_seconds=r.setup_seconds, flops=r.flops,
                     executed_flops=r.executed_flops, block_size=r.block_size,
                     block_triples=r.block_triples, mp2_energy=r.mp2_energy,
+                    cr_denominator=r.cr_denominator,
+                    cr_correlation=(r.correlation / r.cr_denominator
+                                    if r.cr_denominator != 0.0 else None),
                     phase_seconds=dict(zip(("singles", "particle", "hole", "energy"),
                                            list(r.phase_seconds))))
 

@@ -490,6 +490,7 @@ void Handle::triples(const cc4s_cc_triples_options& o, cc4s_cc_triples_result* o
   out->block_size = r.block;
   out->block_triples = r.block_triples;
   for (int k = 0; k < 4; ++k) out->phase_seconds[k] = r.phase_seconds[k];
+  out->cr_denominator = r.cr_denominator;
   // the basis MP2 energy of the (T*) ratio (PerturbativeTriplesStar.hpp:79-99)
   ops::mp2_energy(solver->Vd(), solver->Vd_im(), sys.eh, sys.ep, shape.o, shape.v, scal, ws,
                   stream);

@@ -193,6 +193,16 @@ void triples_energy(const double* S, const double* S_im, const double* t1, const
                     const double* eps_p, const TriplesBlock& b, const double coef[6],
                     double* ws, double* out_dev, Stream s, const double* M = nullptr,
                     const double* M_im = nullptr);
+// The block-triple part of the CR-(T) denominator of the cT branch (ct::getDenominator,
+// CompleteTriples.cxx:138-162, reduced to sum y conj(Z) / D): out_dev[0] = sum Re y Re Z / D,
+// out_dev[1] = sum Im y Im Z / D over the block, with
+//   y = t_ai t_bj t_ck + t_ai T_bcjk + t_bj T_acik + t_ck T_abij
+// (T2 in the pair layout, planar) and Z the hole-permutation combination of S of
+// triples_energy; ws as there.
+void triples_cr_sums(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                     const double* T2, const double* T2_im, const double* eps_h,
+                     const double* eps_p, const TriplesBlock& b, const double coef[6],
+                     double* ws, double* out_dev, Stream s);
 
 // Number of bandwidth-kernel launches issued so far.
 uint64_t launch_count();

@@ -1175,6 +1175,53 @@ __global__ void triples_energy_kernel(TriplesArgs a) {
   }
 }
 
+// The CR-(T) sums of one block triple: the element loop of triples_energy_kernel with
+// y (amplitudes only) in place of W; `b2` is `a` with the pair-layout T2 in place of V.
+template <bool CPLX>
+__global__ void triples_cr_kernel(TriplesArgs a, TriplesArgs b2) {
+  const int64_t L23 = a.L2 * a.L3, o = a.o;
+  const int64_t X1 = a.P1 / o, X2 = a.P2 / o, X3 = a.P3 / o;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < a.total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t q1 = e / L23, r = e - q1 * L23, q2 = r / a.L3, q3 = r - q2 * a.L3;
+    const int64_t x1 = q1 / o, x2 = q2 / o, x3 = q3 / o;
+    const int64_t y0 = q1 - x1 * o, y1 = q2 - x2 * o, y2 = q3 - x3 * o;
+    const int64_t p1 = a.P1 + q1, p2 = a.P2 + q2, p3 = a.P3 + q3;
+    const Cplx ts = triples_singles_at<CPLX>(b2, p1, p2, p3);
+    // t_ai t_bj t_ck
+    const double r1 = a.t1[p1], r2 = a.t1[p2], r3 = a.t1[p3];
+    const double i1 = CPLX ? a.t1i[p1] : 0.0, i2 = CPLX ? a.t1i[p2] : 0.0,
+                 i3 = CPLX ? a.t1i[p3] : 0.0;
+    const double pr = r1 * r2 - i1 * i2, pi = r1 * i2 + i1 * r2;
+    const double yre = ts.re + pr * r3 - pi * i3, yim = ts.im + pr * i3 + pi * r3;
+    const double d = a.eh[y0] + a.eh[y1] + a.eh[y2] - a.ep[X1 + x1] - a.ep[X2 + x2] -
+                     a.ep[X3 + x3];
+    const int64_t b1 = x1 * o * L23, bb2 = x2 * o * a.L3, b3 = x3 * o;
+    const int64_t idx[6] = {e,
+                            b1 + y0 * L23 + bb2 + y2 * a.L3 + b3 + y1,
+                            b1 + y1 * L23 + bb2 + y0 * a.L3 + b3 + y2,
+                            b1 + y1 * L23 + bb2 + y2 * a.L3 + b3 + y0,
+                            b1 + y2 * L23 + bb2 + y0 * a.L3 + b3 + y1,
+                            b1 + y2 * L23 + bb2 + y1 * a.L3 + b3 + y0};
+    double zr = 0.0, zi = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (a.coef[k] == 0.0) continue;
+      zr += a.coef[k] * a.S[idx[k]];
+      if (CPLX) zi += a.coef[k] * a.Si[idx[k]];
+    }
+    const double inv = 1.0 / d;
+    acc[0] += yre * zr * inv;
+    if (CPLX) acc[1] += yim * zi * inv;
+  }
+  block_sum<2>(acc);
+  if (threadIdx.x == 0) {
+    a.ws[2 * blockIdx.x] = acc[0];
+    a.ws[2 * blockIdx.x + 1] = acc[1];
+  }
+}
+
 TriplesArgs triples_args(const double* t1, const double* t1i, const double* V, const double* Vi,
                          const TriplesBlock& b) {
   TriplesArgs a{};
@@ -1212,6 +1259,25 @@ void triples_energy(const double* S, const double* S_im, const double* t1, const
     triples_energy_kernel<true><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
   else
     triples_energy_kernel<false><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a);
+  CC_LAUNCH_CHECK();
+  count();
+  finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 1.0, 1.0, 1.0, 1.0);
+  CC_LAUNCH_CHECK();
+  count();
+}
+
+void triples_cr_sums(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                     const double* T2, const double* T2_im, const double* eps_h,
+                     const double* eps_p, const TriplesBlock& b, const double coef[6],
+                     double* ws, double* out_dev, Stream s) {
+  TriplesArgs a = triples_args(t1, t1_im, nullptr, nullptr, b);
+  a.S = S; a.Si = S_im; a.eh = eps_h; a.ep = eps_p; a.ws = ws;
+  for (int k = 0; k < 6; ++k) a.coef[k] = coef[k];
+  TriplesArgs b2 = triples_args(t1, t1_im, T2, T2_im, b);
+  if (S_im)
+    triples_cr_kernel<true><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a, b2);
+  else
+    triples_cr_kernel<false><<<RED_BLOCKS, RED_THREADS, 0, s>>>(a, b2);
   CC_LAUNCH_CHECK();
   count();
   finish_kernel<<<1, 256, 0, s>>>(out_dev, ws, RED_BLOCKS, 2, 1.0, 1.0, 1.0, 1.0);

@@ -93,6 +93,7 @@ Triples::Triples(const RealSystem& sys, const ComplexSystem* cs, const TriplesOp
     }
     ws_ = take(2048);
     slots_ = take(2 * ntri_ + 2);
+    if (complete_) cr_slots_ = take(2 * ntri_ + 2);
   } catch (...) {
     release_all();
     throw;
@@ -409,6 +410,36 @@ void Triples::complete_intermediates(const double* T) {
   ein(1.0, T2("dfkj"), R(Xa, "cmdf"), 1.0, R(Ih, "mcjk"));
 }
 
+double Triples::cr_amplitude_terms(const double* T) {
+  const int64_t o = o_, v = v_, n1 = n1_, n2 = n1 * n1;
+  const int64_t plane = n1 + n2;
+  const int pl = cplx_ ? 2 : 1;
+  double* X = take(pl * n2);   // T2 + t1 t1^T
+  double* Tx = take(pl * n2);  // T_baij in the pair layout
+  double* r = take(8);
+  const int64_t d[4] = {v, o, v, o};
+  const int perm[4] = {2, 1, 0, 3};
+  if (cplx_) {
+    ops::zrank1(X, X + n2, T + n1, T + plane + n1, T, T + plane, 1.0, n1, s_);
+  } else {
+    ops::rank1(X, 1.0, T + n1, 1.0, T, n1, s_);
+  }
+  for (int p = 0; p < pl; ++p) {
+    ops::permute4(Tx + p * n2, T + p * plane + n1, d, perm, 1.0, 0.0, s_);
+    const double* ys[2] = {T + p * plane + n1, Tx + p * n2};
+    ops::dots(X + p * n2, ys, 2, n2, r + 2 * p, ws_, s_);
+    const double* t1s[1] = {T + p * plane};
+    ops::dots(T + p * plane, t1s, 1, n1, r + 4 + p, ws_, s_);
+  }
+  double h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  ops::d2h(h, r, 8, s_);
+  ops::sync(s_);
+  // Re sum (2T - T^x) X = sum over planes with the sign of Re(a b) = ReRe - ImIm
+  const double wc = (2.0 * h[0] - h[1]) - (cplx_ ? 2.0 * h[2] - h[3] : 0.0);
+  const double tt = h[4] - (cplx_ ? h[5] : 0.0);
+  return 1.0 + 2.0 * tt + wc;
+}
+
 TriplesOutcome Triples::run(const double* T) {
   const int64_t o = o_, v = v_, n1 = n1_, nb = nb_;
   const int64_t nbk = (v + nb - 1) / nb;
@@ -473,11 +504,16 @@ TriplesOutcome Triples::run(const double* T) {
         coefficients(A, B, C, coef);
         ops::triples_energy(S_, Si, t1, t1i, Vpphh_, Vi, sys_.eh, sys_.ep, b, coef, ws_,
                             slots_ + 2 * t, s_, complete_ ? Mb_ : nullptr, Mi);
+        if (complete_)
+          ops::triples_cr_sums(S_, Si, t1, t1i, T + n1, cplx_ ? T + plane + n1 : nullptr, sys_.eh,
+                               sys_.ep, b, coef, ws_, cr_slots_ + 2 * t, s_);
         if (profile_) ops::event_record(pev[5 * t + 4], s_);
         out.executed_flops += (complete_ ? 2.0 : 1.0) * (cplx_ ? 4.0 : 1.0) * 12.0 *
                               double(n[0] * n[1] * n[2]) * o * o * o * double(v + o);
       }
   ops::sum_partials_to(slots_ + 2 * ntri_, slots_, static_cast<int>(ntri_), 2, s_);
+  if (complete_)
+    ops::sum_partials_to(cr_slots_ + 2 * ntri_, cr_slots_, static_cast<int>(ntri_), 2, s_);
   ops::event_record(e1, s_);
   out.seconds = ops::event_ms(e0, e1) * 1e-3;
   ops::event_destroy(e0);
@@ -493,6 +529,13 @@ TriplesOutcome Triples::run(const double* T) {
   // Re conj(W) Z = ReW ReZ + ImW ImZ;  Re conj(W) conj(Z) = ReW ReZ - ImW ImZ;
   // cT: Re M conj(Z) = ReM ReZ + ImM ImZ
   out.energy = reference_form_ && !complete_ ? sums[0] - sums[1] : sums[0] + sums[1];
+  if (complete_) {
+    double cr[2];
+    ops::d2h(cr, cr_slots_ + 2 * ntri_, 2, s_);
+    ops::sync(s_);
+    // Re y conj(Z) / D = Re y Re Z / D + Im y Im Z / D
+    out.cr_denominator = cr_amplitude_terms(T) + cr[0] + cr[1];
+  }
   return out;
 }
 

@@ -53,6 +53,9 @@ struct TriplesOutcome {
   double flops = 0.0;           // 2 o^3 v^3 (o + v), the reference's count
   double executed_flops = 0.0;  // contractions launched (whole block triples)
   int64_t block = 0, block_triples = 0;
+  // cT: the denominator of the CR-(T) energy, correlation / cr_denominator
+  // (ct::getDenominator, CompleteTriples.cxx:120-165); 0 otherwise
+  double cr_denominator = 0.0;
   // with profiling: device time of the singles, the particle contractions, the
   // hole contractions and the energy kernel, summed over the block triples
   double phase_seconds[4] = {0.0, 0.0, 0.0, 0.0};
@@ -126,6 +129,10 @@ class Triples : public Schedule {
   double* sl_mem_[2] = {nullptr, nullptr};
   double* ws_ = nullptr;     // reduction partials
   double* slots_ = nullptr;  // two energy sums of every block triple, then their totals
+  double* cr_slots_ = nullptr;  // cT: the two CR-(T) sums of every block triple, then totals
+  // cT: 1 + 2 sum t_ai t_ai + sum (2 T_abij - T_baij)(T_abij + t_ai t_bj), the amplitude-only
+  // terms of the CR-(T) denominator (real part)
+  double cr_amplitude_terms(const double* T);
   int64_t ntri_ = 0;
   double setup_seconds_ = 0.0;
 };

@@ -229,6 +229,10 @@ typedef struct {
                              (PerturbativeTriplesStar.hpp:79-99): the denominator of the
                              (T*) ratio; starCorrection = (sum of the caller's CBS pair
                              energies) / mp2_energy * correlation */
+  double cr_denominator;  /* cT = 1: the denominator of the CR-(T) energy that
+                             PerturbativeTriplesReference prints (:187-195),
+                             ct::getDenominator (CompleteTriples.cxx:120-165);
+                             CR-(T) = correlation / cr_denominator.  0 when cT = 0 */
 } cc4s_cc_triples_result;
 void cc4s_cc_triples_default_options(cc4s_cc_triples_options* opt);
 /* Perturbative triples energy at the current amplitudes (after cc4s_cc_run or

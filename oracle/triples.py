@@ -121,6 +121,39 @@ def triples_reference(T1, T2, V, eps_h, eps_p, complete=None):
     return float(np.real(np.sum(M * cj(Zs) / D)))
 
 
+def cr_triples_denominator(T1, T2, V, eps_h, eps_p):
+    """ct::getDenominator (src/main/algorithms/CompleteTriples.cxx:120-165) as the cT
+    branch calls it (PerturbativeTriplesReference.cxx:187-195), with tabcijk the
+    reference's T after :139 (conj(W)/D) and zabcijk its S after :155 (the singles'
+    4/3, -2, 2/3 combination, conjugated, over D).  The CR-(T) energy the reference
+    prints is the cT energy over this value."""
+    Vpphh, Vppph, Vhhhp = V["pphh"], V["ppph"], V["hhhp"]
+    cplx = np.iscomplexobj(T2) or np.iscomplexobj(Vppph)
+    cj = np.conj if cplx else (lambda x: x)
+    X = es("bcdk,adij->abcijk", Vppph, T2) - es("jklc,abil->abcijk", cj(Vhhhp), T2)
+    W = (X + es("bacjik->abcijk", X) + es("acbikj->abcijk", X) + es("cbakji->abcijk", X)
+         + es("cabkij->abcijk", X) + es("bcajki->abcijk", X))
+    eh = np.asarray(eps_h, dtype=float)
+    ep = np.asarray(eps_p, dtype=float)
+    D = (eh[None, None, None, :, None, None] + eh[None, None, None, None, :, None]
+         + eh[None, None, None, None, None, :] - ep[:, None, None, None, None, None]
+         - ep[None, :, None, None, None, None] - ep[None, None, :, None, None, None])
+    tT = cj(W) / D
+    # :148-156  R = T1 Vpphh (three terms), S = conj(4/3 R - 2 R_acb + 2/3 R_bca) / D
+    R = (es("ai,bcjk->abcijk", T1, Vpphh) + es("bj,acik->abcijk", T1, Vpphh)
+         + es("ck,abij->abcijk", T1, Vpphh))
+    Sz = cj((4.0 / 3.0) * R - 2.0 * es("acbijk->abcijk", R)
+            + (2.0 / 3.0) * es("bcaijk->abcijk", R)) / D
+    # CompleteTriples.cxx:138-162
+    y = (es("ai,bj,ck->abcijk", T1, T1, T1) + es("ai,bcjk->abcijk", T1, T2)
+         + es("bj,acik->abcijk", T1, T2) + es("ck,abij->abcijk", T1, T2))
+    bt = (4.0 / 3.0) * tT - 2.0 * es("acbijk->abcijk", tT) + (2.0 / 3.0) * es("bcaijk->abcijk", tT)
+    C = T2 + es("ai,bj->abij", T1, T1)
+    Wd = 2.0 * T2 - es("baij->abij", T2)
+    Dn = (2.0 * np.sum(T1 * T1) + np.sum(Wd * C) + np.sum(y * bt) + np.sum(y * Sz))
+    return float(np.real(Dn)) + 1.0
+
+
 def _atrip_doubles(a, b, c, T2, Vppph, Vhhhp, cplx):
     """Connected triples W[i,j,k] of one tuple: Equations.hpp, doublesContribution
     (GEMM branch: the hole integrals enter conjugated, MAYBE_CONJ)."""

@@ -757,5 +757,44 @@ void triples_energy(const double* S, const double* S_im, const double* t1, const
   out[1] = acc[1];
 }
 
+void triples_cr_sums(const double* S, const double* S_im, const double* t1, const double* t1_im,
+                     const double* T2, const double* T2_im, const double* eh, const double* ep,
+                     const TriplesBlock& b, const double coef[6], double*, double* out, Stream) {
+  ++g_ops;
+  static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  const int64_t o = b.o;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t q1 = 0; q1 < b.L[0]; ++q1)
+    for (int64_t q2 = 0; q2 < b.L[1]; ++q2)
+      for (int64_t q3 = 0; q3 < b.L[2]; ++q3) {
+        const int64_t x[3] = {q1 / o, q2 / o, q3 / o};
+        const int64_t y[3] = {q1 % o, q2 % o, q3 % o};
+        auto at = [&](const double* A, int64_t r1, int64_t r2, int64_t r3) {
+          return A[(r1 * b.L[1] + r2) * b.L[2] + r3];
+        };
+        const int64_t p[3] = {b.P[0] + q1, b.P[1] + q2, b.P[2] + q3};
+        const TriplesC ts = triples_singles_at(t1, t1_im, T2, T2_im, b.n1, p[0], p[1], p[2]);
+        double pr = t1[p[0]], pi = t1_im ? t1_im[p[0]] : 0.0;
+        for (int m = 1; m < 3; ++m) {
+          const double r = t1[p[m]], i = t1_im ? t1_im[p[m]] : 0.0;
+          const double nr = pr * r - pi * i, ni = pr * i + pi * r;
+          pr = nr; pi = ni;
+        }
+        double d = 0.0;
+        for (int m = 0; m < 3; ++m) d += eh[y[m]] - ep[b.P[m] / o + x[m]];
+        double zr = 0.0, zi = 0.0;
+        for (int k = 0; k < 6; ++k) {
+          const int64_t r1 = x[0] * o + y[perm[k][0]], r2 = x[1] * o + y[perm[k][1]],
+                        r3 = x[2] * o + y[perm[k][2]];
+          zr += coef[k] * at(S, r1, r2, r3);
+          if (S_im) zi += coef[k] * at(S_im, r1, r2, r3);
+        }
+        acc[0] += (ts.re + pr) * zr / d;
+        if (S_im) acc[1] += (ts.im + pi) * zi / d;
+      }
+  out[0] = acc[0];
+  out[1] = acc[1];
+}
+
 }  // namespace ops
 }  // namespace cc4s_b200

@@ -285,3 +285,28 @@ def test_triples_split_sliced_operands(emu_lib):
     # 120 block triples x 6 contractions, plus 3 x 2 slicing launches for the operands
     # and the integral builds (FP64): far fewer than 5 launches per split contraction
     assert st["split3"] < 2 * 120 * 6, st
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("shape,block", [((3, 8, 14), 0), ((2, 7, 9), 3)])
+def test_triples_cr_denominator(emu_lib, cplx, shape, block):
+    """cT = 1: the CR-(T) denominator (ct::getDenominator, CompleteTriples.cxx:120-165, as
+    PerturbativeTriplesReference.cxx:187-195 calls it) from the block loop (the sum of y
+    with the triples' Z over D, folded over block orderings like the energy) and the
+    amplitude-only terms, against the oracle; 0 without cT."""
+    from cc4s_b200.coupled_cluster import Solver
+    No, Nv, NG = shape
+    s = inputs.synthetic_system(No, Nv, NG, complex=cplx, seed=No + Nv)
+    T1, T2 = _amplitudes(np.random.default_rng(NG), Nv, No, cplx)
+    den = triples.cr_triples_denominator(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    sol = Solver({}, lib=emu_lib)
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+        sol.set_initial_amplitudes(T1, T2)
+        r = sol.perturbative_triples(block, reference_form=True, cT=True)
+        r0 = sol.perturbative_triples(block, reference_form=True)
+    finally:
+        sol.close()
+    assert abs(r["cr_denominator"] - den) < 1e-12 * abs(den), (r["cr_denominator"], den)
+    assert r["cr_correlation"] == r["correlation"] / r["cr_denominator"]
+    assert r0["cr_denominator"] == 0.0 and r0["cr_correlation"] is None

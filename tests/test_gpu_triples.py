@@ -223,3 +223,28 @@ def test_triples_split_sliced_operands_match_fp64(cplx, cT):
             sol.close()
     assert abs(e["split3"] - e["fp64"]) < TOL_SPLIT * abs(e["fp64"]), e
     assert e["split3"] != e["fp64"]  # the split form ran
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_triples_cr_denominator_matches_oracle(cplx):
+    """cT = 1: the denominator of the CR-(T) energy the reference prints
+    (PerturbativeTriplesReference.cxx:187-195, ct::getDenominator in
+    CompleteTriples.cxx:120-165), formed on the device beside the energy."""
+    from cc4s_b200 import Solver
+    No, Nv = 4, 20
+    s = inputs.synthetic_system(No, Nv, 40, complex=cplx, seed=6)
+    rng = np.random.default_rng(3)
+    T1, T2 = _rand_T(rng, Nv, No)
+    if cplx:
+        U1, U2 = _rand_T(rng, Nv, No)
+        T1, T2 = T1 + 1j * U1, T2 + 1j * U2
+    den = triples.cr_triples_denominator(T1, T2, triples.triples_integrals(s), s.eps_h, s.eps_p)
+    sol = Solver({})
+    try:
+        sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
+        sol.set_initial_amplitudes(T1, T2)
+        r = sol.perturbative_triples(3, reference_form=True, cT=True)
+    finally:
+        sol.close()
+    assert abs(r["cr_denominator"] - den) < TOL_FP64 * abs(den), (r["cr_denominator"], den)
+    assert abs(r["cr_correlation"] - r["correlation"] / den) < TOL_FP64 * abs(r["cr_correlation"])
