@@ -201,3 +201,38 @@ def test_real_path_equals_pinned_complex_path():
         assert abs(r["energy"][k] - c["energy"][k]) < 1e-12 * abs(r["energy"][k])
     assert np.abs(r["amplitudes"][1] - c["amplitudes"][1].real).max() < 1e-12
     assert np.abs(c["amplitudes"][1].imag).max() < 1e-14
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_cr_denominator_decomposition(cplx):
+    """The CR-(T) denominator restated from ct::getDenominator (CompleteTriples.cxx:
+    120-165) equals the form the device evaluates: 1 + 2 sum t t + sum (2T - T^x)(T + t t)
+    + sum y conj(Z) / D with Z the energy's 4/3, -2, 2/3 combination of S = W + singles
+    (the t-bar and z arrays of the reference sum to conj(Z) / D)."""
+    from oracle.triples import es
+    s = inputs.synthetic_system(3, 7, 14, complex=cplx, seed=11)
+    rng = np.random.default_rng(2)
+    T1 = rng.standard_normal((7, 3)) * 0.05
+    T2 = rng.standard_normal((7, 7, 3, 3)) * 0.03
+    if cplx:
+        T1 = T1 + 0.05j * rng.standard_normal((7, 3))
+        T2 = T2 + 0.03j * rng.standard_normal((7, 7, 3, 3))
+    T2 = T2 + T2.transpose(1, 0, 3, 2)
+    V = triples.triples_integrals(s)
+    den = triples.cr_triples_denominator(T1, T2, V, s.eps_h, s.eps_p)
+    cj = np.conj if cplx else (lambda x: x)
+    X = es("bcdk,adij->abcijk", V["ppph"], T2) - es("jklc,abil->abcijk", cj(V["hhhp"]), T2)
+    W = sum(es(p + "->abcijk", X) for p in
+            ("abcijk", "bacjik", "acbikj", "cbakji", "cabkij", "bcajki"))
+    S = W + (es("ai,bcjk->abcijk", T1, V["pphh"]) + es("bj,acik->abcijk", T1, V["pphh"])
+             + es("ck,abij->abcijk", T1, V["pphh"]))
+    Z = (4 / 3) * S - 2 * es("acbijk->abcijk", S) + (2 / 3) * es("bcaijk->abcijk", S)
+    eh, ep = s.eps_h, s.eps_p
+    D = (eh[None, None, None, :, None, None] + eh[None, None, None, None, :, None]
+         + eh[None, None, None, None, None, :] - ep[:, None, None, None, None, None]
+         - ep[None, :, None, None, None, None] - ep[None, None, :, None, None, None])
+    y = (es("ai,bj,ck->abcijk", T1, T1, T1) + es("ai,bcjk->abcijk", T1, T2)
+         + es("bj,acik->abcijk", T1, T2) + es("ck,abij->abcijk", T1, T2))
+    small = np.real(2 * np.sum(T1 * T1) + np.sum((2 * T2 - T2.transpose(1, 0, 2, 3))
+                                                  * (T2 + es("ai,bj->abij", T1, T1))))
+    assert abs(den - (1 + small + np.sum(np.real(y * np.conj(Z)) / D))) < 1e-13 * abs(den)
