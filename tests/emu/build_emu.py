@@ -12,7 +12,8 @@ SCHEDULE_SOURCES = ("schedule.cpp", "ccsd_real.cpp", "ccsd_complex.cpp", "drccd.
 
 def build():
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    srcs = [os.path.join(HERE, "ops_emu.cpp")] + [os.path.join(CSRC, f) for f in SCHEDULE_SOURCES]
+    srcs = ([os.path.join(HERE, "ops_emu.cpp"), os.path.join(HERE, "ein_probe.cpp")] +
+            [os.path.join(CSRC, f) for f in SCHEDULE_SOURCES])
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "cc4s_cc.h"))
     if os.path.exists(OUT) and os.path.getmtime(OUT) > max(os.path.getmtime(d) for d in deps):
