@@ -259,20 +259,22 @@ def test_complete_intermediates_reduce_to_integrals_at_zero_amplitudes():
     assert np.array_equal(J["ppph"], V["ppph"]) and np.array_equal(J["hphh"], V["hphh"])
 
 
-def test_triples_split_sliced_operands(emu_lib):
+@pytest.mark.parametrize("cplx", [False, True])
+def test_triples_split_sliced_operands(emu_lib, cplx):
     """The split form once K = v + o >= 64: both concatenated operands sliced once per
     evaluation, every block contraction reading its rows through runs (the p = 2 terms
-    from the (hole, pair) slicing, the columns from runs of one block of pairs), against
-    the FP64 form of the same schedule; the slicing happens outside the block loop."""
+    from the (hole, pair) slicing, the columns from runs of one block of pairs; on the
+    complex path four real products per contraction), against the FP64 form of the same
+    schedule; the slicing happens outside the block loop."""
     from cc4s_b200.coupled_cluster import Solver
     No, Nv = 4, 64
-    s = inputs.synthetic_system(No, Nv, 60, seed=4)
-    T1, T2 = _rand_T(np.random.default_rng(8), Nv, No)
+    s = inputs.synthetic_system(No, Nv, 60, complex=cplx, seed=4)
+    T1, T2 = _amplitudes(np.random.default_rng(8), Nv, No, cplx)
     e, st = {}, {}
     for p in ("fp64", "split3"):
         sol = Solver({"precision": p}, lib=emu_lib)
         try:
-            sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=True)
+            sol.set_inputs(s.eps_h, s.eps_p, s.gamma, half_grid=not cplx)
             sol.set_initial_amplitudes(T1, T2)
             s0 = sol.stats()
             e[p] = sol.perturbative_triples(8)["correlation"]
@@ -282,9 +284,10 @@ def test_triples_split_sliced_operands(emu_lib):
             sol.close()
     assert abs(e["split3"] - e["fp64"]) < 1e-7 * abs(e["fp64"]), e
     assert e["split3"] != e["fp64"]
-    # 120 block triples x 6 contractions, plus 3 x 2 slicing launches for the operands
-    # and the integral builds (FP64): far fewer than 5 launches per split contraction
-    assert st["split3"] < 2 * 120 * 6, st
+    # 120 block triples x 6 contractions (x 4 real products on the complex path), plus
+    # 3 x 2 slicing launches per plane and the integral builds (FP64): far fewer than 5
+    # launches per split product
+    assert st["split3"] < 2 * 120 * 6 * (4 if cplx else 1), st
 
 
 @pytest.mark.parametrize("cplx", [False, True])
